@@ -1,0 +1,158 @@
+/*
+ * lightsim2grid_b200.h -- C ABI of the B200 batched AC Newton-Raphson power-flow engine.
+ *
+ * Plain C types only: int32 indices, doubles, complex numbers as interleaved (re, im)
+ * doubles, caller-owned host buffers.  No C++ exception crosses this boundary: every
+ * entry point returns an int status (0 on success; otherwise the reference's ErrorType
+ * ordinal, src/Utils.hpp:47-56, or -1 for invalid arguments) and pf_last_error() gives a
+ * one-line description.  One plan per thread at a time; plans are not thread-safe.
+ *
+ * Each entry point names the reference interface it replaces (lightsim2grid 0.13.1).
+ */
+#ifndef LIGHTSIM2GRID_B200_H
+#define LIGHTSIM2GRID_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pf_plan pf_plan;
+
+/* Engine options.  Zero-initialised fields select the defaults. */
+typedef struct pf_options {
+    int precision;          /* 0: FP64 LU and solves (plain form); 1: FP32 LU and solves with
+                               FP64 mismatch, update and convergence test (mixed form)        */
+    int threads;            /* threads per CTA (multiple of 32, <= 512); 0: chosen by size   */
+    int lu_placement;       /* 0 auto, 1 shared memory, 2 global memory                      */
+    int chain_max_items;    /* levels with at most this many columns run on one warp; 0: 2  */
+    double pivot_threshold; /* diagonal preference of the first factorisation; 0: 1e-3      */
+    int fp64_fallback;      /* mixed form: re-run instances that did not converge in FP64.
+                               0: default (on), 1: on, 2: off                                  */
+    int max_ctas_per_sm;    /* cap on resident CTAs per SM; 0: occupancy limit               */
+} pf_options;
+
+/* Sizes and schedule statistics of a plan. */
+typedef struct pf_plan_info {
+    int n, m, nnz_ybus, nnz_j, nnz_lu;
+    int levels_refactor, levels_forward, levels_backward;
+    int groups_refactor, groups_forward, groups_backward;
+    long long flops_refactor;  /* multiply-adds of one refactorisation */
+    int precision, threads, lu_in_shared, ctas_per_sm, grid;
+    long long slab_bytes, shared_bytes;
+} pf_plan_info;
+
+/* A batch whose inputs and outputs are already in device memory (pointers from
+   cudaMalloc or torch).  Complex arrays are interleaved double pairs. */
+typedef struct pf_device_batch {
+    int n_inst;
+    const void *V0;          /* complex, n per instance (or one vector if v0_stride == 0)    */
+    long long v0_stride;     /* in complex elements                                          */
+    const void *Sbus;        /* complex, n per instance (or one vector if sbus_stride == 0)  */
+    long long sbus_stride;
+    const int *ovr_ptr;      /* n_inst + 1; Ybus overrides per instance (may be NULL)        */
+    const int *ovr_pos;      /* CSR positions of the overridden Ybus entries                  */
+    const void *ovr_val;     /* complex, new value of each overridden entry                   */
+    int max_iter;
+    double tol;
+    int chain;               /* 1: an instance starts from the previous one's solution        */
+    const int *job_first;    /* njobs; instances [job_first[j], job_first[j] + job_count[j])  */
+    const int *job_count;
+    int njobs;
+    void *Vout;              /* complex, n per instance                                       */
+    int *iters;              /* n_inst                                                        */
+    int *errs;               /* n_inst: ErrorType ordinals                                    */
+} pf_device_batch;
+
+/* Last error message of the calling thread. */
+const char *pf_last_error(void);
+
+/* Builds a plan: J pattern (bit-exact to the reference), fill-reducing order, pivots of the
+   first factorisation at V0, device schedules; uploads the structure to the current device.
+   Replaces the first-call path of BaseNRSingleSlackAlgo::compute_pf / BaseNRAlgo::compute_pf
+   (src/powerflow_algorithm/BaseNRSingleSlackAlgo.tpp:76-111, BaseNRAlgo.tpp:89-116) and
+   KLULinearSolver::initialize (src/linear_solvers/KLUSolver.cpp:24-45).
+   Ybus: CSC (colptr n+1, rowind, values), canonical (sorted rows, no duplicates).
+   distributed: 0 = single slack (KLUSolverSingleSlack), 1 = distributed slack (KLUSolver). */
+int pf_plan_create(int n, const int *colptr, const int *rowind, const double *ybus_ri, const double *V0_ri,
+                   const double *Sbus_ri, const int *slack_ids, int nslack, const double *slack_weights,
+                   const int *pv, int npv, const int *pq, int npq, int distributed, const pf_options *opts,
+                   pf_plan **out);
+
+/* Releases a plan and its device memory. */
+void pf_plan_destroy(pf_plan *plan);
+
+/* Fills *info. */
+int pf_plan_info_get(const pf_plan *plan, pf_plan_info *info);
+
+/* Replaces the base Ybus values (same pattern).  Mirrors the reference's Ybus value
+   updates between calls that keep the sparsity pattern (src/Utils.hpp:79-181, SolverControl). */
+int pf_set_ybus_values(pf_plan *plan, const double *ybus_ri);
+
+/* One power flow: BaseNRSingleSlackAlgo::compute_pf / BaseNRAlgo::compute_pf
+   (src/powerflow_algorithm/BaseNRSingleSlackAlgo.tpp:12-183, BaseNRAlgo.tpp:14-186), bound as
+   KLUSolverSingleSlack.solve / KLUSolver.solve (src/main.cpp:228-254).  V_out receives the
+   final voltages; *converged is 1 when err == NoError. */
+int pf_solve(pf_plan *plan, const double *V0_ri, const double *Sbus_ri, int max_iter, double tol, double *V_out_ri,
+             int *converged, int *iters, int *err);
+
+/* Jacobian of the last iteration of the last pf_solve, CSC.  Pass NULL arrays to get *m and
+   the number of entries (returned).  Replaces get_J_python (src/main.cpp:230). */
+int pf_get_J(pf_plan *plan, int *m, int *Jp, int *Ji, double *Jx);
+
+/* N-1 / N-k batch: ContingencyAnalysis::compute (src/batch_algorithm/ContingencyAnalysis.cpp:166-233)
+   after the base power flow.  Case c removes coef_{row,col,val}[case_ptr[c] .. case_ptr[c+1])
+   from Ybus (entries must exist in the pattern).  Islanded cases (check_invertible,
+   ContingencyAnalysis.cpp:14-45) are skipped: err = SingularMatrix, V row 0.  Every other case
+   starts from V0.  V_out is ncases x n complex, zero for cases that did not converge. */
+int pf_batch_n1(pf_plan *plan, int ncases, const int *case_ptr, const int *coef_row, const int *coef_col,
+                const double *coef_val_ri, const double *V0_ri, const double *Sbus_ri, int max_iter, double tol,
+                double *V_out_ri, int *converged, int *iters, int *errs);
+
+/* Host preparation of an N-1 batch for pf_batch_device: islanding check and Ybus overrides
+   (CSR positions, new values).  solvable[c] = 1 if case c keeps the grid connected.  Overrides
+   are written for solvable cases only, compacted; returns the number of overrides written, or
+   a negative status if `cap` is too small. */
+int pf_n1_prepare(pf_plan *plan, int ncases, const int *case_ptr, const int *coef_row, const int *coef_col,
+                  const double *coef_val_ri, int *solvable, int *ovr_ptr, int *ovr_pos, double *ovr_val_ri,
+                  int cap);
+
+/* Time series: TimeSeries::compute_Vs (src/batch_algorithm/TimeSeries.cpp:14-109).  Sbus is
+   nsteps x n complex.  The steps are cut into `nchunks` contiguous chunks; inside a chunk each
+   step starts from the previous step's solution, the first step of a chunk from V0 (nchunks = 1
+   is the reference's exact chain).  Steps after the first divergence are not reported (V row 0,
+   err = NotInitError).  Returns 0 and sets *status to 1 when every step converged. */
+int pf_batch_ts(pf_plan *plan, int nsteps, const double *Sbus_ri, const double *V0_ri, int nchunks, int max_iter,
+                double tol, double *V_out_ri, int *converged, int *iters, int *errs, int *status);
+
+/* Device-resident batch on `stream` (a cudaStream_t, NULL for the default stream).  No
+   host synchronisation; capturable in a CUDA graph once the plan exists. */
+int pf_batch_device(pf_plan *plan, const pf_device_batch *batch, void *stream);
+
+/* Timers of the last call (seconds): [0] total, [1] host preparation, [2] host->device,
+   [3] kernel, [4] device->host, [5] instances re-run in FP64 (count, as a double).
+   Replaces get_timers (src/main.cpp:236) and the batch timers (src/main.cpp:1174-1178). */
+int pf_timers(const pf_plan *plan, double *out, int nout);
+
+/* ---- host diagnostics (no device needed) ---------------------------------------------- */
+
+/* Jacobian sparsity pattern the engine builds for this problem (CSC), as the reference's
+   fill_jacobian_matrix_unkown_sparsity_pattern (BaseNRSingleSlackAlgo.tpp:247-378,
+   BaseNRAlgo.tpp:396-555).  Pass NULL Jp / Ji to get *m and the entry count (returned). */
+int pf_host_jacobian_pattern(int n, const int *colptr, const int *rowind, const double *ybus_ri,
+                             const int *slack_ids, int nslack, const double *slack_weights, const int *pv,
+                             int npv, const int *pq, int npq, int distributed, int *m, int *Jp, int *Ji);
+
+/* Runs the device schedules (refactorisation update lists and level order, forward and
+   backward substitution level order) sequentially on the host: factorises J(V) with the pivots
+   chosen at V0 and solves J x = b.  b and x are in J row / column numbering (length m).  Used
+   to test a plan's schedules on machines without a GPU. */
+int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const double *ybus_ri, const double *V0_ri,
+                           const double *V_ri, const int *slack_ids, int nslack, const double *slack_weights,
+                           const int *pv, int npv, const int *pq, int npq, int distributed, const double *b,
+                           double *x, pf_plan_info *info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIGHTSIM2GRID_B200_H */

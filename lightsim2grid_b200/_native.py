@@ -1,0 +1,133 @@
+"""ctypes binding of the C ABI declared in include/lightsim2grid_b200.h.
+
+The library is built in-tree by ``lightsim2grid_b200.build``.  There is no fallback:
+when the library is missing or no CUDA device is present the calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .build import LIB
+
+_lib = None
+
+i32p = ctypes.POINTER(ctypes.c_int32)
+f64p = ctypes.POINTER(ctypes.c_double)
+
+
+class PfOptions(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("threads", ctypes.c_int), ("lu_placement", ctypes.c_int),
+                ("chain_max_items", ctypes.c_int), ("pivot_threshold", ctypes.c_double),
+                ("fp64_fallback", ctypes.c_int), ("max_ctas_per_sm", ctypes.c_int)]
+
+
+class PfPlanInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("m", ctypes.c_int), ("nnz_ybus", ctypes.c_int), ("nnz_j", ctypes.c_int),
+                ("nnz_lu", ctypes.c_int), ("levels_refactor", ctypes.c_int), ("levels_forward", ctypes.c_int),
+                ("levels_backward", ctypes.c_int), ("groups_refactor", ctypes.c_int),
+                ("groups_forward", ctypes.c_int), ("groups_backward", ctypes.c_int),
+                ("flops_refactor", ctypes.c_longlong), ("precision", ctypes.c_int), ("threads", ctypes.c_int),
+                ("lu_in_shared", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("grid", ctypes.c_int),
+                ("slab_bytes", ctypes.c_longlong), ("shared_bytes", ctypes.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class PfDeviceBatch(ctypes.Structure):
+    _fields_ = [("n_inst", ctypes.c_int), ("V0", ctypes.c_void_p), ("v0_stride", ctypes.c_longlong),
+                ("Sbus", ctypes.c_void_p), ("sbus_stride", ctypes.c_longlong), ("ovr_ptr", ctypes.c_void_p),
+                ("ovr_pos", ctypes.c_void_p), ("ovr_val", ctypes.c_void_p), ("max_iter", ctypes.c_int),
+                ("tol", ctypes.c_double), ("chain", ctypes.c_int), ("job_first", ctypes.c_void_p),
+                ("job_count", ctypes.c_void_p), ("njobs", ctypes.c_int), ("Vout", ctypes.c_void_p),
+                ("iters", ctypes.c_void_p), ("errs", ctypes.c_void_p)]
+
+
+#: exported symbols, as declared in include/lightsim2grid_b200.h
+SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_get", "pf_set_ybus_values",
+           "pf_solve", "pf_get_J", "pf_batch_n1", "pf_n1_prepare", "pf_batch_ts", "pf_batch_device", "pf_timers",
+           "pf_host_jacobian_pattern", "pf_host_schedule_solve")
+
+
+def load(path=None):
+    """Load the native library (raises if it is missing)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB
+    if not os.path.exists(p):
+        raise ImportError("lightsim2grid_b200: native library {} is missing; run "
+                          "`python -m lightsim2grid_b200.build`".format(p))
+    lib = ctypes.CDLL(p)
+    lib.pf_last_error.restype = ctypes.c_char_p
+    lib.pf_last_error.argtypes = []
+    lib.pf_plan_create.restype = ctypes.c_int
+    lib.pf_plan_create.argtypes = [ctypes.c_int, i32p, i32p, f64p, f64p, f64p, i32p, ctypes.c_int, f64p, i32p,
+                                   ctypes.c_int, i32p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PfOptions),
+                                   ctypes.POINTER(ctypes.c_void_p)]
+    lib.pf_plan_destroy.restype = None
+    lib.pf_plan_destroy.argtypes = [ctypes.c_void_p]
+    lib.pf_plan_info_get.restype = ctypes.c_int
+    lib.pf_plan_info_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfPlanInfo)]
+    lib.pf_set_ybus_values.restype = ctypes.c_int
+    lib.pf_set_ybus_values.argtypes = [ctypes.c_void_p, f64p]
+    lib.pf_solve.restype = ctypes.c_int
+    lib.pf_solve.argtypes = [ctypes.c_void_p, f64p, f64p, ctypes.c_int, ctypes.c_double, f64p, i32p, i32p, i32p]
+    lib.pf_get_J.restype = ctypes.c_int
+    lib.pf_get_J.argtypes = [ctypes.c_void_p, i32p, i32p, i32p, f64p]
+    lib.pf_batch_n1.restype = ctypes.c_int
+    lib.pf_batch_n1.argtypes = [ctypes.c_void_p, ctypes.c_int, i32p, i32p, i32p, f64p, f64p, f64p, ctypes.c_int,
+                                ctypes.c_double, f64p, i32p, i32p, i32p]
+    lib.pf_n1_prepare.restype = ctypes.c_int
+    lib.pf_n1_prepare.argtypes = [ctypes.c_void_p, ctypes.c_int, i32p, i32p, i32p, f64p, i32p, i32p, i32p, f64p,
+                                  ctypes.c_int]
+    lib.pf_batch_ts.restype = ctypes.c_int
+    lib.pf_batch_ts.argtypes = [ctypes.c_void_p, ctypes.c_int, f64p, f64p, ctypes.c_int, ctypes.c_int,
+                                ctypes.c_double, f64p, i32p, i32p, i32p, i32p]
+    lib.pf_batch_device.restype = ctypes.c_int
+    lib.pf_batch_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfDeviceBatch), ctypes.c_void_p]
+    lib.pf_timers.restype = ctypes.c_int
+    lib.pf_timers.argtypes = [ctypes.c_void_p, f64p, ctypes.c_int]
+    lib.pf_host_jacobian_pattern.restype = ctypes.c_int
+    lib.pf_host_jacobian_pattern.argtypes = [ctypes.c_int, i32p, i32p, f64p, i32p, ctypes.c_int, f64p, i32p,
+                                             ctypes.c_int, i32p, ctypes.c_int, ctypes.c_int, i32p, i32p, i32p]
+    lib.pf_host_schedule_solve.restype = ctypes.c_int
+    lib.pf_host_schedule_solve.argtypes = [ctypes.c_int, i32p, i32p, f64p, f64p, f64p, i32p, ctypes.c_int, f64p,
+                                           i32p, ctypes.c_int, i32p, ctypes.c_int, ctypes.c_int, f64p, f64p,
+                                           ctypes.POINTER(PfPlanInfo)]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def last_error(lib=None):
+    lib = lib or load()
+    msg = lib.pf_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(rc, what, lib=None):
+    if rc != 0:
+        raise RuntimeError("{} failed (status {}): {}".format(what, rc, last_error(lib)))
+
+
+def as_i32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32).ravel())
+
+
+def as_c128(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.complex128))
+
+
+def as_f64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+
+
+def ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+def cptr(a):
+    """Pointer to a complex128 array as interleaved doubles."""
+    return a.view(np.float64).ctypes.data_as(f64p)

@@ -1,0 +1,944 @@
+// C ABI of the engine: plan lifetime, device upload, batch orchestration.
+#include "../../include/lightsim2grid_b200.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pf_engine.cuh"
+#include "pf_plan.hpp"
+
+using l2g::cplx;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+    g_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return -2;
+}
+
+double now() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct pf_plan {
+    l2g::Plan P;
+    pf_options opt{};
+    int device = 0;
+    int num_sms = 0;
+    int precision = 0;
+    int threads = 256;
+    bool lu_in_smem = false;
+    int ctas_per_sm = 1;
+    int grid = 1;
+    size_t slab = 0, smem = 0;
+    // device structure
+    void *d_int = nullptr;
+    void *d_dbl = nullptr;
+    l2g::DevPlan dp{};
+    // device work buffers
+    DevBuf scratch, counter, V0, Sbus, optr, opos, oval, jfirst, jcount, Vout, iters, errs, Jout;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // host state
+    std::vector<double> lastJ;
+    bool haveJ = false;
+    double timers[6] = {0, 0, 0, 0, 0, 0};
+    // islanding: undirected graph of off-diagonal entries with |y| > 1e-8 and its bridges
+    std::vector<char> is_bridge_csr;  // per CSR position
+    bool base_connected = false;
+    bool graph_symmetric = true;
+};
+
+namespace {
+
+// ------------------------------------------------------------------ islanding check
+// Reference: ContingencyAnalysis::check_invertible (ContingencyAnalysis.cpp:14-45), a BFS from
+// bus 0 that follows entries Y(r, c) with |y| > 1e-8 from column c to row r.
+bool bfs_connected(const l2g::Plan &P, const std::vector<int> &opos, const std::vector<cplx> &oval) {
+    const int n = P.n;
+    std::vector<char> seen(n, 0);
+    std::vector<int> queue;
+    queue.reserve(n);
+    // CSC traversal with overrides (positions are CSR; map through csr_of_csc)
+    auto value_at_csc = [&](int p) {
+        int d = P.csr_of_csc[p];
+        for (size_t i = 0; i < opos.size(); ++i)
+            if (opos[i] == d) return oval[i];
+        return P.Rx[d];
+    };
+    seen[0] = 1;
+    queue.push_back(0);
+    for (size_t h = 0; h < queue.size(); ++h) {
+        int c = queue[h];
+        for (int p = P.Yp[c]; p < P.Yp[c + 1]; ++p) {
+            int r = P.Yi[p];
+            if (seen[r]) continue;
+            if (std::abs(value_at_csc(p)) > 1e-8) {
+                seen[r] = 1;
+                queue.push_back(r);
+            }
+        }
+    }
+    return (int)queue.size() == n;
+}
+
+void compute_bridges(pf_plan *pl) {
+    const l2g::Plan &P = pl->P;
+    const int n = P.n;
+    pl->is_bridge_csr.assign(P.nnzY, 0);
+    // symmetric strong-entry graph?
+    pl->graph_symmetric = true;
+    std::vector<std::vector<std::pair<int, int>>> adj(n);  // (neighbour, CSR position of (r=u, c=v))
+    for (int r = 0; r < n; ++r)
+        for (int d = P.Rp[r]; d < P.Rp[r + 1]; ++d) {
+            int c = P.Rj[d];
+            if (c == r) continue;
+            bool strong = std::abs(P.Rx[d]) > 1e-8;
+            // transposed entry
+            int dt = -1;
+            for (int e = P.Rp[c]; e < P.Rp[c + 1]; ++e)
+                if (P.Rj[e] == r) { dt = e; break; }
+            bool strong_t = dt >= 0 && std::abs(P.Rx[dt]) > 1e-8;
+            if (strong != strong_t) pl->graph_symmetric = false;
+            if (strong && r < c) {
+                adj[r].push_back({c, d});
+                adj[c].push_back({r, d});
+            }
+        }
+    std::vector<int> none, ops;
+    std::vector<cplx> ovs;
+    pl->base_connected = bfs_connected(P, ops, ovs);
+    // Tarjan's bridge finding (iterative)
+    std::vector<int> disc(n, -1), low(n, 0), parent_edge(n, -1), it(n, 0);
+    int timer = 0;
+    for (int s = 0; s < n; ++s) {
+        if (disc[s] >= 0) continue;
+        std::vector<int> st{s};
+        disc[s] = low[s] = timer++;
+        while (!st.empty()) {
+            int u = st.back();
+            if (it[u] < (int)adj[u].size()) {
+                auto [v, d] = adj[u][it[u]++];
+                if (d == parent_edge[u]) continue;
+                if (disc[v] < 0) {
+                    parent_edge[v] = d;
+                    disc[v] = low[v] = timer++;
+                    st.push_back(v);
+                } else {
+                    low[u] = std::min(low[u], disc[v]);
+                }
+            } else {
+                st.pop_back();
+                if (!st.empty()) {
+                    int p = st.back();
+                    low[p] = std::min(low[p], low[u]);
+                    if (low[u] > disc[p]) pl->is_bridge_csr[parent_edge[u]] = 1;
+                }
+            }
+        }
+    }
+}
+
+int csr_find(const l2g::Plan &P, int r, int c) {
+    if (r < 0 || r >= P.n || c < 0 || c >= P.n) return -1;
+    const int *b = P.Rj.data() + P.Rp[r], *e = P.Rj.data() + P.Rp[r + 1];
+    const int *f = std::lower_bound(b, e, c);
+    if (f == e || *f != c) return -1;
+    return (int)(f - P.Rj.data());
+}
+
+// overrides of one case; returns 0, or -1 if a coefficient is outside the pattern
+int case_overrides(const l2g::Plan &P, int k0, int k1, const int *row, const int *col, const cplx *val,
+                   std::vector<int> &opos, std::vector<cplx> &oval) {
+    opos.clear();
+    oval.clear();
+    for (int k = k0; k < k1; ++k) {
+        int d = csr_find(P, row[k], col[k]);
+        if (d < 0) return -1;
+        size_t i = 0;
+        for (; i < opos.size(); ++i)
+            if (opos[i] == d) break;
+        if (i == opos.size()) {
+            opos.push_back(d);
+            oval.push_back(P.Rx[d]);
+        }
+        oval[i] -= val[k];
+    }
+    return 0;
+}
+
+bool case_connected(pf_plan *pl, const std::vector<int> &opos, const std::vector<cplx> &oval) {
+    const l2g::Plan &P = pl->P;
+    if (!pl->base_connected) return false;
+    // edges of the strong graph turned off / on by this case
+    int removed = 0, removed_pos = -1;
+    bool added = false;
+    for (size_t i = 0; i < opos.size(); ++i) {
+        int d = opos[i];
+        int r = P.Rrow[d], c = P.Rj[d];
+        if (r == c) continue;
+        bool before = std::abs(P.Rx[d]) > 1e-8, after = std::abs(oval[i]) > 1e-8;
+        if (before && !after) {
+            ++removed;
+            if (r < c) removed_pos = d;
+        }
+        if (!before && after) added = true;
+    }
+    if (removed == 0 && !added) return true;
+    if (pl->graph_symmetric && !added && removed == 2 && removed_pos >= 0) {
+        // one undirected edge gone (both directions): connected unless it is a bridge
+        int r = P.Rrow[removed_pos], c = P.Rj[removed_pos];
+        bool other_gone = false;
+        for (size_t i = 0; i < opos.size(); ++i)
+            if (P.Rrow[opos[i]] == c && P.Rj[opos[i]] == r && !(std::abs(oval[i]) > 1e-8)) other_gone = true;
+        if (other_gone) return !pl->is_bridge_csr[removed_pos];
+    }
+    return bfs_connected(P, opos, oval);
+}
+
+// ------------------------------------------------------------------ device upload
+template <typename T>
+size_t push(std::vector<unsigned char> &blob, const std::vector<T> &v) {
+    size_t off = (blob.size() + 15) & ~(size_t)15;
+    blob.resize(off + v.size() * sizeof(T));
+    if (!v.empty()) std::memcpy(blob.data() + off, v.data(), v.size() * sizeof(T));
+    return off;
+}
+
+std::vector<int> flat_groups(const std::vector<l2g::LevelGroup> &g) {
+    std::vector<int> out;
+    for (auto &x : g) {
+        out.push_back(x.begin);
+        out.push_back(x.end);
+        out.push_back(x.kind);
+        out.push_back(x.lanes);
+    }
+    return out;
+}
+
+int upload(pf_plan *pl) {
+    const l2g::Plan &P = pl->P;
+    std::vector<unsigned char> bi, bd;
+    size_t oRp = push(bi, P.Rp), oRj = push(bi, P.Rj), oRrow = push(bi, P.Rrow);
+    size_t oyt = push(bi, P.ytarget), oyj = push(bi, P.yjpos);
+    size_t ofill = push(bi, P.fillpos), ocpos = push(bi, P.cpos), ocj = push(bi, P.cjpos);
+    size_t oxP = push(bi, P.xP), oxQ = push(bi, P.xQ), oxVa = push(bi, P.xVa), oxVm = push(bi, P.xVm);
+    size_t oup = push(bi, P.upd_ptr), ouc = push(bi, P.upd_c), ouu = push(bi, P.upd_upos), oud = push(bi, P.upd_dst);
+    size_t odst = push(bi, P.dst), odpos = push(bi, P.dpos), ols = push(bi, P.lstart), olc = push(bi, P.lcount);
+    size_t oro = push(bi, P.ref_order), org = push(bi, flat_groups(P.ref_groups));
+    size_t olp = push(bi, P.lrow_ptr), olcol = push(bi, P.lrow_col), olpos = push(bi, P.lrow_pos);
+    size_t oup2 = push(bi, P.urow_ptr), oucol = push(bi, P.urow_col), oupos = push(bi, P.urow_pos);
+    size_t ofo = push(bi, P.fwd_order), obo = push(bi, P.bwd_order);
+    size_t ofg = push(bi, flat_groups(P.fwd_groups)), obg = push(bi, flat_groups(P.bwd_groups));
+    std::vector<double> rx(2 * (size_t)P.nnzY);
+    for (int i = 0; i < P.nnzY; ++i) {
+        rx[2 * i] = P.Rx[i].real();
+        rx[2 * i + 1] = P.Rx[i].imag();
+    }
+    size_t oRx = push(bd, rx), ow = push(bd, P.weights), ocv = push(bd, P.cval);
+    if (pl->d_int) cudaFree(pl->d_int);
+    if (pl->d_dbl) cudaFree(pl->d_dbl);
+    pl->d_int = pl->d_dbl = nullptr;
+    cudaError_t e = cudaMalloc(&pl->d_int, std::max<size_t>(bi.size(), 16));
+    if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: cudaMalloc");
+    e = cudaMalloc(&pl->d_dbl, std::max<size_t>(bd.size(), 16));
+    if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: cudaMalloc");
+    e = cudaMemcpy(pl->d_int, bi.data(), bi.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: upload");
+    e = cudaMemcpy(pl->d_dbl, bd.data(), bd.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: upload");
+    auto I = [&](size_t o) { return reinterpret_cast<const int *>(static_cast<unsigned char *>(pl->d_int) + o); };
+    auto I4 = [&](size_t o) { return reinterpret_cast<const int4 *>(static_cast<unsigned char *>(pl->d_int) + o); };
+    auto D = [&](size_t o) { return reinterpret_cast<const double *>(static_cast<unsigned char *>(pl->d_dbl) + o); };
+    l2g::DevPlan &d = pl->dp;
+    d.n = P.n;
+    d.m = P.m;
+    d.nnzY = P.nnzY;
+    d.nnzLU = P.nnzLU;
+    d.distributed = P.distributed ? 1 : 0;
+    d.Rp = I(oRp);
+    d.Rj = I(oRj);
+    d.Rrow = I(oRrow);
+    d.Rx = reinterpret_cast<const double2 *>(D(oRx));
+    d.w = D(ow);
+    d.ytarget = I4(oyt);
+    d.yjpos = I4(oyj);
+    d.fillpos = I(ofill);
+    d.nfill = (int)P.fillpos.size();
+    d.cpos = I(ocpos);
+    d.cjpos = I(ocj);
+    d.cval = D(ocv);
+    d.nconst = (int)P.cpos.size();
+    d.xP = I(oxP);
+    d.xQ = I(oxQ);
+    d.xVa = I(oxVa);
+    d.xVm = I(oxVm);
+    d.xSlack = P.xSlack;
+    d.upd_ptr = I(oup);
+    d.upd_c = I(ouc);
+    d.upd_upos = I(ouu);
+    d.upd_dst = I(oud);
+    d.dst = I(odst);
+    d.dpos = I(odpos);
+    d.lstart = I(ols);
+    d.lcount = I(olc);
+    d.ref_order = I(oro);
+    d.ref_groups = I4(org);
+    d.nref = (int)P.ref_groups.size();
+    d.lrow_ptr = I(olp);
+    d.lrow_col = I(olcol);
+    d.lrow_pos = I(olpos);
+    d.urow_ptr = I(oup2);
+    d.urow_col = I(oucol);
+    d.urow_pos = I(oupos);
+    d.fwd_order = I(ofo);
+    d.bwd_order = I(obo);
+    d.fwd_groups = I4(ofg);
+    d.bwd_groups = I4(obg);
+    d.nfwd = (int)P.fwd_groups.size();
+    d.nbwd = (int)P.bwd_groups.size();
+    return 0;
+}
+
+int configure(pf_plan *pl) {
+    const l2g::Plan &P = pl->P;
+    cudaError_t e = cudaGetDevice(&pl->device);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: no CUDA device");
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, pl->device);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: cudaGetDeviceProperties");
+    pl->num_sms = prop.multiProcessorCount;
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, pl->device);
+    pl->precision = pl->opt.precision ? 1 : 0;
+    int thr = pl->opt.threads;
+    if (thr <= 0) thr = P.m > 2000 ? 512 : (P.m > 300 ? 256 : 128);
+    thr = std::max(32, std::min(512, (thr / 32) * 32));
+    pl->threads = thr;
+    const int lub = pl->precision ? 4 : 8, xb = pl->precision ? 4 : 8;
+    const size_t static_smem = 2048;  // Shared struct of the kernel, rounded up
+    size_t sm_in = l2g::smem_bytes(pl->dp, lub, xb, true);
+    size_t sm_out = l2g::smem_bytes(pl->dp, lub, xb, false);
+    bool fits = sm_in + static_smem <= (size_t)optin;
+    if (pl->opt.lu_placement == 1 && !fits) return fail(-1, "pf_plan_create: LU does not fit in shared memory");
+    if (sm_out + static_smem > (size_t)optin)
+        return fail(-1, "pf_plan_create: the solve vector does not fit in shared memory");
+    pl->lu_in_smem = pl->opt.lu_placement == 2 ? false : fits;
+    pl->smem = pl->lu_in_smem ? sm_in : sm_out;
+    pl->slab = l2g::slab_bytes(pl->dp, lub, pl->lu_in_smem);
+    int occ = l2g::nr_occupancy(pl->precision, thr, pl->smem);
+    if (occ <= 0) return fail(-1, "pf_plan_create: the kernel cannot be launched with this configuration");
+    if (pl->opt.max_ctas_per_sm > 0) occ = std::min(occ, pl->opt.max_ctas_per_sm);
+    pl->ctas_per_sm = occ;
+    pl->grid = pl->num_sms * occ;
+    e = pl->scratch.ensure(pl->slab * (size_t)pl->grid);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: scratch allocation");
+    e = pl->counter.ensure(256);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: counter allocation");
+    return 0;
+}
+
+void release(pf_plan *pl) {
+    for (DevBuf *b : {&pl->scratch, &pl->counter, &pl->V0, &pl->Sbus, &pl->optr, &pl->opos, &pl->oval,
+                      &pl->jfirst, &pl->jcount, &pl->Vout, &pl->iters, &pl->errs, &pl->Jout})
+        b->release();
+    if (pl->d_int) cudaFree(pl->d_int);
+    if (pl->d_dbl) cudaFree(pl->d_dbl);
+    pl->d_int = pl->d_dbl = nullptr;
+    if (pl->ev0) cudaEventDestroy(pl->ev0);
+    if (pl->ev1) cudaEventDestroy(pl->ev1);
+    if (pl->stream) cudaStreamDestroy(pl->stream);
+    pl->ev0 = pl->ev1 = nullptr;
+    pl->stream = nullptr;
+}
+
+// launches the kernel for a batch whose device buffers are set up in `a` (no sync)
+int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
+    a.scratch = static_cast<unsigned char *>(pl->scratch.p);
+    a.slab_bytes = (long long)pl->slab;
+    a.job_counter = static_cast<int *>(pl->counter.p);
+    a.lu_in_smem = pl->lu_in_smem ? 1 : 0;
+    if (a.njobs <= 0) return 0;
+    cudaError_t e = cudaMemsetAsync(pl->counter.p, 0, sizeof(int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
+    int grid = std::min(pl->grid, a.njobs);
+    // the FP64 re-run of a mixed plan uses the FP64 kernel with this plan's layout:
+    // LU bytes differ, so recompute shared memory and slab use for that precision
+    size_t smem = pl->smem;
+    int lub = precision ? 4 : 8;
+    if (precision != pl->precision) {
+        bool in = pl->lu_in_smem;
+        size_t need = l2g::smem_bytes(pl->dp, lub, lub, in);
+        size_t slab = l2g::slab_bytes(pl->dp, lub, in);
+        int optin = 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, pl->device);
+        if (in && need + 2048 > (size_t)optin) {
+            in = false;
+            need = l2g::smem_bytes(pl->dp, lub, lub, false);
+            slab = l2g::slab_bytes(pl->dp, lub, false);
+        }
+        if (slab > pl->slab) {
+            // FP64 needs a larger slab than the plan reserved: fewer CTAs
+            grid = std::max(1, std::min(grid, (int)((pl->slab * (size_t)pl->grid) / slab)));
+        }
+        a.slab_bytes = (long long)slab;
+        a.lu_in_smem = in ? 1 : 0;
+        smem = need;
+        int occ = l2g::nr_occupancy(precision, pl->threads, smem);
+        if (occ <= 0) return fail(-1, "launch: FP64 re-run configuration cannot launch");
+        grid = std::min(grid, pl->num_sms * occ);
+    }
+    e = l2g::launch_nr_batch(pl->dp, a, precision, pl->threads, grid, smem, st);
+    if (e != cudaSuccess) return cuda_fail(e, "launch: kernel");
+    return 0;
+}
+
+template <typename T>
+cudaError_t h2d(DevBuf &b, const T *src, size_t count, cudaStream_t st) {
+    cudaError_t e = b.ensure(count * sizeof(T));
+    if (e != cudaSuccess || count == 0) return e;
+    return cudaMemcpyAsync(b.p, src, count * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+// runs instances [0, n_inst) described by host arrays; results into host arrays.
+// V0: shared (v0_stride 0) or per instance; Sbus likewise.
+int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, const cplx *Sbus, long long sbus_stride,
+              const std::vector<int> &optr, const std::vector<int> &opos, const std::vector<cplx> &oval,
+              const std::vector<int> &jfirst, const std::vector<int> &jcount, int chain, int max_iter, double tol,
+              cplx *Vout, int *iters, int *errs, bool want_J) {
+    const int n = pl->P.n;
+    cudaStream_t st = pl->stream;
+    double t0 = now();
+    cudaError_t e;
+    size_t nv0 = v0_stride ? (size_t)n_inst * n : (size_t)n;
+    size_t nsb = sbus_stride ? (size_t)n_inst * n : (size_t)n;
+    if ((e = h2d(pl->V0, V0, nv0, st)) != cudaSuccess) return cuda_fail(e, "batch: V0 upload");
+    if ((e = h2d(pl->Sbus, Sbus, nsb, st)) != cudaSuccess) return cuda_fail(e, "batch: Sbus upload");
+    bool have_ovr = !optr.empty();
+    if (have_ovr) {
+        if ((e = h2d(pl->optr, optr.data(), optr.size(), st)) != cudaSuccess) return cuda_fail(e, "batch: upload");
+        if ((e = h2d(pl->opos, opos.data(), opos.size(), st)) != cudaSuccess) return cuda_fail(e, "batch: upload");
+        if ((e = h2d(pl->oval, oval.data(), oval.size(), st)) != cudaSuccess) return cuda_fail(e, "batch: upload");
+    }
+    if ((e = h2d(pl->jfirst, jfirst.data(), jfirst.size(), st)) != cudaSuccess) return cuda_fail(e, "batch: upload");
+    if ((e = h2d(pl->jcount, jcount.data(), jcount.size(), st)) != cudaSuccess) return cuda_fail(e, "batch: upload");
+    if ((e = pl->Vout.ensure((size_t)n_inst * n * sizeof(cplx))) != cudaSuccess) return cuda_fail(e, "batch: alloc");
+    if ((e = pl->iters.ensure((size_t)n_inst * sizeof(int))) != cudaSuccess) return cuda_fail(e, "batch: alloc");
+    if ((e = pl->errs.ensure((size_t)n_inst * sizeof(int))) != cudaSuccess) return cuda_fail(e, "batch: alloc");
+    if (want_J && (e = pl->Jout.ensure(pl->P.Ji.size() * sizeof(double))) != cudaSuccess)
+        return cuda_fail(e, "batch: alloc");
+    double t1 = now();
+    l2g::BatchArgs a{};
+    a.n_inst = n_inst;
+    a.V0 = static_cast<const double2 *>(pl->V0.p);
+    a.v0_stride = v0_stride;
+    a.Sbus = static_cast<const double2 *>(pl->Sbus.p);
+    a.sbus_stride = sbus_stride;
+    a.ovr_ptr = have_ovr ? static_cast<const int *>(pl->optr.p) : nullptr;
+    a.ovr_pos = have_ovr ? static_cast<const int *>(pl->opos.p) : nullptr;
+    a.ovr_val = have_ovr ? static_cast<const double2 *>(pl->oval.p) : nullptr;
+    a.max_iter = max_iter;
+    a.tol = tol;
+    a.job_first = static_cast<const int *>(pl->jfirst.p);
+    a.job_count = static_cast<const int *>(pl->jcount.p);
+    a.njobs = (int)jfirst.size();
+    a.chain = chain;
+    a.Vout = static_cast<double2 *>(pl->Vout.p);
+    a.iters = static_cast<int *>(pl->iters.p);
+    a.errs = static_cast<int *>(pl->errs.p);
+    a.Jout = want_J ? static_cast<double *>(pl->Jout.p) : nullptr;
+    a.j_inst = 0;
+    cudaEventRecord(pl->ev0, st);
+    int rc = launch(pl, a, pl->precision, st);
+    if (rc) return rc;
+    cudaEventRecord(pl->ev1, st);
+    if ((e = cudaMemcpyAsync(iters, pl->iters.p, (size_t)n_inst * sizeof(int), cudaMemcpyDeviceToHost, st)) !=
+        cudaSuccess)
+        return cuda_fail(e, "batch: download");
+    if ((e = cudaMemcpyAsync(errs, pl->errs.p, (size_t)n_inst * sizeof(int), cudaMemcpyDeviceToHost, st)) !=
+        cudaSuccess)
+        return cuda_fail(e, "batch: download");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "batch: kernel execution");
+    float kms = 0.f;
+    cudaEventElapsedTime(&kms, pl->ev0, pl->ev1);
+    double kernel_s = kms * 1e-3;
+    // mixed form: re-run in FP64 the jobs that contain a failure
+    int rerun = 0;
+    if (pl->precision == 1 && pl->opt.fp64_fallback != 2) {
+        std::vector<int> rf, rc2;
+        for (size_t j = 0; j < jfirst.size(); ++j) {
+            bool bad = false;
+            for (int s = 0; s < jcount[j]; ++s)
+                if (errs[jfirst[j] + s] != 0) bad = true;
+            if (bad) {
+                rf.push_back(jfirst[j]);
+                rc2.push_back(jcount[j]);
+                rerun += jcount[j];
+            }
+        }
+        if (!rf.empty()) {
+            if ((e = h2d(pl->jfirst, rf.data(), rf.size(), st)) != cudaSuccess) return cuda_fail(e, "rerun: upload");
+            if ((e = h2d(pl->jcount, rc2.data(), rc2.size(), st)) != cudaSuccess) return cuda_fail(e, "rerun: upload");
+            a.job_first = static_cast<const int *>(pl->jfirst.p);
+            a.job_count = static_cast<const int *>(pl->jcount.p);
+            a.njobs = (int)rf.size();
+            cudaEventRecord(pl->ev0, st);
+            rc = launch(pl, a, 0, st);
+            if (rc) return rc;
+            cudaEventRecord(pl->ev1, st);
+            if ((e = cudaMemcpyAsync(iters, pl->iters.p, (size_t)n_inst * sizeof(int), cudaMemcpyDeviceToHost,
+                                     st)) != cudaSuccess)
+                return cuda_fail(e, "rerun: download");
+            if ((e = cudaMemcpyAsync(errs, pl->errs.p, (size_t)n_inst * sizeof(int), cudaMemcpyDeviceToHost, st)) !=
+                cudaSuccess)
+                return cuda_fail(e, "rerun: download");
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "rerun: kernel execution");
+            cudaEventElapsedTime(&kms, pl->ev0, pl->ev1);
+            kernel_s += kms * 1e-3;
+        }
+    }
+    double t2 = now();
+    if ((e = cudaMemcpyAsync(Vout, pl->Vout.p, (size_t)n_inst * n * sizeof(cplx), cudaMemcpyDeviceToHost, st)) !=
+        cudaSuccess)
+        return cuda_fail(e, "batch: download");
+    if (want_J) {
+        pl->lastJ.resize(pl->P.Ji.size());
+        if ((e = cudaMemcpyAsync(pl->lastJ.data(), pl->Jout.p, pl->lastJ.size() * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return cuda_fail(e, "batch: download");
+    }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "batch: download");
+    double t3 = now();
+    pl->timers[2] = t1 - t0;
+    pl->timers[3] = kernel_s;
+    pl->timers[4] = t3 - t2;
+    pl->timers[5] = rerun;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pf_last_error(void) { return g_err.c_str(); }
+
+int pf_plan_create(int n, const int *colptr, const int *rowind, const double *ybus_ri, const double *V0_ri,
+                   const double *Sbus_ri, const int *slack_ids, int nslack, const double *slack_weights,
+                   const int *pv, int npv, const int *pq, int npq, int distributed, const pf_options *opts,
+                   pf_plan **out) {
+    if (!out || !colptr || !rowind || !ybus_ri || !V0_ri || !Sbus_ri || !slack_ids || !slack_weights ||
+        (npv && !pv) || (npq && !pq))
+        return fail(-1, "pf_plan_create: null argument");
+    *out = nullptr;
+    pf_plan *pl = new pf_plan();
+    if (opts) pl->opt = *opts;
+    l2g::PlanOptions po;
+    if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
+    if (pl->opt.chain_max_items > 0) po.chain_max_items = pl->opt.chain_max_items;
+    std::string msg;
+    int rc;
+    try {
+        rc = l2g::build_plan(pl->P, n, colptr, rowind, reinterpret_cast<const cplx *>(ybus_ri),
+                             reinterpret_cast<const cplx *>(V0_ri), reinterpret_cast<const cplx *>(Sbus_ri),
+                             slack_ids, nslack, slack_weights, pv, npv, pq, npq, distributed != 0, po, msg);
+    } catch (const std::exception &ex) {
+        rc = -1;
+        msg = std::string("pf_plan_create: ") + ex.what();
+    }
+    if (rc != 0) {
+        delete pl;
+        return fail(rc, msg);
+    }
+    compute_bridges(pl);
+    cudaError_t e = cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete pl;
+        return cuda_fail(e, "pf_plan_create: stream");
+    }
+    cudaEventCreate(&pl->ev0);
+    cudaEventCreate(&pl->ev1);
+    rc = upload(pl);
+    if (!rc) rc = configure(pl);
+    if (rc) {
+        std::string keep = g_err;
+        release(pl);
+        delete pl;
+        g_err = keep;
+        return rc;
+    }
+    *out = pl;
+    return 0;
+}
+
+void pf_plan_destroy(pf_plan *plan) {
+    if (!plan) return;
+    release(plan);
+    delete plan;
+}
+
+int pf_plan_info_get(const pf_plan *pl, pf_plan_info *info) {
+    if (!pl || !info) return fail(-1, "pf_plan_info_get: null argument");
+    const l2g::Plan &P = pl->P;
+    info->n = P.n;
+    info->m = P.m;
+    info->nnz_ybus = P.nnzY;
+    info->nnz_j = (int)P.Ji.size();
+    info->nnz_lu = P.nnzLU;
+    info->levels_refactor = P.levels_refactor;
+    info->levels_forward = P.levels_fwd;
+    info->levels_backward = P.levels_bwd;
+    info->groups_refactor = (int)P.ref_groups.size();
+    info->groups_forward = (int)P.fwd_groups.size();
+    info->groups_backward = (int)P.bwd_groups.size();
+    info->flops_refactor = P.flops_refactor;
+    info->precision = pl->precision;
+    info->threads = pl->threads;
+    info->lu_in_shared = pl->lu_in_smem ? 1 : 0;
+    info->ctas_per_sm = pl->ctas_per_sm;
+    info->grid = pl->grid;
+    info->slab_bytes = (long long)pl->slab;
+    info->shared_bytes = (long long)pl->smem;
+    return 0;
+}
+
+int pf_set_ybus_values(pf_plan *pl, const double *ybus_ri) {
+    if (!pl || !ybus_ri) return fail(-1, "pf_set_ybus_values: null argument");
+    l2g::Plan &P = pl->P;
+    const cplx *y = reinterpret_cast<const cplx *>(ybus_ri);
+    for (int p = 0; p < P.nnzY; ++p) {
+        P.Yx[p] = y[p];
+        P.Rx[P.csr_of_csc[p]] = y[p];
+    }
+    std::vector<double> rx(2 * (size_t)P.nnzY);
+    for (int i = 0; i < P.nnzY; ++i) {
+        rx[2 * i] = P.Rx[i].real();
+        rx[2 * i + 1] = P.Rx[i].imag();
+    }
+    cudaError_t e = cudaMemcpy(const_cast<double2 *>(pl->dp.Rx), rx.data(), rx.size() * sizeof(double),
+                               cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_set_ybus_values");
+    compute_bridges(pl);
+    return 0;
+}
+
+int pf_solve(pf_plan *pl, const double *V0_ri, const double *Sbus_ri, int max_iter, double tol, double *V_out_ri,
+             int *converged, int *iters, int *err) {
+    if (!pl || !V0_ri || !Sbus_ri || !V_out_ri) return fail(-1, "pf_solve: null argument");
+    double t0 = now();
+    std::vector<int> empty, jf{0}, jc{1};
+    std::vector<cplx> ev;
+    int it = 0, er = 0;
+    int rc = run_batch(pl, 1, reinterpret_cast<const cplx *>(V0_ri), 0, reinterpret_cast<const cplx *>(Sbus_ri), 0,
+                       empty, empty, ev, jf, jc, 0, max_iter, tol, reinterpret_cast<cplx *>(V_out_ri), &it, &er,
+                       true);
+    if (rc) return rc;
+    pl->haveJ = it > 0;
+    if (iters) *iters = it;
+    if (err) *err = er;
+    if (converged) *converged = er == 0;
+    pl->timers[0] = now() - t0;
+    pl->timers[1] = 0.0;
+    return 0;
+}
+
+int pf_get_J(pf_plan *pl, int *m, int *Jp, int *Ji, double *Jx) {
+    if (!pl) return fail(-1, "pf_get_J: null argument");
+    const l2g::Plan &P = pl->P;
+    if (m) *m = P.m;
+    if (Jp) std::memcpy(Jp, P.Jp.data(), P.Jp.size() * sizeof(int));
+    if (Ji) std::memcpy(Ji, P.Ji.data(), P.Ji.size() * sizeof(int));
+    if (Jx) {
+        if (!pl->haveJ) return fail(-1, "pf_get_J: no iteration has been run yet");
+        std::memcpy(Jx, pl->lastJ.data(), pl->lastJ.size() * sizeof(double));
+    }
+    return (int)P.Ji.size();
+}
+
+int pf_n1_prepare(pf_plan *pl, int ncases, const int *case_ptr, const int *coef_row, const int *coef_col,
+                  const double *coef_val_ri, int *solvable, int *ovr_ptr, int *ovr_pos, double *ovr_val_ri, int cap) {
+    if (!pl || ncases < 0 || !case_ptr || !solvable || !ovr_ptr) return fail(-1, "pf_n1_prepare: null argument");
+    const cplx *cv = reinterpret_cast<const cplx *>(coef_val_ri);
+    std::vector<int> opos;
+    std::vector<cplx> oval;
+    int w = 0, ns = 0;
+    ovr_ptr[0] = 0;
+    for (int c = 0; c < ncases; ++c) {
+        if (case_overrides(pl->P, case_ptr[c], case_ptr[c + 1], coef_row, coef_col, cv, opos, oval) != 0)
+            return fail(-1, "pf_n1_prepare: case " + std::to_string(c) +
+                                " removes a coefficient that is not in the Ybus pattern");
+        if ((int)opos.size() > l2g::kMaxOverrides)
+            return fail(-1, "pf_n1_prepare: case " + std::to_string(c) + " changes more than 32 Ybus entries");
+        solvable[c] = case_connected(pl, opos, oval) ? 1 : 0;
+        if (!solvable[c]) continue;
+        if (w + (int)opos.size() > cap) return -3;
+        for (size_t i = 0; i < opos.size(); ++i) {
+            if (ovr_pos) ovr_pos[w] = opos[i];
+            if (ovr_val_ri) {
+                ovr_val_ri[2 * w] = oval[i].real();
+                ovr_val_ri[2 * w + 1] = oval[i].imag();
+            }
+            ++w;
+        }
+        ++ns;
+        ovr_ptr[ns] = w;
+    }
+    return w;
+}
+
+int pf_batch_n1(pf_plan *pl, int ncases, const int *case_ptr, const int *coef_row, const int *coef_col,
+                const double *coef_val_ri, const double *V0_ri, const double *Sbus_ri, int max_iter, double tol,
+                double *V_out_ri, int *converged, int *iters, int *errs) {
+    if (!pl || ncases < 0 || !case_ptr || !V0_ri || !Sbus_ri || !V_out_ri || !converged || !iters || !errs)
+        return fail(-1, "pf_batch_n1: null argument");
+    double t0 = now();
+    const int n = pl->P.n;
+    std::vector<int> solv(ncases), optr(ncases + 1);
+    int total = case_ptr[ncases] - case_ptr[0];
+    std::vector<int> opos(std::max(total, 1));
+    std::vector<cplx> oval(std::max(total, 1));
+    int w = pf_n1_prepare(pl, ncases, case_ptr, coef_row, coef_col, coef_val_ri, solv.data(), optr.data(),
+                          opos.data(), reinterpret_cast<double *>(oval.data()), (int)opos.size());
+    if (w < 0) return w == -3 ? fail(-1, "pf_batch_n1: internal override buffer too small") : w;
+    std::vector<int> idx;
+    for (int c = 0; c < ncases; ++c)
+        if (solv[c]) idx.push_back(c);
+    const int ns = (int)idx.size();
+    optr.resize(ns + 1);
+    opos.resize(std::max(w, 1));
+    oval.resize(std::max(w, 1));
+    std::vector<int> jf(ns), jc(ns, 1);
+    for (int i = 0; i < ns; ++i) jf[i] = i;
+    std::vector<cplx> vout((size_t)std::max(ns, 1) * n);
+    std::vector<int> it(std::max(ns, 1)), er(std::max(ns, 1));
+    double t1 = now();
+    if (ns > 0) {
+        int rc = run_batch(pl, ns, reinterpret_cast<const cplx *>(V0_ri), 0, reinterpret_cast<const cplx *>(Sbus_ri),
+                           0, optr, opos, oval, jf, jc, 0, max_iter, tol, vout.data(), it.data(), er.data(), false);
+        if (rc) return rc;
+    }
+    cplx *Vo = reinterpret_cast<cplx *>(V_out_ri);
+    std::fill(Vo, Vo + (size_t)ncases * n, cplx(0.0, 0.0));
+    for (int c = 0; c < ncases; ++c) {
+        converged[c] = 0;
+        iters[c] = 0;
+        errs[c] = 1;  // SingularMatrix: islanded, not computed
+    }
+    for (int i = 0; i < ns; ++i) {
+        int c = idx[i];
+        iters[c] = it[i];
+        errs[c] = er[i];
+        converged[c] = er[i] == 0;
+        if (er[i] == 0) std::memcpy(Vo + (size_t)c * n, vout.data() + (size_t)i * n, sizeof(cplx) * n);
+    }
+    pl->timers[0] = now() - t0;
+    pl->timers[1] = t1 - t0;
+    return 0;
+}
+
+int pf_batch_ts(pf_plan *pl, int nsteps, const double *Sbus_ri, const double *V0_ri, int nchunks, int max_iter,
+                double tol, double *V_out_ri, int *converged, int *iters, int *errs, int *status) {
+    if (!pl || nsteps < 0 || !Sbus_ri || !V0_ri || !V_out_ri || !converged || !iters || !errs)
+        return fail(-1, "pf_batch_ts: null argument");
+    double t0 = now();
+    const int n = pl->P.n;
+    if (nchunks <= 0) nchunks = pl->grid;
+    nchunks = std::max(1, std::min(nchunks, std::max(nsteps, 1)));
+    std::vector<int> jf, jc;
+    for (int c = 0; c < nchunks; ++c) {
+        int a = (int)((long long)nsteps * c / nchunks), b = (int)((long long)nsteps * (c + 1) / nchunks);
+        if (b > a) {
+            jf.push_back(a);
+            jc.push_back(b - a);
+        }
+    }
+    std::vector<int> empty;
+    std::vector<cplx> ev;
+    int rc = 0;
+    if (nsteps > 0)
+        rc = run_batch(pl, nsteps, reinterpret_cast<const cplx *>(V0_ri), 0, reinterpret_cast<const cplx *>(Sbus_ri), n,
+                       empty, empty, ev, jf, jc, 1, max_iter, tol, reinterpret_cast<cplx *>(V_out_ri), iters, errs,
+                       false);
+    if (rc) return rc;
+    int first_bad = nsteps;
+    for (int s = 0; s < nsteps; ++s)
+        if (errs[s] != 0) {
+            first_bad = s;
+            break;
+        }
+    cplx *Vo = reinterpret_cast<cplx *>(V_out_ri);
+    for (int s = 0; s < nsteps; ++s) {
+        converged[s] = s < first_bad;
+        if (s >= first_bad) {
+            std::fill(Vo + (size_t)s * n, Vo + (size_t)(s + 1) * n, cplx(0.0, 0.0));
+            if (s > first_bad) {
+                iters[s] = 0;
+                errs[s] = 8;
+            }
+        }
+    }
+    if (status) *status = first_bad == nsteps ? 1 : 0;
+    pl->timers[0] = now() - t0;
+    pl->timers[1] = 0.0;
+    return 0;
+}
+
+int pf_batch_device(pf_plan *pl, const pf_device_batch *b, void *stream) {
+    if (!pl || !b) return fail(-1, "pf_batch_device: null argument");
+    l2g::BatchArgs a{};
+    a.n_inst = b->n_inst;
+    a.V0 = static_cast<const double2 *>(b->V0);
+    a.v0_stride = b->v0_stride;
+    a.Sbus = static_cast<const double2 *>(b->Sbus);
+    a.sbus_stride = b->sbus_stride;
+    a.ovr_ptr = b->ovr_ptr;
+    a.ovr_pos = b->ovr_pos;
+    a.ovr_val = static_cast<const double2 *>(b->ovr_val);
+    a.max_iter = b->max_iter;
+    a.tol = b->tol;
+    a.job_first = b->job_first;
+    a.job_count = b->job_count;
+    a.njobs = b->njobs;
+    a.chain = b->chain;
+    a.Vout = static_cast<double2 *>(b->Vout);
+    a.iters = b->iters;
+    a.errs = b->errs;
+    a.Jout = nullptr;
+    a.j_inst = -1;
+    return launch(pl, a, pl->precision, static_cast<cudaStream_t>(stream));
+}
+
+int pf_timers(const pf_plan *pl, double *out, int nout) {
+    if (!pl || !out) return fail(-1, "pf_timers: null argument");
+    for (int i = 0; i < nout && i < 6; ++i) out[i] = pl->timers[i];
+    return 0;
+}
+
+int pf_host_jacobian_pattern(int n, const int *colptr, const int *rowind, const double *ybus_ri,
+                             const int *slack_ids, int nslack, const double *slack_weights, const int *pv, int npv,
+                             const int *pq, int npq, int distributed, int *m, int *Jp, int *Ji) {
+    if (!colptr || !rowind || !ybus_ri || !slack_ids || !slack_weights) return fail(-1, "null argument");
+    l2g::Plan P;
+    l2g::PlanOptions po;
+    std::string msg;
+    std::vector<cplx> V0(n, cplx(1.0, 0.0)), S(n, cplx(0.0, 0.0));
+    int rc = l2g::build_plan(P, n, colptr, rowind, reinterpret_cast<const cplx *>(ybus_ri), V0.data(), S.data(),
+                             slack_ids, nslack, slack_weights, pv, npv, pq, npq, distributed != 0, po, msg);
+    // a flat start may give a singular first Jacobian; the pattern is still valid then
+    if (rc != 0 && P.Jp.empty()) return fail(rc, msg);
+    if (m) *m = P.m;
+    if (Jp) std::memcpy(Jp, P.Jp.data(), P.Jp.size() * sizeof(int));
+    if (Ji) std::memcpy(Ji, P.Ji.data(), P.Ji.size() * sizeof(int));
+    return (int)P.Ji.size();
+}
+
+int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const double *ybus_ri, const double *V0_ri,
+                           const double *V_ri, const int *slack_ids, int nslack, const double *slack_weights,
+                           const int *pv, int npv, const int *pq, int npq, int distributed, const double *b,
+                           double *x, pf_plan_info *info) {
+    if (!colptr || !rowind || !ybus_ri || !V0_ri || !V_ri || !b || !x) return fail(-1, "null argument");
+    l2g::Plan P;
+    l2g::PlanOptions po;
+    std::string msg;
+    std::vector<cplx> S(n, cplx(0.0, 0.0));
+    int rc = l2g::build_plan(P, n, colptr, rowind, reinterpret_cast<const cplx *>(ybus_ri),
+                             reinterpret_cast<const cplx *>(V0_ri), S.data(), slack_ids, nslack, slack_weights, pv,
+                             npv, pq, npq, distributed != 0, po, msg);
+    if (rc != 0) return fail(rc, msg);
+    const int m = P.m;
+    std::vector<double> Jx;
+    l2g::host_jacobian(P, P.Yx.data(), reinterpret_cast<const cplx *>(V_ri), Jx);
+    // scatter J into the LU layout exactly as the device fill does
+    std::vector<double> lu(P.nnzLU, 0.0);
+    std::vector<char> seen(P.nnzLU, 0);
+    for (int d = 0; d < P.nnzY; ++d)
+        for (int k = 0; k < 4; ++k) {
+            int t = P.ytarget[4 * (size_t)d + k], j = P.yjpos[4 * (size_t)d + k];
+            if (t >= 0) { lu[t] = Jx[j]; seen[t] = 1; }
+        }
+    for (size_t i = 0; i < P.cpos.size(); ++i) { lu[P.cpos[i]] = P.cval[i]; seen[P.cpos[i]] = 1; }
+    for (int p : P.fillpos) { lu[p] = 0.0; seen[p] = 1; }
+    for (int p = 0; p < P.nnzLU; ++p)
+        if (!seen[p]) return fail(-1, "schedule check: an LU position is never written by the fill");
+    // refactorisation in group / level order
+    for (const auto &G : P.ref_groups)
+        for (int t = G.begin; t < G.end; ++t) {
+            int k = P.ref_order[t];
+            for (int u = P.upd_ptr[k]; u < P.upd_ptr[k + 1]; ++u) {
+                int c = P.upd_c[u];
+                double uv = lu[P.upd_upos[u]];
+                for (int s = 0; s < P.lcount[c]; ++s) lu[P.dst[P.upd_dst[u] + s]] -= lu[P.lstart[c] + s] * uv;
+            }
+            double piv = lu[P.dpos[k]];
+            if (piv == 0.0) return fail(l2g::SolverReFactor, "schedule check: zero pivot");
+            for (int s = 0; s < P.lcount[k]; ++s) lu[P.lstart[k] + s] /= piv;
+        }
+    // permuted right-hand side, as the device mismatch writes it
+    std::vector<double> xs(m, 0.0);
+    for (int f = 0; f < m; ++f) xs[P.pinv[f]] = b[f];
+    for (const auto &G : P.fwd_groups)
+        for (int t = G.begin; t < G.end; ++t) {
+            int i = P.fwd_order[t];
+            double s = 0.0;
+            for (int e = P.lrow_ptr[i]; e < P.lrow_ptr[i + 1]; ++e) s += lu[P.lrow_pos[e]] * xs[P.lrow_col[e]];
+            xs[i] -= s;
+        }
+    for (const auto &G : P.bwd_groups)
+        for (int t = G.begin; t < G.end; ++t) {
+            int i = P.bwd_order[t];
+            double s = 0.0;
+            for (int e = P.urow_ptr[i]; e < P.urow_ptr[i + 1]; ++e) s += lu[P.urow_pos[e]] * xs[P.urow_col[e]];
+            xs[i] = (xs[i] - s) / lu[P.dpos[i]];
+        }
+    for (int v = 0; v < m; ++v) x[v] = xs[P.qinv[v]];
+    if (info) {
+        std::memset(info, 0, sizeof(*info));
+        info->n = P.n;
+        info->m = P.m;
+        info->nnz_ybus = P.nnzY;
+        info->nnz_j = (int)P.Ji.size();
+        info->nnz_lu = P.nnzLU;
+        info->levels_refactor = P.levels_refactor;
+        info->levels_forward = P.levels_fwd;
+        info->levels_backward = P.levels_bwd;
+        info->groups_refactor = (int)P.ref_groups.size();
+        info->groups_forward = (int)P.fwd_groups.size();
+        info->groups_backward = (int)P.bwd_groups.size();
+        info->flops_refactor = P.flops_refactor;
+    }
+    return 0;
+}
+
+}  // extern "C"

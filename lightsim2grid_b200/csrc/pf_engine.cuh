@@ -1,0 +1,76 @@
+// Device-side data of the batched Newton-Raphson engine (shared by the kernels and the
+// host orchestration).  Plain pointers only: the structure arrays are uploaded once per
+// plan; the batch arrays are per call.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace l2g {
+
+// Structure arrays of one plan on the device (see pf_plan.hpp for their meaning).
+struct DevPlan {
+    int n, m, nnzY, nnzLU, distributed;
+    const int *Rp, *Rj, *Rrow;
+    const double2 *Rx;
+    const double *w;
+    const int4 *ytarget;   // 4 LU positions per CSR position
+    const int4 *yjpos;     // 4 J positions per CSR position
+    const int *fillpos;
+    int nfill;
+    const int *cpos, *cjpos;
+    const double *cval;
+    int nconst;
+    const int *xP, *xQ, *xVa, *xVm;
+    int xSlack;
+    const int *upd_ptr, *upd_c, *upd_upos, *upd_dst, *dst;
+    const int *dpos, *lstart, *lcount;
+    const int *ref_order;
+    const int4 *ref_groups;
+    int nref;
+    const int *lrow_ptr, *lrow_col, *lrow_pos, *urow_ptr, *urow_col, *urow_pos;
+    const int *fwd_order, *bwd_order;
+    const int4 *fwd_groups, *bwd_groups;
+    int nfwd, nbwd;
+};
+
+// One batch launch.
+struct BatchArgs {
+    int n_inst;
+    const double2 *V0;        // start voltages; instance i reads V0 + i * v0_stride
+    long long v0_stride;      // 0: one start point shared by all instances
+    const double2 *Sbus;      // injections; instance i reads Sbus + i * sbus_stride
+    long long sbus_stride;
+    const int *ovr_ptr;       // per-instance Ybus overrides (CSR positions / new values), may be null
+    const int *ovr_pos;
+    const double2 *ovr_val;
+    int max_iter;
+    double tol;
+    const int *job_first;     // jobs: instances [job_first[j], job_first[j] + job_count[j])
+    const int *job_count;
+    int njobs;
+    int chain;                // 1: an instance starts from the previous instance's solution
+    int *job_counter;         // zero before the launch
+    double2 *Vout;            // n per instance
+    int *iters;
+    int *errs;
+    double *Jout;             // J values (CSC order) of the last iteration of instance j_inst
+    int j_inst;
+    unsigned char *scratch;   // per-CTA slab
+    long long slab_bytes;
+    int lu_in_smem;
+};
+
+constexpr int kMaxOverrides = 32;
+
+// Bytes of the per-CTA global slab and of the dynamic shared memory.
+size_t slab_bytes(const DevPlan &P, int lu_bytes, bool lu_in_smem);
+size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem);
+
+// precision: 0 = FP64 LU and solves, 1 = FP32 LU and solves (FP64 mismatch and update).
+cudaError_t launch_nr_batch(const DevPlan &P, const BatchArgs &A, int precision, int threads, int grid,
+                            size_t smem, cudaStream_t stream);
+// Resident CTAs per SM for a configuration (0 if it cannot launch).
+int nr_occupancy(int precision, int threads, size_t smem);
+
+}  // namespace l2g

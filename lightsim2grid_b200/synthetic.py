@@ -1,0 +1,200 @@
+"""Seeded synthetic transmission grids.
+
+There is no public grid data in this project: every benchmark grid is generated from a
+seed.  Topology: ``n`` buses at uniform random points of the unit square; a random
+spanning tree over the graph of each bus's 8 nearest neighbours (Kruskal on random edge
+weights); extra branches drawn from the remaining nearest-neighbour pairs, short ones
+first (length times U[0.5, 1.5]).  Real transmission grids are near-planar graphs of
+short lines, which this reproduces; chords drawn uniformly at random instead make an
+expander graph whose LU fill is 5-200 times larger than any real grid's.
+
+Electrical data (per unit, ``sn_mva`` = 1): ``r ~ U[0.01, 0.08]``, ``x ~ U[0.04, 0.25]``,
+line charging ``b ~ U[0, 0.05]`` (``h = j b``, split half / half).  Bus 0 is the slack;
+``n_pv`` other buses carry a voltage-regulating generator with ``|V| ~ U[0.98, 1.06]``
+(the slack too).  Injections are consistent with a drawn true state: ``|V| ~ U[0.95,
+1.05]`` at PQ buses, angles ``~ N(0, 0.05)`` rad (slack angle 0), and
+``S = V * conj(Ybus V)``; generators take ``Re S`` at PV / slack buses and one load per
+PQ bus takes ``-S``.  The magnitudes and angles keep those marginal distributions but
+are spatially correlated: each is a standard-normal field smoothed over 16 hops of the
+branch graph, mapped through the normal CDF for the uniform marginals (generator
+set-points use the same field).  Independent per-bus draws put several per-unit of
+reactive power on single short lines, and Newton-Raphson from a flat start then
+diverges on every grid above ~300 buses.
+"""
+import numpy as np
+
+from .gridmodel import GridModel
+
+#: The grids used by the benchmarks and tests: name -> (buses, branches, PV buses).
+GRID_SIZES = {
+    "grid14": (14, 20, 4),
+    "grid118": (118, 186, 54),
+    "grid300": (300, 405, 60),
+    "grid1354": (1354, 1991, 260),
+    "grid2848": (2848, 3776, 500),
+    "grid6515": (6515, 8796, 1100),
+}
+
+
+#: Seeds of the named grids (each one's base case converges from a flat start).
+NAMED_SEEDS = {"grid14": 14, "grid118": 118, "grid300": 300, "grid1354": 1354, "grid2848": 2848,
+               "grid6515": 6516}
+
+
+def _knn_pairs(pts, k):
+    n = pts.shape[0]
+    k = min(k, n - 1)
+    # blocked brute-force k-nearest neighbours (n <= ~10k)
+    pairs = set()
+    blk = 512
+    for s in range(0, n, blk):
+        d = ((pts[s:s + blk, None, :] - pts[None, :, :]) ** 2).sum(-1)
+        for t in range(d.shape[0]):
+            d[t, s + t] = np.inf
+        idx = np.argpartition(d, k - 1, axis=1)[:, :k]
+        for t in range(d.shape[0]):
+            i = s + t
+            for j in idx[t]:
+                j = int(j)
+                pairs.add((i, j) if i < j else (j, i))
+    return sorted(pairs)
+
+
+def _find(parent, x):
+    while parent[x] != x:
+        parent[x] = parent[parent[x]]
+        x = parent[x]
+    return x
+
+
+def _normal_cdf(z):
+    from math import erf, sqrt
+    return np.array([0.5 * (1.0 + erf(v / sqrt(2.0))) for v in z])
+
+
+def _graph_field(n, f, t, rng, n_smooth):
+    """Standard-normal marginals, correlated along branches.
+
+    White noise is averaged ``n_smooth`` times with the mean of each bus's neighbours
+    (a lazy random walk on the branch graph), then standardised.
+    """
+    z = rng.normal(0.0, 1.0, n)
+    deg = np.bincount(f, minlength=n) + np.bincount(t, minlength=n)
+    for _ in range(n_smooth):
+        acc = np.zeros(n)
+        np.add.at(acc, f, z[t])
+        np.add.at(acc, t, z[f])
+        z = 0.5 * z + 0.5 * acc / np.maximum(deg, 1)
+    z = z - z.mean()
+    sd = z.std()
+    return z / sd if sd > 0 else z
+
+
+def make_grid(n_bus, n_branch, n_pv, seed=0, knn=8, smooth=16):
+    """Build one seeded synthetic grid; returns ``(GridModel, V_true)``."""
+    if n_branch < n_bus - 1:
+        raise ValueError("a connected grid needs at least n_bus - 1 branches")
+    rng = np.random.default_rng(seed)
+    pts = rng.random((n_bus, 2))
+    cand = _knn_pairs(pts, knn)
+    w = rng.random(len(cand))
+    order = np.argsort(w, kind="stable")
+    parent = list(range(n_bus))
+    tree, rest = [], []
+    for o in order:
+        a, b = cand[o]
+        ra, rb = _find(parent, a), _find(parent, b)
+        if ra != rb:
+            parent[ra] = rb
+            tree.append((a, b))
+        else:
+            rest.append((a, b))
+    # join components the nearest-neighbour graph left apart (rare)
+    while len(tree) < n_bus - 1:
+        roots = {}
+        for i in range(n_bus):
+            roots.setdefault(_find(parent, i), []).append(i)
+        comps = list(roots.values())
+        a_set, others = comps[0], [i for c in comps[1:] for i in c]
+        d = ((pts[a_set][:, None, :] - pts[others][None, :, :]) ** 2).sum(-1)
+        ia, ib = np.unravel_index(np.argmin(d), d.shape)
+        a, b = a_set[ia], others[ib]
+        parent[_find(parent, a)] = _find(parent, b)
+        tree.append((min(a, b), max(a, b)))
+    n_extra = n_branch - (n_bus - 1)
+    if n_extra > len(rest):
+        raise ValueError("not enough nearest-neighbour pairs for {} extra branches".format(n_extra))
+    length = np.array([np.hypot(*(pts[a] - pts[b])) for (a, b) in rest])
+    key = length * rng.uniform(0.5, 1.5, size=len(rest))
+    extra = [rest[i] for i in np.argsort(key, kind="stable")[:n_extra]]
+    edges = tree + extra
+    perm = rng.permutation(len(edges))
+    edges = [edges[i] for i in perm]
+    f = np.array([e[0] for e in edges], dtype=np.int64)
+    t = np.array([e[1] for e in edges], dtype=np.int64)
+    nb = len(edges)
+    r = rng.uniform(0.01, 0.08, nb)
+    x = rng.uniform(0.04, 0.25, nb)
+    b = rng.uniform(0.0, 0.05, nb)
+
+    g = GridModel(n_bus, sn_mva=1.0, init_vm_pu=1.0)
+    g.init_powerlines(r, x, 1j * b, f, t)
+
+    slack = 0
+    pv = rng.choice(np.arange(1, n_bus), size=n_pv, replace=False)
+    z_vm = _graph_field(n_bus, f, t, rng, smooth)
+    z_va = _graph_field(n_bus, f, t, rng, smooth)
+    u_vm = _normal_cdf(z_vm)
+    vm = 0.95 + 0.10 * u_vm
+    gen_bus = np.concatenate([[slack], pv])
+    vset = 0.98 + 0.08 * u_vm[gen_bus]
+    vm[gen_bus] = vset
+    va = 0.05 * (z_va - z_va[slack])
+    V = vm * np.exp(1j * va)
+    Y = g.get_Ybus()
+    S = V * np.conj(Y @ V)
+
+    gen_p = S[gen_bus].real.copy()
+    sw = np.zeros(gen_bus.size)
+    sw[0] = 1.0
+    g.init_generators(gen_p, vset, gen_bus, sw)
+    is_gen = np.zeros(n_bus, dtype=bool)
+    is_gen[gen_bus] = True
+    load_bus = np.nonzero(~is_gen)[0]
+    g.init_loads(-S[load_bus].real, -S[load_bus].imag, load_bus)
+    return g, V
+
+
+def make_named_grid(name, seed=None):
+    n, nbr, npv = GRID_SIZES[name]
+    if seed is None:
+        # default seed = bus count, except grid6515 whose seed 6515 draws a case that
+        # Newton-Raphson cannot solve from a flat start; 6516 is the next seed that it can.
+        seed = NAMED_SEEDS[name]
+    return make_grid(n, nbr, npv, seed=seed)
+
+
+def ar1_profiles(n_steps, n_series, seed=0, phi=0.9, sigma=0.03, daily=0.15, steps_per_day=24):
+    """Per-series AR(1) multipliers times a shared daily sinusoid: ``(n_steps, n_series)``.
+
+    ``m[t, s] = (1 + e[t, s]) * (1 + daily * sin(2 pi t / steps_per_day))`` with
+    ``e[t] = phi e[t-1] + N(0, sigma^2)``.
+    """
+    rng = np.random.default_rng(seed)
+    e = np.zeros((n_steps, n_series))
+    eps = rng.normal(0.0, sigma, size=(n_steps, n_series))
+    for k in range(1, n_steps):
+        e[k] = phi * e[k - 1] + eps[k]
+    day = 1.0 + daily * np.sin(2.0 * np.pi * np.arange(n_steps) / steps_per_day)
+    return (1.0 + e) * day[:, None]
+
+
+def time_series_injections(grid, n_steps, seed=0):
+    """Gen / load injections for a time series on ``grid`` (AR(1) x daily sinusoid)."""
+    m_gen = ar1_profiles(n_steps, grid.gen_bus.size, seed=seed)
+    m_load = ar1_profiles(n_steps, grid.load_bus.size, seed=seed + 1)
+    gen_p = grid.gen_p_mw[None, :] * m_gen
+    load_p = grid.load_p_mw[None, :] * m_load
+    load_q = grid.load_q_mvar[None, :] * m_load
+    sgen_p = np.zeros((n_steps, 0))
+    return gen_p, sgen_p, load_p, load_q
