@@ -29,6 +29,8 @@ typedef struct pf_options {
     int fp64_fallback;      /* mixed form: re-run instances that did not converge in FP64.
                                0: default (on), 1: on, 2: off                                  */
     int max_ctas_per_sm;    /* cap on resident CTAs per SM; 0: occupancy limit               */
+    int refine;             /* mixed form: refine every Newton step once against the FP64
+                               Jacobian.  0: default (on), 1: on, 2: off                       */
 } pf_options;
 
 /* Sizes and schedule statistics of a plan. */

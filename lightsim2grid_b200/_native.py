@@ -19,7 +19,7 @@ f64p = ctypes.POINTER(ctypes.c_double)
 class PfOptions(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("threads", ctypes.c_int), ("lu_placement", ctypes.c_int),
                 ("chain_max_items", ctypes.c_int), ("pivot_threshold", ctypes.c_double),
-                ("fp64_fallback", ctypes.c_int), ("max_ctas_per_sm", ctypes.c_int)]
+                ("fp64_fallback", ctypes.c_int), ("max_ctas_per_sm", ctypes.c_int), ("refine", ctypes.c_int)]
 
 
 class PfPlanInfo(ctypes.Structure):

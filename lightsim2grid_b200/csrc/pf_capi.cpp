@@ -61,6 +61,7 @@ struct pf_plan {
     int precision = 0;
     int threads = 256;
     bool lu_in_smem = false;
+    bool refine = false;
     int ctas_per_sm = 1;
     int grid = 1;
     size_t slab = 0, smem = 0;
@@ -249,6 +250,28 @@ std::vector<int> flat_groups(const std::vector<l2g::LevelGroup> &g) {
     return out;
 }
 
+std::vector<int> pack_rows(const std::vector<int> &order, const std::vector<int> &rptr, const std::vector<int> &dpos,
+                           bool with_diag) {
+    std::vector<int> out;
+    out.reserve(order.size() * 4);
+    for (int i : order) {
+        out.push_back(i);
+        out.push_back(rptr[i]);
+        out.push_back(rptr[i + 1] - rptr[i]);
+        out.push_back(with_diag ? dpos[i] : 0);
+    }
+    return out;
+}
+
+std::vector<int> pack_pairs(const std::vector<int> &a, const std::vector<int> &b) {
+    std::vector<int> out(2 * a.size());
+    for (size_t i = 0; i < a.size(); ++i) {
+        out[2 * i] = a[i];
+        out[2 * i + 1] = b[i];
+    }
+    return out;
+}
+
 int upload(pf_plan *pl) {
     const l2g::Plan &P = pl->P;
     std::vector<unsigned char> bi, bd;
@@ -256,19 +279,42 @@ int upload(pf_plan *pl) {
     size_t oyt = push(bi, P.ytarget), oyj = push(bi, P.yjpos);
     size_t ofill = push(bi, P.fillpos), ocpos = push(bi, P.cpos), ocj = push(bi, P.cjpos);
     size_t oxP = push(bi, P.xP), oxQ = push(bi, P.xQ), oxVa = push(bi, P.xVa), oxVm = push(bi, P.xVm);
-    size_t oup = push(bi, P.upd_ptr), ouc = push(bi, P.upd_c), ouu = push(bi, P.upd_upos), oud = push(bi, P.upd_dst);
-    size_t odst = push(bi, P.dst), odpos = push(bi, P.dpos), ols = push(bi, P.lstart), olc = push(bi, P.lcount);
-    size_t oro = push(bi, P.ref_order), org = push(bi, flat_groups(P.ref_groups));
-    size_t olp = push(bi, P.lrow_ptr), olcol = push(bi, P.lrow_col), olpos = push(bi, P.lrow_pos);
-    size_t oup2 = push(bi, P.urow_ptr), oucol = push(bi, P.urow_col), oupos = push(bi, P.urow_pos);
-    size_t ofo = push(bi, P.fwd_order), obo = push(bi, P.bwd_order);
+    std::vector<int> grp(4 * P.grp_lstart.size());
+    for (size_t g = 0; g < P.grp_lstart.size(); ++g) {
+        grp[4 * g] = P.grp_lstart[g];
+        grp[4 * g + 1] = P.grp_upos[g];
+        grp[4 * g + 2] = P.grp_dpos[g];
+        grp[4 * g + 3] = P.grp_dst[g];
+    }
+    std::vector<int> ph(4 * P.phases.size()), phl(P.phases.size());
+    for (size_t i = 0; i < P.phases.size(); ++i) {
+        ph[4 * i] = P.phases[i].gbeg;
+        ph[4 * i + 1] = P.phases[i].gend;
+        ph[4 * i + 2] = P.phases[i].dbeg;
+        ph[4 * i + 3] = P.phases[i].dend;
+        phl[i] = P.phases[i].lanes;
+    }
+    size_t ogrp = push(bi, grp), oglc = push(bi, P.grp_lcount), odst = push(bi, P.dst);
+    size_t oph = push(bi, ph), ophl = push(bi, phl), odiv = push(bi, pack_pairs(P.div_pos, P.div_dpos));
+    size_t odpos = push(bi, P.dpos);
+    size_t ofd = push(bi, pack_rows(P.fwd_order, P.lrow_ptr, P.dpos, false));
+    size_t obd = push(bi, pack_rows(P.bwd_order, P.urow_ptr, P.dpos, true));
+    size_t olpc = push(bi, pack_pairs(P.lrow_pos, P.lrow_col)), oupc = push(bi, pack_pairs(P.urow_pos, P.urow_col));
     size_t ofg = push(bi, flat_groups(P.fwd_groups)), obg = push(bi, flat_groups(P.bwd_groups));
     std::vector<double> rx(2 * (size_t)P.nnzY);
     for (int i = 0; i < P.nnzY; ++i) {
         rx[2 * i] = P.Rx[i].real();
         rx[2 * i + 1] = P.Rx[i].imag();
     }
-    size_t oRx = push(bd, rx), ow = push(bd, P.weights), ocv = push(bd, P.cval);
+    // J(P(r), 0) of the distributed-slack Jacobian (BaseNRAlgo.tpp:542-552)
+    std::vector<double> wJ(P.n, 0.0);
+    if (P.distributed)
+        for (int r = 0; r < P.n; ++r) {
+            if (P.xP[r] < 0) continue;
+            if (r == P.slack0) wJ[r] = P.weights[r];
+            else if (std::fabs(P.weights[r]) > 1e-7) wJ[r] = P.weights[r];
+        }
+    size_t oRx = push(bd, rx), ow = push(bd, P.weights), ocv = push(bd, P.cval), owJ = push(bd, wJ);
     if (pl->d_int) cudaFree(pl->d_int);
     if (pl->d_dbl) cudaFree(pl->d_dbl);
     pl->d_int = pl->d_dbl = nullptr;
@@ -280,9 +326,11 @@ int upload(pf_plan *pl) {
     if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: upload");
     e = cudaMemcpy(pl->d_dbl, bd.data(), bd.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: upload");
-    auto I = [&](size_t o) { return reinterpret_cast<const int *>(static_cast<unsigned char *>(pl->d_int) + o); };
-    auto I4 = [&](size_t o) { return reinterpret_cast<const int4 *>(static_cast<unsigned char *>(pl->d_int) + o); };
-    auto D = [&](size_t o) { return reinterpret_cast<const double *>(static_cast<unsigned char *>(pl->d_dbl) + o); };
+    unsigned char *bI = static_cast<unsigned char *>(pl->d_int), *bD = static_cast<unsigned char *>(pl->d_dbl);
+    auto I = [&](size_t o) { return reinterpret_cast<const int *>(bI + o); };
+    auto I2 = [&](size_t o) { return reinterpret_cast<const int2 *>(bI + o); };
+    auto I4 = [&](size_t o) { return reinterpret_cast<const int4 *>(bI + o); };
+    auto D = [&](size_t o) { return reinterpret_cast<const double *>(bD + o); };
     l2g::DevPlan &d = pl->dp;
     d.n = P.n;
     d.m = P.m;
@@ -307,25 +355,19 @@ int upload(pf_plan *pl) {
     d.xVa = I(oxVa);
     d.xVm = I(oxVm);
     d.xSlack = P.xSlack;
-    d.upd_ptr = I(oup);
-    d.upd_c = I(ouc);
-    d.upd_upos = I(ouu);
-    d.upd_dst = I(oud);
+    d.wJ = D(owJ);
+    d.grp = I4(ogrp);
+    d.grp_lc = I(oglc);
     d.dst = I(odst);
+    d.phases = I4(oph);
+    d.ph_lanes = I(ophl);
+    d.nphases = (int)P.phases.size();
+    d.divs = I2(odiv);
     d.dpos = I(odpos);
-    d.lstart = I(ols);
-    d.lcount = I(olc);
-    d.ref_order = I(oro);
-    d.ref_groups = I4(org);
-    d.nref = (int)P.ref_groups.size();
-    d.lrow_ptr = I(olp);
-    d.lrow_col = I(olcol);
-    d.lrow_pos = I(olpos);
-    d.urow_ptr = I(oup2);
-    d.urow_col = I(oucol);
-    d.urow_pos = I(oupos);
-    d.fwd_order = I(ofo);
-    d.bwd_order = I(obo);
+    d.fwd_desc = I4(ofd);
+    d.bwd_desc = I4(obd);
+    d.lrow_pc = I2(olpc);
+    d.urow_pc = I2(oupc);
     d.fwd_groups = I4(ofg);
     d.bwd_groups = I4(obg);
     d.nfwd = (int)P.fwd_groups.size();
@@ -359,7 +401,8 @@ int configure(pf_plan *pl) {
     pl->lu_in_smem = pl->opt.lu_placement == 2 ? false : fits;
     pl->smem = pl->lu_in_smem ? sm_in : sm_out;
     pl->slab = l2g::slab_bytes(pl->dp, lub, pl->lu_in_smem);
-    int occ = l2g::nr_occupancy(pl->precision, thr, pl->smem);
+    pl->refine = pl->precision == 1 && pl->opt.refine != 2;
+    int occ = l2g::nr_occupancy(pl->precision, pl->lu_in_smem, pl->refine, thr, pl->smem);
     if (occ <= 0) return fail(-1, "pf_plan_create: the kernel cannot be launched with this configuration");
     if (pl->opt.max_ctas_per_sm > 0) occ = std::min(occ, pl->opt.max_ctas_per_sm);
     pl->ctas_per_sm = occ;
@@ -391,6 +434,7 @@ int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
     a.slab_bytes = (long long)pl->slab;
     a.job_counter = static_cast<int *>(pl->counter.p);
     a.lu_in_smem = pl->lu_in_smem ? 1 : 0;
+    a.refine = (precision == 1 && pl->refine) ? 1 : 0;
     if (a.njobs <= 0) return 0;
     cudaError_t e = cudaMemsetAsync(pl->counter.p, 0, sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
@@ -417,7 +461,7 @@ int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
         a.slab_bytes = (long long)slab;
         a.lu_in_smem = in ? 1 : 0;
         smem = need;
-        int occ = l2g::nr_occupancy(precision, pl->threads, smem);
+        int occ = l2g::nr_occupancy(precision, in, false, pl->threads, smem);
         if (occ <= 0) return fail(-1, "launch: FP64 re-run configuration cannot launch");
         grid = std::min(grid, pl->num_sms * occ);
     }
@@ -620,7 +664,7 @@ int pf_plan_info_get(const pf_plan *pl, pf_plan_info *info) {
     info->levels_refactor = P.levels_refactor;
     info->levels_forward = P.levels_fwd;
     info->levels_backward = P.levels_bwd;
-    info->groups_refactor = (int)P.ref_groups.size();
+    info->groups_refactor = (int)P.phases.size();
     info->groups_forward = (int)P.fwd_groups.size();
     info->groups_backward = (int)P.bwd_groups.size();
     info->flops_refactor = P.flops_refactor;
@@ -892,19 +936,17 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
     for (int p : P.fillpos) { lu[p] = 0.0; seen[p] = 1; }
     for (int p = 0; p < P.nnzLU; ++p)
         if (!seen[p]) return fail(-1, "schedule check: an LU position is never written by the fill");
-    // refactorisation in group / level order
-    for (const auto &G : P.ref_groups)
-        for (int t = G.begin; t < G.end; ++t) {
-            int k = P.ref_order[t];
-            for (int u = P.upd_ptr[k]; u < P.upd_ptr[k + 1]; ++u) {
-                int c = P.upd_c[u];
-                double uv = lu[P.upd_upos[u]];
-                for (int s = 0; s < P.lcount[c]; ++s) lu[P.dst[P.upd_dst[u] + s]] -= lu[P.lstart[c] + s] * uv;
-            }
-            double piv = lu[P.dpos[k]];
-            if (piv == 0.0) return fail(l2g::SolverReFactor, "schedule check: zero pivot");
-            for (int s = 0; s < P.lcount[k]; ++s) lu[P.lstart[k] + s] /= piv;
+    // refactorisation in the device's phase order (each phase's work is order independent)
+    for (const auto &Q : P.phases) {
+        for (int e = Q.dbeg; e < Q.dend; ++e) lu[P.div_pos[e]] /= lu[P.div_dpos[e]];
+        for (int g = Q.gbeg; g < Q.gend; ++g) {
+            double f = lu[P.grp_upos[g]] / lu[P.grp_dpos[g]];
+            for (int s2 = 0; s2 < P.grp_lcount[g]; ++s2)
+                lu[P.dst[P.grp_dst[g] + s2]] -= lu[P.grp_lstart[g] + s2] * f;
         }
+    }
+    for (int k = 0; k < m; ++k)
+        if (lu[P.dpos[k]] == 0.0) return fail(l2g::SolverReFactor, "schedule check: zero pivot");
     // permuted right-hand side, as the device mismatch writes it
     std::vector<double> xs(m, 0.0);
     for (int f = 0; f < m; ++f) xs[P.pinv[f]] = b[f];
@@ -933,7 +975,7 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         info->levels_refactor = P.levels_refactor;
         info->levels_forward = P.levels_fwd;
         info->levels_backward = P.levels_bwd;
-        info->groups_refactor = (int)P.ref_groups.size();
+        info->groups_refactor = (int)P.phases.size();
         info->groups_forward = (int)P.fwd_groups.size();
         info->groups_backward = (int)P.bwd_groups.size();
         info->flops_refactor = P.flops_refactor;

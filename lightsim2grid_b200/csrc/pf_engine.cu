@@ -5,18 +5,18 @@
 //   mismatch   F = V .* conj(Ybus V) - Sbus (+ slack term)     BaseAlgo.cpp:30-118
 //   J fill     dS/dVm, dS/dVa scattered into the LU array      BaseNRAlgo.tpp:202-260,
 //                                                              BaseNRSingleSlackAlgo.tpp:449-490
-//   refactor   left-looking LU with the plan's fixed pivots    (KLUSolver.cpp:47-59 contract)
+//   refactor   LU with the plan's fixed pivots                 (KLUSolver.cpp:47-59 contract)
 //   solve      forward / backward substitution                 (KLUSolver.cpp:61-69 contract)
 //   update     Va, Vm, V and the convergence test              BaseNRSingleSlackAlgo.tpp:129-162,
 //                                                              BaseNRAlgo.tpp:136-167
-// The refactorisation assigns one warp per column of an elimination level (lanes over
-// the rows of each L column it applies); levels with few columns run as one chain on
-// warp 0 with warp barriers only.  Both triangular solves are row oriented and level
-// scheduled with 1..32 lanes per row.  LU values live in shared memory when they fit,
-// otherwise in the CTA's global slab (L2 resident).
+// Refactorisation: right-looking by elimination level; the update groups (pivot c, column j)
+// of a level are spread over the CTA's threads in conflict-free phases, one barrier per
+// phase, no atomics, so the result is deterministic.  Solves: row oriented and level
+// scheduled with 1..32 lanes per row; levels with one or two rows run as a chain on warp 0
+// with the next row's indices prefetched.  LU values live in shared memory when they fit,
+// else in the CTA's global slab (L2 resident).  The mixed form (FP32 LU) refines every
+// Newton step once against the FP64 Jacobian, computed on the fly from dS/dV.
 #include "pf_engine.cuh"
-
-#include <cstdio>
 
 namespace l2g {
 
@@ -43,11 +43,9 @@ struct Shared {
     int job;
     int piv_err;
     double slack_absorbed;
-    double bcast;
-    int ibcast;
 };
 
-// block-wide max of |F| and "all finite" flag; every thread receives the result
+// block-wide max of |F| and "any non-finite" flag; every thread receives the result
 __device__ __forceinline__ void block_norm(Shared &S, double lmax, int lbad, double &norm, int &bad) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int o = 16; o > 0; o >>= 1) {
@@ -99,11 +97,33 @@ __device__ __forceinline__ double2 ybus_value(const DevPlan &P, const Shared &S,
     return y;
 }
 
-// F at V: writes Ibus and the permuted right-hand side x; returns ||F||_inf and a
-// non-finite flag to every thread.
+// dS/dVa and dS/dVm of Ybus entry (r, c), as BaseNRAlgo::_dSbus_dV (BaseNRAlgo.tpp:228-257)
+__device__ __forceinline__ void dsbus(double2 y, double2 vr, double2 vc, bool diag, double2 ib, double &dvar,
+                                      double &dvai, double2 &dvm) {
+    const double ic = 1.0 / cabs2(vc);
+    const double2 vnc = make_double2(vc.x * ic, vc.y * ic);
+    double2 a = cmul(cconj(cmul(y, vnc)), vr);  // conj(Y * Vnorm_c) * V_r
+    double2 b = cmul(y, vc);                    // Y * V_c
+    if (diag) {
+        const double ir = 1.0 / cabs2(vr);
+        const double2 vnr = make_double2(vr.x * ir, vr.y * ir);
+        const double2 t = cmul(cconj(ib), vnr);
+        a.x += t.x;
+        a.y += t.y;
+        b.x -= ib.x;
+        b.y -= ib.y;
+    }
+    dvar = b.x * vr.y - b.y * vr.x;  // conj(-b) * (j V_r)
+    dvai = -(b.x * vr.x + b.y * vr.y);
+    dvm = a;
+}
+
+// F at V: writes Ibus, the FP64 mismatch per bus and the permuted right-hand side x;
+// returns ||F||_inf and a non-finite flag to every thread.
 template <typename XT>
 __device__ void mismatch(const DevPlan &P, Shared &S, const double2 *__restrict__ V, double2 *__restrict__ Ibus,
-                         const double2 *__restrict__ Sbus, XT *x, double &norm, int &bad) {
+                         double2 *__restrict__ Fbus, const double2 *__restrict__ Sbus, XT *x, double &norm,
+                         int &bad) {
     double lmax = 0.0;
     int lbad = 0;
     const double sa = S.slack_absorbed;
@@ -111,17 +131,18 @@ __device__ void mismatch(const DevPlan &P, Shared &S, const double2 *__restrict_
         double2 s = make_double2(0.0, 0.0);
         const int p1 = P.Rp[r + 1];
         for (int p = P.Rp[r]; p < p1; ++p) {
-            double2 y = ybus_value(P, S, p);
-            double2 v = V[P.Rj[p]];
+            const double2 y = ybus_value(P, S, p);
+            const double2 v = V[P.Rj[p]];
             s.x += y.x * v.x - y.y * v.y;
             s.y += y.x * v.y + y.y * v.x;
         }
         Ibus[r] = s;
-        double2 vr = V[r];
-        double2 sb = Sbus[r];
+        const double2 vr = V[r];
+        const double2 sb = Sbus[r];
         double mr = vr.x * s.x + vr.y * s.y - sb.x;  // V * conj(I) - S
-        double mi = vr.y * s.x - vr.x * s.y - sb.y;
+        const double mi = vr.y * s.x - vr.x * s.y - sb.y;
         if (P.distributed) mr += sa * P.w[r];
+        Fbus[r] = make_double2(mr, mi);
         const int ip = P.xP[r], iq = P.xQ[r];
         if (ip >= 0) {
             x[ip] = (XT)mr;
@@ -143,36 +164,20 @@ __device__ void jacobian_fill(const DevPlan &P, Shared &S, const double2 *__rest
                               const double2 *__restrict__ Ibus, LT *lu, double *Jout) {
     for (int p = threadIdx.x; p < P.nnzY; p += blockDim.x) {
         const int r = P.Rrow[p], c = P.Rj[p];
-        const double2 y = ybus_value(P, S, p);
-        const double2 vr = V[r], vc = V[c];
-        const double ic = 1.0 / cabs2(vc);
-        const double2 vnc = make_double2(vc.x * ic, vc.y * ic);
-        double2 a = cmul(cconj(cmul(y, vnc)), vr);  // conj(Y * Vnorm_c) * V_r
-        double2 b = cmul(y, vc);                    // Y * V_c
-        if (r == c) {
-            const double2 ib = Ibus[r];
-            const double ir = 1.0 / cabs2(vr);
-            const double2 vnr = make_double2(vr.x * ir, vr.y * ir);
-            const double2 t = cmul(cconj(ib), vnr);
-            a.x += t.x;
-            a.y += t.y;
-            b.x -= ib.x;
-            b.y -= ib.y;
-        }
-        // dS/dVa = conj(-b) * (j V_r)
-        const double dvar = b.x * vr.y - b.y * vr.x;
-        const double dvai = -(b.x * vr.x + b.y * vr.y);
+        double dvar, dvai;
+        double2 dvm;
+        dsbus(ybus_value(P, S, p), V[r], V[c], r == c, r == c ? Ibus[r] : make_double2(0.0, 0.0), dvar, dvai, dvm);
         const int4 t = P.ytarget[p];
         if (t.x >= 0) lu[t.x] = (LT)dvar;
         if (t.y >= 0) lu[t.y] = (LT)dvai;
-        if (t.z >= 0) lu[t.z] = (LT)a.x;
-        if (t.w >= 0) lu[t.w] = (LT)a.y;
+        if (t.z >= 0) lu[t.z] = (LT)dvm.x;
+        if (t.w >= 0) lu[t.w] = (LT)dvm.y;
         if (Jout) {
             const int4 j = P.yjpos[p];
             if (j.x >= 0) Jout[j.x] = dvar;
             if (j.y >= 0) Jout[j.y] = dvai;
-            if (j.z >= 0) Jout[j.z] = a.x;
-            if (j.w >= 0) Jout[j.w] = a.y;
+            if (j.z >= 0) Jout[j.z] = dvm.x;
+            if (j.w >= 0) Jout[j.w] = dvm.y;
         }
     }
     for (int i = threadIdx.x; i < P.nfill; i += blockDim.x) lu[P.fillpos[i]] = (LT)0;
@@ -182,54 +187,43 @@ __device__ void jacobian_fill(const DevPlan &P, Shared &S, const double2 *__rest
     }
 }
 
-// one column of the left-looking factorisation, by one warp
-template <typename LT>
-__device__ __forceinline__ void factor_column(const DevPlan &P, Shared &S, LT *lu, int k, int lane) {
-    const int u1 = P.upd_ptr[k + 1];
-    for (int u = P.upd_ptr[k]; u < u1; ++u) {
-        const int c = P.upd_c[u];
-        const LT uval = lu[P.upd_upos[u]];
-        const int ls = P.lstart[c], lc = P.lcount[c];
-        const int *d = P.dst + P.upd_dst[u];
-        for (int s = lane; s < lc; s += 32) {
-            const int dp = d[s];
-            lu[dp] -= lu[ls + s] * uval;
-        }
-        __syncwarp();
-    }
-    const LT piv = lu[P.dpos[k]];
-    if (piv == (LT)0) {
-        if (lane == 0) S.piv_err = 1;
-    } else {
-        const int ls = P.lstart[k], lc = P.lcount[k];
-        for (int s = lane; s < lc; s += 32) lu[ls + s] = lu[ls + s] / piv;
-    }
-    __syncwarp();
-}
-
+// Right-looking refactorisation in conflict-free phases; sets S.piv_err on a zero pivot.
 template <typename LT>
 __device__ void refactor(const DevPlan &P, Shared &S, LT *lu) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int g = 0; g < P.nref; ++g) {
-        const int4 G = P.ref_groups[g];
-        if (G.z == 0) {
-            for (int t = G.x + warp; t < G.y; t += nw) factor_column(P, S, lu, P.ref_order[t], lane);
-        } else if (warp == 0) {
-            for (int t = G.x; t < G.y; ++t) factor_column(P, S, lu, P.ref_order[t], lane);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    for (int ph = 0; ph < P.nphases; ++ph) {
+        const int4 Q = P.phases[ph];
+        const int lanes = P.ph_lanes[ph];
+        for (int e = Q.z + tid; e < Q.w; e += nt) {
+            const int2 dv = P.divs[e];
+            lu[dv.x] = lu[dv.x] / lu[dv.y];
+        }
+        const int per_warp = 32 / lanes;
+        const int sub = lane & (lanes - 1);
+        const int nslots = nw * per_warp;
+        for (int g = Q.x + warp * per_warp + lane / lanes; g < Q.y; g += nslots) {
+            const int4 G = P.grp[g];
+            const int lc = P.grp_lc[g];
+            const LT f = lu[G.y] / lu[G.z];  // U(c, j) / U(c, c)
+            const int *d = P.dst + G.w;
+            for (int s = sub; s < lc; s += lanes) lu[d[s]] -= lu[G.x + s] * f;
         }
         __syncthreads();
     }
+    int zero = 0;
+    for (int k = tid; k < P.m; k += nt) zero |= lu[P.dpos[k]] == (LT)0;
+    if (zero) S.piv_err = 1;
+    __syncthreads();
 }
 
-// row-oriented, level-scheduled substitution.  upper == false: x_i -= L(i,:) x (unit
+// Row-oriented, level-scheduled substitution.  upper == false: x_i -= L(i,:) x (unit
 // diagonal); upper == true: x_i = (x_i - U(i,:) x) / U(i,i).
 template <typename LT, typename XT, bool upper>
 __device__ void tri_solve(const DevPlan &P, const LT *lu, XT *x) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int *rp = upper ? P.urow_ptr : P.lrow_ptr;
-    const int *rc = upper ? P.urow_col : P.lrow_col;
-    const int *rpos = upper ? P.urow_pos : P.lrow_pos;
-    const int *order = upper ? P.bwd_order : P.fwd_order;
+    const int4 *desc = upper ? P.bwd_desc : P.fwd_desc;
+    const int2 *pc = upper ? P.urow_pc : P.lrow_pc;
     const int4 *groups = upper ? P.bwd_groups : P.fwd_groups;
     const int ng = upper ? P.nbwd : P.nfwd;
     for (int g = 0; g < ng; ++g) {
@@ -242,28 +236,41 @@ __device__ void tri_solve(const DevPlan &P, const LT *lu, XT *x) {
             for (int base = G.x + warp * per_warp; base < G.y; base += nw * per_warp) {
                 const int t = base + slot;
                 XT s = (XT)0;
-                int i = -1;
+                int4 d = make_int4(-1, 0, 0, 0);
                 if (t < G.y) {
-                    i = order[t];
-                    const int e1 = rp[i + 1];
-                    for (int e = rp[i] + sub; e < e1; e += lanes) s += (XT)lu[rpos[e]] * x[rc[e]];
+                    d = desc[t];
+                    for (int e = sub; e < d.z; e += lanes) {
+                        const int2 q = pc[d.y + e];
+                        s += (XT)lu[q.x] * x[q.y];
+                    }
                 }
                 s = warp_sum(s, lanes);
-                if (i >= 0 && sub == 0) {
-                    if (upper) x[i] = (x[i] - s) / (XT)lu[P.dpos[i]];
-                    else x[i] -= s;
+                if (d.x >= 0 && sub == 0) {
+                    if (upper) x[d.x] = (x[d.x] - s) / (XT)lu[d.w];
+                    else x[d.x] -= s;
                 }
             }
         } else if (warp == 0) {
+            // chain: one row after the other; the next row's descriptor and first 32
+            // entries are loaded while the current row is reduced
+            int4 dn = desc[G.x];
+            int2 qn = lane < dn.z ? pc[dn.y + lane] : make_int2(0, 0);
             for (int t = G.x; t < G.y; ++t) {
-                const int i = order[t];
-                XT s = (XT)0;
-                const int e1 = rp[i + 1];
-                for (int e = rp[i] + lane; e < e1; e += 32) s += (XT)lu[rpos[e]] * x[rc[e]];
+                const int4 d = dn;
+                const int2 q = qn;
+                if (t + 1 < G.y) {
+                    dn = desc[t + 1];
+                    qn = lane < dn.z ? pc[dn.y + lane] : make_int2(0, 0);
+                }
+                XT s = lane < d.z ? (XT)lu[q.x] * x[q.y] : (XT)0;
+                for (int e = lane + 32; e < d.z; e += 32) {
+                    const int2 q2 = pc[d.y + e];
+                    s += (XT)lu[q2.x] * x[q2.y];
+                }
                 s = warp_sum(s, 32);
                 if (lane == 0) {
-                    if (upper) x[i] = (x[i] - s) / (XT)lu[P.dpos[i]];
-                    else x[i] -= s;
+                    if (upper) x[d.x] = (x[d.x] - s) / (XT)lu[d.w];
+                    else x[d.x] -= s;
                 }
                 __syncwarp();
             }
@@ -272,21 +279,55 @@ __device__ void tri_solve(const DevPlan &P, const LT *lu, XT *x) {
     }
 }
 
-template <typename LT, typename XT>
+// FP64 residual of the Newton system, F - J dx, written as the next right-hand side.
+// J dx is formed row by row from dS/dV (the FP64 Jacobian, never stored).
+template <typename XT>
+__device__ void newton_residual(const DevPlan &P, Shared &S, const double2 *__restrict__ V,
+                                const double2 *__restrict__ Ibus, const double2 *__restrict__ Fbus,
+                                const double *__restrict__ dxg, XT *x) {
+    for (int r = threadIdx.x; r < P.n; r += blockDim.x) {
+        const int ip = P.xP[r], iq = P.xQ[r];
+        if (ip < 0 && iq < 0) continue;
+        const double2 vr = V[r];
+        double accP = 0.0, accQ = 0.0;
+        const int p1 = P.Rp[r + 1];
+        for (int p = P.Rp[r]; p < p1; ++p) {
+            const int c = P.Rj[p];
+            const int ia = P.xVa[c], im = P.xVm[c];
+            const double dA = ia >= 0 ? dxg[ia] : 0.0;
+            const double dM = im >= 0 ? dxg[im] : 0.0;
+            if (ia < 0 && im < 0) continue;
+            double dvar, dvai;
+            double2 dvm;
+            dsbus(ybus_value(P, S, p), vr, V[c], r == c, r == c ? Ibus[r] : make_double2(0.0, 0.0), dvar, dvai,
+                  dvm);
+            accP += dvar * dA + dvm.x * dM;
+            accQ += dvai * dA + dvm.y * dM;
+        }
+        if (P.distributed && ip >= 0) accP += P.wJ[r] * dxg[P.xSlack];
+        const double2 F = Fbus[r];
+        if (ip >= 0) x[ip] = (XT)(F.x - accP);
+        if (iq >= 0) x[iq] = (XT)(F.y - accQ);
+    }
+}
+
+template <typename LT, typename XT, bool LU_SMEM, bool REFINE>
 __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const BatchArgs A) {
     extern __shared__ __align__(16) unsigned char dyn[];
     __shared__ Shared S;
     const int tid = threadIdx.x;
-    const int n = P.n;
-    const size_t xbytes = ((size_t)P.m * sizeof(XT) + 15) & ~(size_t)15;
+    const int n = P.n, m = P.m;
+    const size_t xbytes = ((size_t)m * sizeof(XT) + 15) & ~(size_t)15;
     XT *x = reinterpret_cast<XT *>(dyn);
     unsigned char *slab = A.scratch + (size_t)blockIdx.x * (size_t)A.slab_bytes;
     double2 *V = reinterpret_cast<double2 *>(slab);
     double2 *Ibus = V + n;
-    double *Vm = reinterpret_cast<double *>(Ibus + n);
+    double2 *Fbus = Ibus + n;
+    double *Vm = reinterpret_cast<double *>(Fbus + n);
     double *Va = Vm + n;
-    const size_t bus_bytes = (((size_t)n * 48) + 255) & ~(size_t)255;
-    LT *lu = A.lu_in_smem ? reinterpret_cast<LT *>(dyn + xbytes) : reinterpret_cast<LT *>(slab + bus_bytes);
+    double *dxg = Va + n;
+    const size_t bus_bytes = (((size_t)n * 64 + (size_t)m * 8) + 255) & ~(size_t)255;
+    LT *lu = LU_SMEM ? reinterpret_cast<LT *>(dyn + xbytes) : reinterpret_cast<LT *>(slab + bus_bytes);
 
     for (;;) {
         if (tid == 0) S.job = atomicAdd(A.job_counter, 1);
@@ -321,6 +362,7 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
                 }
                 S.novr = min(k1 - k0, kMaxOverrides);
                 S.piv_err = 0;
+                S.slack_absorbed = 0.0;
             }
             __syncthreads();
             if (tid < S.novr) {
@@ -337,7 +379,7 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
             __syncthreads();
             double norm;
             int bad;
-            mismatch<XT>(P, S, V, Ibus, Sb, x, norm, bad);
+            mismatch<XT>(P, S, V, Ibus, Fbus, Sb, x, norm, bad);
             bool conv = !bad && norm < A.tol;
             int it = 0, err = 0;
             double *Jout = (A.Jout && inst == A.j_inst) ? A.Jout : nullptr;
@@ -352,6 +394,14 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
                 }
                 tri_solve<LT, XT, false>(P, lu, x);
                 tri_solve<LT, XT, true>(P, lu, x);
+                if (REFINE) {
+                    for (int k = tid; k < m; k += blockDim.x) dxg[k] = (double)x[k];
+                    __syncthreads();
+                    newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, x);
+                    __syncthreads();
+                    tri_solve<LT, XT, false>(P, lu, x);
+                    tri_solve<LT, XT, true>(P, lu, x);
+                }
                 // voltage update
                 double lmin = 1.0;
                 for (int b = tid; b < n; b += blockDim.x) {
@@ -365,8 +415,8 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
                         va = atan2(v.y, v.x);
                     }
                     const int ia = P.xVa[b], im = P.xVm[b];
-                    if (ia >= 0) va -= (double)x[ia];
-                    if (im >= 0) vm -= (double)x[im];
+                    if (ia >= 0) va -= REFINE ? dxg[ia] + (double)x[ia] : (double)x[ia];
+                    if (im >= 0) vm -= REFINE ? dxg[im] + (double)x[im] : (double)x[im];
                     double sn, cs;
                     sincos(va, &sn, &cs);
                     V[b] = make_double2(vm * cs, vm * sn);
@@ -375,7 +425,8 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
                     lmin = fmin(lmin, vm);
                 }
                 if (P.distributed) {
-                    const double dxs = (double)x[P.xSlack];
+                    const double dxs =
+                        REFINE ? dxg[P.xSlack] + (double)x[P.xSlack] : (double)x[P.xSlack];
                     const double vmin = block_min(S, lmin);  // contains barriers
                     if (tid == 0) S.slack_absorbed -= dxs;
                     if (vmin < 0.0) {
@@ -387,7 +438,7 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
                     }
                 }
                 __syncthreads();
-                mismatch<XT>(P, S, V, Ibus, Sb, x, norm, bad);
+                mismatch<XT>(P, S, V, Ibus, Fbus, Sb, x, norm, bad);
                 if (bad) {
                     err = 3;  // InifiniteValue
                     break;
@@ -415,15 +466,32 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
     }
 }
 
-template <typename LT, typename XT>
-void *kernel_ptr() {
-    return reinterpret_cast<void *>(&nr_batch_kernel<LT, XT>);
+template <typename LT, typename XT, bool SM, bool RF>
+cudaError_t launch_variant(const DevPlan &P, const BatchArgs &A, int threads, int grid, size_t smem,
+                           cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(nr_batch_kernel<LT, XT, SM, RF>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    nr_batch_kernel<LT, XT, SM, RF><<<grid, threads, smem, st>>>(P, A);
+    return cudaGetLastError();
+}
+
+template <typename LT, typename XT, bool SM, bool RF>
+int occupancy_variant(int threads, size_t smem) {
+    int nb = 0;
+    if (cudaFuncSetAttribute(nr_batch_kernel<LT, XT, SM, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, nr_batch_kernel<LT, XT, SM, RF>, threads, smem) !=
+        cudaSuccess)
+        return 0;
+    return nb;
 }
 
 }  // namespace
 
 size_t slab_bytes(const DevPlan &P, int lu_bytes, bool lu_in_smem) {
-    size_t bus = (((size_t)P.n * 48) + 255) & ~(size_t)255;
+    size_t bus = (((size_t)P.n * 64 + (size_t)P.m * 8) + 255) & ~(size_t)255;
     size_t lu = lu_in_smem ? 0 : (((size_t)P.nnzLU * lu_bytes + 255) & ~(size_t)255);
     return bus + lu;
 }
@@ -435,37 +503,27 @@ size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem) 
 
 cudaError_t launch_nr_batch(const DevPlan &P, const BatchArgs &A, int precision, int threads, int grid,
                             size_t smem, cudaStream_t stream) {
-    cudaError_t e;
+    const bool sm = A.lu_in_smem != 0;
     if (precision == 0) {
-        e = cudaFuncSetAttribute(nr_batch_kernel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return e;
-        nr_batch_kernel<double, double><<<grid, threads, smem, stream>>>(P, A);
-    } else {
-        e = cudaFuncSetAttribute(nr_batch_kernel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return e;
-        nr_batch_kernel<float, float><<<grid, threads, smem, stream>>>(P, A);
+        return sm ? launch_variant<double, double, true, false>(P, A, threads, grid, smem, stream)
+                  : launch_variant<double, double, false, false>(P, A, threads, grid, smem, stream);
     }
-    return cudaGetLastError();
+    if (A.refine)
+        return sm ? launch_variant<float, float, true, true>(P, A, threads, grid, smem, stream)
+                  : launch_variant<float, float, false, true>(P, A, threads, grid, smem, stream);
+    return sm ? launch_variant<float, float, true, false>(P, A, threads, grid, smem, stream)
+              : launch_variant<float, float, false, false>(P, A, threads, grid, smem, stream);
 }
 
-int nr_occupancy(int precision, int threads, size_t smem) {
-    int nb = 0;
-    cudaError_t e;
-    if (precision == 0) {
-        e = cudaFuncSetAttribute(nr_batch_kernel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, nr_batch_kernel<double, double>, threads, smem);
-    } else {
-        e = cudaFuncSetAttribute(nr_batch_kernel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, nr_batch_kernel<float, float>, threads, smem);
-    }
-    if (e != cudaSuccess) return 0;
-    return nb;
+int nr_occupancy(int precision, bool lu_in_smem, bool refine, int threads, size_t smem) {
+    if (precision == 0)
+        return lu_in_smem ? occupancy_variant<double, double, true, false>(threads, smem)
+                          : occupancy_variant<double, double, false, false>(threads, smem);
+    if (refine)
+        return lu_in_smem ? occupancy_variant<float, float, true, true>(threads, smem)
+                          : occupancy_variant<float, float, false, true>(threads, smem);
+    return lu_in_smem ? occupancy_variant<float, float, true, false>(threads, smem)
+                      : occupancy_variant<float, float, false, false>(threads, smem);
 }
 
 }  // namespace l2g

@@ -23,13 +23,19 @@ struct DevPlan {
     int nconst;
     const int *xP, *xQ, *xVa, *xVm;
     int xSlack;
-    const int *upd_ptr, *upd_c, *upd_upos, *upd_dst, *dst;
-    const int *dpos, *lstart, *lcount;
-    const int *ref_order;
-    const int4 *ref_groups;
-    int nref;
-    const int *lrow_ptr, *lrow_col, *lrow_pos, *urow_ptr, *urow_col, *urow_pos;
-    const int *fwd_order, *bwd_order;
+    const double *wJ;        // distributed slack: J(P(r), 0) per bus (0 if none)
+    // right-looking refactorisation
+    const int4 *grp;         // per update group: L(:,c) start, U(c,j) position, pivot position, dst offset
+    const int *grp_lc;       // per update group: rows of L(:,c)
+    const int *dst;
+    const int4 *phases;      // group range, division range
+    const int *ph_lanes;
+    int nphases;
+    const int2 *divs;        // (L entry, pivot) per division
+    const int *dpos;         // pivot position per column (m)
+    // triangular solves: rows in level order as (row, first entry, entries, diagonal)
+    const int4 *fwd_desc, *bwd_desc;
+    const int2 *lrow_pc, *urow_pc;  // (LU position, column) per entry
     const int4 *fwd_groups, *bwd_groups;
     int nfwd, nbwd;
 };
@@ -59,6 +65,7 @@ struct BatchArgs {
     unsigned char *scratch;   // per-CTA slab
     long long slab_bytes;
     int lu_in_smem;
+    int refine;               // FP32 LU only: one FP64-residual refinement of every Newton step
 };
 
 constexpr int kMaxOverrides = 32;
@@ -68,9 +75,10 @@ size_t slab_bytes(const DevPlan &P, int lu_bytes, bool lu_in_smem);
 size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem);
 
 // precision: 0 = FP64 LU and solves, 1 = FP32 LU and solves (FP64 mismatch and update).
+// A.lu_in_smem and A.refine select the kernel variant.
 cudaError_t launch_nr_batch(const DevPlan &P, const BatchArgs &A, int precision, int threads, int grid,
                             size_t smem, cudaStream_t stream);
 // Resident CTAs per SM for a configuration (0 if it cannot launch).
-int nr_occupancy(int precision, int threads, size_t smem);
+int nr_occupancy(int precision, bool lu_in_smem, bool refine, int threads, size_t smem);
 
 }  // namespace l2g

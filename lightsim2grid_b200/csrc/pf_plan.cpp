@@ -434,38 +434,118 @@ int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, con
         for (int t = 0; t < P.lcount[k]; ++t) P.Urow_k[P.lstart[k] + t] = Lrows[k][t];
     }
 
-    // ---------------------------------------------------------------- refactorisation lists
-    std::vector<int> rowpos(m, -1);
-    P.upd_ptr.assign(m + 1, 0);
-    std::vector<int> level(m, 0), worklen(m, 0);
+    // ---------------------------------------------------------------- refactorisation schedule
+    // levels: a pivot can be applied once every pivot updating its column is done
+    std::vector<int> level(m, 0);
     P.flops_refactor = 0;
     for (int k = 0; k < m; ++k) {
-        for (int p = P.colstart[k]; p < P.colstart[k + 1]; ++p) rowpos[P.Urow_k[p]] = p;
-        int lv = 0, wl = P.lcount[k];
-        for (size_t t = 0; t < Ucols[k].size(); ++t) {
-            int c = Ucols[k][t];
-            P.upd_c.push_back(c);
-            P.upd_upos.push_back(P.colstart[k] + (int)t);
-            P.upd_dst.push_back((int)P.dst.size());
+        int lv = 0;
+        for (int c : Ucols[k]) lv = std::max(lv, level[c] + 1);
+        level[k] = lv;
+        for (int c : Ucols[k]) P.flops_refactor += P.lcount[c];
+    }
+    P.colleve = level;
+    int nlev = 0;
+    for (int v : level) nlev = std::max(nlev, v + 1);
+    P.levels_refactor = nlev;
+    // U row lists: for pivot c, the columns j > c with U(c, j) != 0 and the position of U(c, j)
+    std::vector<std::vector<std::pair<int, int>>> urows(m);
+    for (int k = 0; k < m; ++k)
+        for (size_t t = 0; t < Ucols[k].size(); ++t) urows[Ucols[k][t]].push_back({k, P.colstart[k] + (int)t});
+    std::vector<std::vector<int>> bylevel(nlev);
+    for (int k = 0; k < m; ++k) bylevel[level[k]].push_back(k);
+    std::vector<int> rowpos(m, -1);
+    std::vector<uint64_t> used(P.nnzLU, 0);  // phases of the current level writing an entry
+    std::vector<int> used_level(P.nnzLU, -1);
+    std::vector<int> pend_div;               // pivots whose divisions are pending
+    for (int l = 0; l < nlev; ++l) {
+        // the groups of this level
+        struct G { int c, j, upos; };
+        std::vector<G> gs;
+        for (int c : bylevel[l])
+            for (auto &e : urows[c]) gs.push_back({c, e.first, e.second});
+        // greedy colouring into conflict-free phases (first fit in group order)
+        std::vector<std::vector<int>> ph_groups;
+        std::vector<std::vector<int>> gdst(gs.size());
+        for (size_t g = 0; g < gs.size(); ++g) {
+            const int c = gs[g].c, j = gs[g].j;
+            for (int p = P.colstart[j]; p < P.colstart[j + 1]; ++p) rowpos[P.Urow_k[p]] = p;
             for (int s = 0; s < P.lcount[c]; ++s) {
-                int r = Lrows[c][s];
-                int d = rowpos[r];
+                int d = rowpos[Lrows[c][s]];
                 if (d < 0) {
                     msg = "build_plan: internal error, LU pattern is not closed";
                     return SolverAnalyze;
                 }
-                P.dst.push_back(d);
+                gdst[g].push_back(d);
             }
-            P.flops_refactor += P.lcount[c];
-            wl += P.lcount[c];
-            lv = std::max(lv, level[c] + 1);
+            for (int p = P.colstart[j]; p < P.colstart[j + 1]; ++p) rowpos[P.Urow_k[p]] = -1;
+            uint64_t busy = 0;
+            for (int d : gdst[g]) {
+                if (used_level[d] != l) {
+                    used_level[d] = l;
+                    used[d] = 0;
+                }
+                busy |= used[d];
+            }
+            int ph = 0;
+            while (ph < 64 && ((busy >> ph) & 1u)) ++ph;
+            if (ph == 64) {
+                msg = "build_plan: more than 64 conflicting update phases in one level";
+                return SolverAnalyze;
+            }
+            for (int d : gdst[g]) used[d] |= (uint64_t)1 << ph;
+            if ((int)ph_groups.size() <= ph) ph_groups.resize(ph + 1);
+            ph_groups[ph].push_back((int)g);
         }
-        level[k] = lv;
-        worklen[k] = wl;
-        P.upd_ptr[k + 1] = (int)P.upd_c.size();
-        for (int p = P.colstart[k]; p < P.colstart[k + 1]; ++p) rowpos[P.Urow_k[p]] = -1;
+        if (ph_groups.empty()) ph_groups.resize(1);  // a level with no updates still divides
+        for (size_t ph = 0; ph < ph_groups.size(); ++ph) {
+            Plan::Phase Q;
+            Q.gbeg = (int)P.grp_lstart.size();
+            int maxlc = 0;
+            // longest groups first: better balance of the round-robin
+            std::stable_sort(ph_groups[ph].begin(), ph_groups[ph].end(), [&](int a, int b) {
+                return P.lcount[gs[a].c] > P.lcount[gs[b].c];
+            });
+            for (int g : ph_groups[ph]) {
+                const int c = gs[g].c;
+                P.grp_lstart.push_back(P.lstart[c]);
+                P.grp_lcount.push_back(P.lcount[c]);
+                P.grp_upos.push_back(gs[g].upos);
+                P.grp_dpos.push_back(P.dpos[c]);
+                P.grp_dst.push_back((int)P.dst.size());
+                P.dst.insert(P.dst.end(), gdst[g].begin(), gdst[g].end());
+                maxlc = std::max(maxlc, P.lcount[c]);
+            }
+            Q.gend = (int)P.grp_lstart.size();
+            Q.dbeg = (int)P.div_pos.size();
+            if (ph == 0) {
+                for (int c : pend_div)
+                    for (int t = 0; t < P.lcount[c]; ++t) {
+                        P.div_pos.push_back(P.lstart[c] + t);
+                        P.div_dpos.push_back(P.dpos[c]);
+                    }
+                pend_div.clear();
+            }
+            Q.dend = (int)P.div_pos.size();
+            Q.lanes = lanes_for(maxlc);
+            P.phases.push_back(Q);
+        }
+        pend_div = bylevel[l];
     }
-    make_groups(level, worklen, opt.chain_max_items, P.ref_order, P.ref_groups, P.levels_refactor, false);
+    {
+        // trailing phase: divisions of the last level, and the pivot check of every column
+        Plan::Phase Q;
+        Q.gbeg = Q.gend = (int)P.grp_lstart.size();
+        Q.dbeg = (int)P.div_pos.size();
+        for (int c : pend_div)
+            for (int t = 0; t < P.lcount[c]; ++t) {
+                P.div_pos.push_back(P.lstart[c] + t);
+                P.div_dpos.push_back(P.dpos[c]);
+            }
+        Q.dend = (int)P.div_pos.size();
+        Q.lanes = 1;
+        P.phases.push_back(Q);
+    }
 
     // ---------------------------------------------------------------- triangular solves
     {

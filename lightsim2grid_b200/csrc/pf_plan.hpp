@@ -78,12 +78,21 @@ struct Plan {
     std::vector<int> dpos;            // per step: position of the diagonal
     std::vector<int> lstart, lcount;  // per step: L part (rows > k, ascending)
     std::vector<int> Urow_k;          // per LU position: row (step numbering)
-    // refactorisation: per column k, updates (c, position of U(c,k), first dst index)
-    std::vector<int> upd_ptr;         // m + 1
-    std::vector<int> upd_c, upd_upos, upd_dst;
-    std::vector<int> dst;             // destination positions of L(:,c) rows in column k
-    std::vector<int> ref_order;       // columns in level order
-    std::vector<LevelGroup> ref_groups;
+    // Right-looking refactorisation.  An update group (c, j) applies pivot c to column j:
+    // A(i, j) -= A(i, c) * U(c, j) / U(c, c) for every row i of L(:, c).  Groups of one
+    // elimination level are independent except when they write the same entry; they are
+    // coloured into conflict-free phases.  The divisions L(:, c) /= U(c, c) of a level run
+    // at the start of the next level's first phase (they touch no entry that phase uses).
+    std::vector<int> grp_lstart, grp_lcount, grp_upos, grp_dpos, grp_dst;  // per group
+    std::vector<int> dst;             // destination positions, grp_dst[g] .. + grp_lcount[g]
+    struct Phase {
+        int gbeg, gend;               // update groups
+        int dbeg, dend;               // division entries
+        int lanes;                    // lanes per group (1..32)
+    };
+    std::vector<Phase> phases;
+    std::vector<int> div_pos, div_dpos;  // L entry and its pivot, per division entry
+    std::vector<int> colleve;         // elimination level per column
     // triangular solves (row oriented)
     std::vector<int> lrow_ptr, lrow_col, lrow_pos;   // L(i, k < i)
     std::vector<int> urow_ptr, urow_col, urow_pos;   // U(i, k > i)
@@ -108,7 +117,7 @@ struct Plan {
 
 struct PlanOptions {
     double pivot_threshold = 1e-3;    // diagonal preference of the first factorisation
-    int chain_max_items = 2;          // levels with at most this many items join a chain
+    int chain_max_items = 2;          // solve levels with at most this many rows join a chain
     int warps = 16;                   // warps per CTA the schedules are sized for
 };
 

@@ -1,0 +1,95 @@
+"""One N-1 batch launch of the engine, for profilers (ncu) and quick timing.
+
+    python -m lightsim2grid_b200.profile_case --grid grid2848 --cases 600 --precision 1 --repeat 3
+
+Builds the plan, prepares the outages (islanding check), runs ``--warmup`` untimed launches
+and ``--repeat`` timed launches of ``nr_batch_kernel`` through ``pf_batch_device``, and prints
+the CUDA-event time per launch and the converged count.
+"""
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--grid", default="grid2848")
+    ap.add_argument("--cases", type=int, default=0, help="first N branches (0: all)")
+    ap.add_argument("--precision", type=int, default=1)
+    ap.add_argument("--repeat", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--lu-placement", type=int, default=0)
+    ap.add_argument("--chain-max", type=int, default=0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
+    args = ap.parse_args()
+
+    import torch
+    from lightsim2grid_b200 import Plan, GPUNRSolverSingleSlack, synthetic, _native as nat
+
+    g, _ = synthetic.make_named_grid(args.grid)
+    Y, S = g.get_Ybus(), g.get_Sbus()
+    sl, w, pv, pq = g.get_slack_ids(), g.get_slack_weights(), g.get_pv(), g.get_pq()
+    base = GPUNRSolverSingleSlack()
+    if not base.compute_pf(Y, g.flat_start(), S, sl, w, pv, pq, 10, 1e-8):
+        raise SystemExit("base case did not converge")
+    Vn = base.get_V()
+    nb = g.nb_powerline() if args.cases <= 0 else min(args.cases, g.nb_powerline())
+    coeffs = [g.branch_coeffs([b]) for b in range(nb)]
+    plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, threads=args.threads,
+                lu_placement=args.lu_placement, chain_max_items=args.chain_max, max_ctas_per_sm=args.ctas_per_sm)
+    lib = plan._lib
+    cp = np.zeros(nb + 1, np.int32)
+    rows, cols, vals = [], [], []
+    for k, lst in enumerate(coeffs):
+        cp[k + 1] = cp[k] + len(lst)
+        for (r, c, y) in lst:
+            rows.append(r)
+            cols.append(c)
+            vals.append(y)
+    rows, cols, vals = nat.as_i32(rows), nat.as_i32(cols), nat.as_c128(vals).ravel()
+    solv = np.zeros(nb, np.int32)
+    optr = np.zeros(nb + 1, np.int32)
+    cap = int(cp[-1])
+    opos = np.zeros(cap, np.int32)
+    oval = np.zeros(cap, np.complex128)
+    nw = lib.pf_n1_prepare(plan.handle, nb, nat.ptr(cp, nat.i32p), nat.ptr(rows, nat.i32p), nat.ptr(cols, nat.i32p),
+                           nat.cptr(vals), nat.ptr(solv, nat.i32p), nat.ptr(optr, nat.i32p), nat.ptr(opos, nat.i32p),
+                           nat.cptr(oval), cap)
+    assert nw >= 0, nat.last_error(lib)
+    ns = int(solv.sum())
+    dev = torch.device("cuda:0")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    bufs = [t(nat.as_c128(Vn).ravel().view(np.float64)), t(nat.as_c128(S).ravel().view(np.float64)),
+            t(optr[:ns + 1]), t(opos[:nw]), t(oval[:nw].view(np.float64)), t(np.arange(ns, dtype=np.int32)),
+            t(np.ones(ns, np.int32)), torch.zeros(ns * g.n_bus * 2, dtype=torch.float64, device=dev),
+            torch.zeros(ns, dtype=torch.int32, device=dev), torch.zeros(ns, dtype=torch.int32, device=dev)]
+    b = nat.PfDeviceBatch(n_inst=ns, V0=bufs[0].data_ptr(), v0_stride=0, Sbus=bufs[1].data_ptr(), sbus_stride=0,
+                          ovr_ptr=bufs[2].data_ptr(), ovr_pos=bufs[3].data_ptr(), ovr_val=bufs[4].data_ptr(),
+                          max_iter=10, tol=1e-8, chain=0, job_first=bufs[5].data_ptr(), job_count=bufs[6].data_ptr(),
+                          njobs=ns, Vout=bufs[7].data_ptr(), iters=bufs[8].data_ptr(), errs=bufs[9].data_ptr())
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        assert lib.pf_batch_device(plan.handle, nat.ctypes.byref(b), stream.cuda_stream) == 0, nat.last_error(lib)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.repeat):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        assert lib.pf_batch_device(plan.handle, nat.ctypes.byref(b), stream.cuda_stream) == 0, nat.last_error(lib)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    it = bufs[8].cpu().numpy()
+    er = bufs[9].cpu().numpy()
+    out = {"grid": args.grid, "cases": ns, "precision": args.precision, "ms": times,
+           "converged": int((er == 0).sum()), "iterations": int(it.sum()),
+           "pf_per_s": float((er == 0).sum() / (np.mean(times) * 1e-3)), "plan": plan.info()}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    sys.exit(main())
