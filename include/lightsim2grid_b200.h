@@ -24,13 +24,15 @@ typedef struct pf_options {
                                FP64 mismatch, update and convergence test (mixed form)        */
     int threads;            /* threads per CTA (multiple of 32, <= 512); 0: chosen by size   */
     int lu_placement;       /* 0 auto, 1 shared memory, 2 global memory                      */
-    int chain_max_items;    /* levels with at most this many columns run on one warp; 0: 2  */
+    int fuse_forward;       /* forward substitution fused into the refactorisation program.
+                               0: default (on), 1: on, 2: off                                  */
     double pivot_threshold; /* diagonal preference of the first factorisation; 0: 1e-3      */
     int fp64_fallback;      /* mixed form: re-run instances that did not converge in FP64.
                                0: default (on), 1: on, 2: off                                  */
     int max_ctas_per_sm;    /* cap on resident CTAs per SM; 0: occupancy limit               */
-    int refine;             /* mixed form: refine every Newton step once against the FP64
+    int refine;             /* mixed form: refine Newton steps once against the FP64
                                Jacobian.  0: default (on), 1: on, 2: off                       */
+    double refine_threshold;/* ... the steps taken from ||F||_inf below this; 0: 1e-3          */
 } pf_options;
 
 /* Sizes and schedule statistics of a plan. */
@@ -129,6 +131,20 @@ int pf_batch_ts(pf_plan *plan, int nsteps, const double *Sbus_ri, const double *
 /* Device-resident batch on `stream` (a cudaStream_t, NULL for the default stream).  No
    host synchronisation; capturable in a CUDA graph once the plan exists. */
 int pf_batch_device(pf_plan *plan, const pf_device_batch *batch, void *stream);
+
+/* pf_batch_device, synchronously, with per-phase SM-cycle counters: out[0..7] = cycles summed
+   over CTAs spent in mismatch, J fill, refactorisation, forward substitution, backward
+   substitution, refinement (mixed form), voltage update / start-up, and the number of
+   instances.  The device counterpart of the reference's per-phase NR timers
+   (get_timers_jacobian, src/powerflow_algorithm/BaseNRAlgo.hpp:48-62). */
+int pf_batch_device_phase_cycles(pf_plan *plan, const pf_device_batch *batch, void *stream, double *out);
+
+/* pf_batch_device, synchronously, recording the SM clock after every phase of the first
+   Newton iteration of CTA 0's first instance: out[i] = cycles since the first mark (the
+   marks follow the J fill, then every phase of the refactorisation, backward and, when the
+   step is refined, forward and backward programs, then the update).  Returns the number of
+   marks (<= cap).  A diagnostic of the phase programs' critical path. */
+int pf_batch_device_phase_trace(pf_plan *plan, const pf_device_batch *batch, void *stream, double *out, int cap);
 
 /* Timers of the last call (seconds): [0] total, [1] host preparation, [2] host->device,
    [3] kernel, [4] device->host, [5] instances re-run in FP64 (count, as a double).

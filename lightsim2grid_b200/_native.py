@@ -18,8 +18,9 @@ f64p = ctypes.POINTER(ctypes.c_double)
 
 class PfOptions(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("threads", ctypes.c_int), ("lu_placement", ctypes.c_int),
-                ("chain_max_items", ctypes.c_int), ("pivot_threshold", ctypes.c_double),
-                ("fp64_fallback", ctypes.c_int), ("max_ctas_per_sm", ctypes.c_int), ("refine", ctypes.c_int)]
+                ("fuse_forward", ctypes.c_int), ("pivot_threshold", ctypes.c_double),
+                ("fp64_fallback", ctypes.c_int), ("max_ctas_per_sm", ctypes.c_int), ("refine", ctypes.c_int),
+                ("refine_threshold", ctypes.c_double)]
 
 
 class PfPlanInfo(ctypes.Structure):
@@ -47,7 +48,8 @@ class PfDeviceBatch(ctypes.Structure):
 #: exported symbols, as declared in include/lightsim2grid_b200.h
 SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_get", "pf_set_ybus_values",
            "pf_solve", "pf_get_J", "pf_batch_n1", "pf_n1_prepare", "pf_batch_ts", "pf_batch_device", "pf_timers",
-           "pf_host_jacobian_pattern", "pf_host_schedule_solve")
+           "pf_host_jacobian_pattern", "pf_host_schedule_solve", "pf_batch_device_phase_cycles",
+           "pf_batch_device_phase_trace")
 
 
 def load(path=None):
@@ -87,6 +89,11 @@ def load(path=None):
                                 ctypes.c_double, f64p, i32p, i32p, i32p, i32p]
     lib.pf_batch_device.restype = ctypes.c_int
     lib.pf_batch_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfDeviceBatch), ctypes.c_void_p]
+    lib.pf_batch_device_phase_cycles.restype = ctypes.c_int
+    lib.pf_batch_device_phase_cycles.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfDeviceBatch), ctypes.c_void_p, f64p]
+    lib.pf_batch_device_phase_trace.restype = ctypes.c_int
+    lib.pf_batch_device_phase_trace.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfDeviceBatch), ctypes.c_void_p,
+                                                f64p, ctypes.c_int]
     lib.pf_timers.restype = ctypes.c_int
     lib.pf_timers.argtypes = [ctypes.c_void_p, f64p, ctypes.c_int]
     lib.pf_host_jacobian_pattern.restype = ctypes.c_int

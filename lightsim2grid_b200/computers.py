@@ -41,7 +41,7 @@ class _BatchBase:
         return self._solver_type
 
     def set_plan_options(self, **kwargs):
-        """Engine options (threads, lu_placement, chain_max_items, fp64_fallback, max_ctas_per_sm)."""
+        """Engine options (threads, lu_placement, fuse_forward, fp64_fallback, max_ctas_per_sm, refine)."""
         self._plan_options = dict(kwargs)
         self._plan = None
 

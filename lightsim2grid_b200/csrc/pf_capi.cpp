@@ -70,7 +70,7 @@ struct pf_plan {
     void *d_dbl = nullptr;
     l2g::DevPlan dp{};
     // device work buffers
-    DevBuf scratch, counter, V0, Sbus, optr, opos, oval, jfirst, jcount, Vout, iters, errs, Jout;
+    DevBuf scratch, counter, V0, Sbus, optr, opos, oval, jfirst, jcount, Vout, iters, errs, Jout, cycles;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // host state
@@ -239,30 +239,6 @@ size_t push(std::vector<unsigned char> &blob, const std::vector<T> &v) {
     return off;
 }
 
-std::vector<int> flat_groups(const std::vector<l2g::LevelGroup> &g) {
-    std::vector<int> out;
-    for (auto &x : g) {
-        out.push_back(x.begin);
-        out.push_back(x.end);
-        out.push_back(x.kind);
-        out.push_back(x.lanes);
-    }
-    return out;
-}
-
-std::vector<int> pack_rows(const std::vector<int> &order, const std::vector<int> &rptr, const std::vector<int> &dpos,
-                           bool with_diag) {
-    std::vector<int> out;
-    out.reserve(order.size() * 4);
-    for (int i : order) {
-        out.push_back(i);
-        out.push_back(rptr[i]);
-        out.push_back(rptr[i + 1] - rptr[i]);
-        out.push_back(with_diag ? dpos[i] : 0);
-    }
-    return out;
-}
-
 std::vector<int> pack_pairs(const std::vector<int> &a, const std::vector<int> &b) {
     std::vector<int> out(2 * a.size());
     for (size_t i = 0; i < a.size(); ++i) {
@@ -279,28 +255,10 @@ int upload(pf_plan *pl) {
     size_t oyt = push(bi, P.ytarget), oyj = push(bi, P.yjpos);
     size_t ofill = push(bi, P.fillpos), ocpos = push(bi, P.cpos), ocj = push(bi, P.cjpos);
     size_t oxP = push(bi, P.xP), oxQ = push(bi, P.xQ), oxVa = push(bi, P.xVa), oxVm = push(bi, P.xVm);
-    std::vector<int> grp(4 * P.grp_lstart.size());
-    for (size_t g = 0; g < P.grp_lstart.size(); ++g) {
-        grp[4 * g] = P.grp_lstart[g];
-        grp[4 * g + 1] = P.grp_upos[g];
-        grp[4 * g + 2] = P.grp_dpos[g];
-        grp[4 * g + 3] = P.grp_dst[g];
-    }
-    std::vector<int> ph(4 * P.phases.size()), phl(P.phases.size());
-    for (size_t i = 0; i < P.phases.size(); ++i) {
-        ph[4 * i] = P.phases[i].gbeg;
-        ph[4 * i + 1] = P.phases[i].gend;
-        ph[4 * i + 2] = P.phases[i].dbeg;
-        ph[4 * i + 3] = P.phases[i].dend;
-        phl[i] = P.phases[i].lanes;
-    }
-    size_t ogrp = push(bi, grp), oglc = push(bi, P.grp_lcount), odst = push(bi, P.dst);
-    size_t oph = push(bi, ph), ophl = push(bi, phl), odiv = push(bi, pack_pairs(P.div_pos, P.div_dpos));
+    size_t ofo = push(bi, P.factor.ops), ofb = push(bi, P.factor.base), ofw = push(bi, P.factor.width);
+    size_t obo = push(bi, P.backward.ops), obb = push(bi, P.backward.base), obw = push(bi, P.backward.width);
+    size_t owo = push(bi, P.forward.ops), owb = push(bi, P.forward.base), oww = push(bi, P.forward.width);
     size_t odpos = push(bi, P.dpos);
-    size_t ofd = push(bi, pack_rows(P.fwd_order, P.lrow_ptr, P.dpos, false));
-    size_t obd = push(bi, pack_rows(P.bwd_order, P.urow_ptr, P.dpos, true));
-    size_t olpc = push(bi, pack_pairs(P.lrow_pos, P.lrow_col)), oupc = push(bi, pack_pairs(P.urow_pos, P.urow_col));
-    size_t ofg = push(bi, flat_groups(P.fwd_groups)), obg = push(bi, flat_groups(P.bwd_groups));
     std::vector<double> rx(2 * (size_t)P.nnzY);
     for (int i = 0; i < P.nnzY; ++i) {
         rx[2 * i] = P.Rx[i].real();
@@ -328,7 +286,6 @@ int upload(pf_plan *pl) {
     if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: upload");
     unsigned char *bI = static_cast<unsigned char *>(pl->d_int), *bD = static_cast<unsigned char *>(pl->d_dbl);
     auto I = [&](size_t o) { return reinterpret_cast<const int *>(bI + o); };
-    auto I2 = [&](size_t o) { return reinterpret_cast<const int2 *>(bI + o); };
     auto I4 = [&](size_t o) { return reinterpret_cast<const int4 *>(bI + o); };
     auto D = [&](size_t o) { return reinterpret_cast<const double *>(bD + o); };
     l2g::DevPlan &d = pl->dp;
@@ -356,22 +313,19 @@ int upload(pf_plan *pl) {
     d.xVm = I(oxVm);
     d.xSlack = P.xSlack;
     d.wJ = D(owJ);
-    d.grp = I4(ogrp);
-    d.grp_lc = I(oglc);
-    d.dst = I(odst);
-    d.phases = I4(oph);
-    d.ph_lanes = I(ophl);
-    d.nphases = (int)P.phases.size();
-    d.divs = I2(odiv);
+    d.fac_ops = I4(ofo);
+    d.fac_base = I(ofb);
+    d.fac_width = I(ofw);
+    d.bwd_width = I(obw);
+    d.fwd_width = I(oww);
+    d.fac_nph = P.factor.nphases();
+    d.bwd_ops = I4(obo);
+    d.bwd_base = I(obb);
+    d.bwd_nph = P.backward.nphases();
+    d.fwd_ops = I4(owo);
+    d.fwd_base = I(owb);
+    d.fwd_nph = P.forward.nphases();
     d.dpos = I(odpos);
-    d.fwd_desc = I4(ofd);
-    d.bwd_desc = I4(obd);
-    d.lrow_pc = I2(olpc);
-    d.urow_pc = I2(oupc);
-    d.fwd_groups = I4(ofg);
-    d.bwd_groups = I4(obg);
-    d.nfwd = (int)P.fwd_groups.size();
-    d.nbwd = (int)P.bwd_groups.size();
     return 0;
 }
 
@@ -386,10 +340,7 @@ int configure(pf_plan *pl) {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, pl->device);
     pl->precision = pl->opt.precision ? 1 : 0;
-    int thr = pl->opt.threads;
-    if (thr <= 0) thr = P.m > 2000 ? 512 : (P.m > 300 ? 256 : 128);
-    thr = std::max(32, std::min(512, (thr / 32) * 32));
-    pl->threads = thr;
+    const int thr = pl->threads;
     const int lub = pl->precision ? 4 : 8, xb = pl->precision ? 4 : 8;
     const size_t static_smem = 2048;  // Shared struct of the kernel, rounded up
     size_t sm_in = l2g::smem_bytes(pl->dp, lub, xb, true);
@@ -416,7 +367,7 @@ int configure(pf_plan *pl) {
 
 void release(pf_plan *pl) {
     for (DevBuf *b : {&pl->scratch, &pl->counter, &pl->V0, &pl->Sbus, &pl->optr, &pl->opos, &pl->oval,
-                      &pl->jfirst, &pl->jcount, &pl->Vout, &pl->iters, &pl->errs, &pl->Jout})
+                      &pl->jfirst, &pl->jcount, &pl->Vout, &pl->iters, &pl->errs, &pl->Jout, &pl->cycles})
         b->release();
     if (pl->d_int) cudaFree(pl->d_int);
     if (pl->d_dbl) cudaFree(pl->d_dbl);
@@ -435,6 +386,7 @@ int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
     a.job_counter = static_cast<int *>(pl->counter.p);
     a.lu_in_smem = pl->lu_in_smem ? 1 : 0;
     a.refine = (precision == 1 && pl->refine) ? 1 : 0;
+    a.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
     if (a.njobs <= 0) return 0;
     cudaError_t e = cudaMemsetAsync(pl->counter.p, 0, sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
@@ -611,7 +563,15 @@ int pf_plan_create(int n, const int *colptr, const int *rowind, const double *yb
     if (opts) pl->opt = *opts;
     l2g::PlanOptions po;
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
-    if (pl->opt.chain_max_items > 0) po.chain_max_items = pl->opt.chain_max_items;
+    {
+        const int m_est = npv + (distributed && nslack > 1 ? nslack - 1 : 0) + 2 * npq + (distributed ? 1 : 0);
+        int thr = pl->opt.threads;
+        if (thr <= 0) thr = m_est > 2000 ? 512 : (m_est > 300 ? 256 : 128);
+        thr = std::max(32, std::min(512, (thr / 32) * 32));
+        po.threads = thr;
+        pl->threads = thr;
+    }
+    po.fuse_forward = pl->opt.fuse_forward != 2;
     std::string msg;
     int rc;
     try {
@@ -664,9 +624,9 @@ int pf_plan_info_get(const pf_plan *pl, pf_plan_info *info) {
     info->levels_refactor = P.levels_refactor;
     info->levels_forward = P.levels_fwd;
     info->levels_backward = P.levels_bwd;
-    info->groups_refactor = (int)P.phases.size();
-    info->groups_forward = (int)P.fwd_groups.size();
-    info->groups_backward = (int)P.bwd_groups.size();
+    info->groups_refactor = P.factor.nphases();
+    info->groups_forward = P.forward.nphases();
+    info->groups_backward = P.backward.nphases();
     info->flops_refactor = P.flops_refactor;
     info->precision = pl->precision;
     info->threads = pl->threads;
@@ -859,8 +819,7 @@ int pf_batch_ts(pf_plan *pl, int nsteps, const double *Sbus_ri, const double *V0
     return 0;
 }
 
-int pf_batch_device(pf_plan *pl, const pf_device_batch *b, void *stream) {
-    if (!pl || !b) return fail(-1, "pf_batch_device: null argument");
+static l2g::BatchArgs device_args(const pf_device_batch *b) {
     l2g::BatchArgs a{};
     a.n_inst = b->n_inst;
     a.V0 = static_cast<const double2 *>(b->V0);
@@ -881,7 +840,62 @@ int pf_batch_device(pf_plan *pl, const pf_device_batch *b, void *stream) {
     a.errs = b->errs;
     a.Jout = nullptr;
     a.j_inst = -1;
+    return a;
+}
+
+static int batch_device_impl(pf_plan *pl, const pf_device_batch *b, void *stream, unsigned long long *cycles) {
+    l2g::BatchArgs a = device_args(b);
+    a.phase_cycles = cycles;
     return launch(pl, a, pl->precision, static_cast<cudaStream_t>(stream));
+}
+
+int pf_batch_device(pf_plan *pl, const pf_device_batch *b, void *stream) {
+    if (!pl || !b) return fail(-1, "pf_batch_device: null argument");
+    return batch_device_impl(pl, b, stream, nullptr);
+}
+
+int pf_batch_device_phase_trace(pf_plan *pl, const pf_device_batch *b, void *stream, double *out, int cap) {
+    if (!pl || !b || !out || cap <= 0) return fail(-1, "pf_batch_device_phase_trace: null argument");
+    cudaError_t e = pl->cycles.ensure((size_t)cap * sizeof(unsigned long long));
+    if (e != cudaSuccess) return cuda_fail(e, "pf_batch_device_phase_trace: alloc");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    e = cudaMemsetAsync(pl->cycles.p, 0, (size_t)cap * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_batch_device_phase_trace: memset");
+    l2g::BatchArgs a = device_args(b);
+    a.trace = static_cast<unsigned long long *>(pl->cycles.p);
+    a.trace_cap = cap;
+    int rc = launch(pl, a, pl->precision, st);
+    if (rc) return rc;
+    std::vector<unsigned long long> h(cap);
+    e = cudaMemcpyAsync(h.data(), pl->cycles.p, (size_t)cap * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_batch_device_phase_trace: download");
+    int n = 0;
+    while (n < cap && h[n] != 0) ++n;
+    for (int i = 0; i < n; ++i) out[i] = i == 0 ? 0.0 : (double)(h[i] - h[0]);
+    return n;
+}
+
+int pf_batch_device_phase_cycles(pf_plan *pl, const pf_device_batch *b, void *stream, double *out) {
+    if (!pl || !b || !out) return fail(-1, "pf_batch_device_phase_cycles: null argument");
+    const size_t slots = (size_t)pl->grid * l2g::kPhaseSlots;
+    cudaError_t e = pl->cycles.ensure(slots * sizeof(unsigned long long));
+    if (e != cudaSuccess) return cuda_fail(e, "pf_batch_device_phase_cycles: alloc");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    e = cudaMemsetAsync(pl->cycles.p, 0, slots * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_batch_device_phase_cycles: memset");
+    int rc = batch_device_impl(pl, b, stream, static_cast<unsigned long long *>(pl->cycles.p));
+    if (rc) return rc;
+    std::vector<unsigned long long> h(slots);
+    e = cudaMemcpyAsync(h.data(), pl->cycles.p, slots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_batch_device_phase_cycles: download");
+    for (int i = 0; i < l2g::kPhaseSlots; ++i) {
+        double acc = 0.0;
+        for (int b2 = 0; b2 < pl->grid; ++b2) acc += (double)h[(size_t)b2 * l2g::kPhaseSlots + i];
+        out[i] = acc;
+    }
+    return 0;
 }
 
 int pf_timers(const pf_plan *pl, double *out, int nout) {
@@ -936,34 +950,45 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
     for (int p : P.fillpos) { lu[p] = 0.0; seen[p] = 1; }
     for (int p = 0; p < P.nnzLU; ++p)
         if (!seen[p]) return fail(-1, "schedule check: an LU position is never written by the fill");
-    // refactorisation in the device's phase order (each phase's work is order independent)
-    for (const auto &Q : P.phases) {
-        for (int e = Q.dbeg; e < Q.dend; ++e) lu[P.div_pos[e]] /= lu[P.div_dpos[e]];
-        for (int g = Q.gbeg; g < Q.gend; ++g) {
-            double f = lu[P.grp_upos[g]] / lu[P.grp_dpos[g]];
-            for (int s2 = 0; s2 < P.grp_lcount[g]; ++s2)
-                lu[P.dst[P.grp_dst[g] + s2]] -= lu[P.grp_lstart[g] + s2] * f;
-        }
-    }
-    for (int k = 0; k < m; ++k)
-        if (lu[P.dpos[k]] == 0.0) return fail(l2g::SolverReFactor, "schedule check: zero pivot");
     // permuted right-hand side, as the device mismatch writes it
     std::vector<double> xs(m, 0.0);
     for (int f = 0; f < m; ++f) xs[P.pinv[f]] = b[f];
-    for (const auto &G : P.fwd_groups)
-        for (int t = G.begin; t < G.end; ++t) {
-            int i = P.fwd_order[t];
-            double s = 0.0;
-            for (int e = P.lrow_ptr[i]; e < P.lrow_ptr[i + 1]; ++e) s += lu[P.lrow_pos[e]] * xs[P.lrow_col[e]];
-            xs[i] -= s;
+    // the device's phase programs, one operation after the other (a phase's operations are
+    // independent, so any order gives the device's result)
+    auto run = [&](const l2g::Plan::Program &pr) {
+        for (int o = 0; o < pr.nops(); ++o) {
+            const int X = pr.ops[4 * o], Y = pr.ops[4 * o + 1], Z = pr.ops[4 * o + 2];
+            const int W = pr.ops[4 * o + 3] & 0x0fffffff, kind = (unsigned)pr.ops[4 * o + 3] >> 28;
+            switch (kind) {
+                case 0: lu[X] -= lu[Y] * (lu[Z] / lu[W]); break;
+                case 1: lu[X] = lu[X] / lu[W]; break;
+                case 2: xs[X] -= lu[Y] * xs[Z] / lu[W]; break;
+                case 3: xs[X] -= lu[Y] * xs[Z]; break;
+                case 4: xs[X] = xs[X] / lu[W]; break;
+                default: break;
+            }
         }
-    for (const auto &G : P.bwd_groups)
-        for (int t = G.begin; t < G.end; ++t) {
-            int i = P.bwd_order[t];
-            double s = 0.0;
-            for (int e = P.urow_ptr[i]; e < P.urow_ptr[i + 1]; ++e) s += lu[P.urow_pos[e]] * xs[P.urow_col[e]];
-            xs[i] = (xs[i] - s) / lu[P.dpos[i]];
+    };
+    run(P.factor);
+    for (int k = 0; k < m; ++k)
+        if (lu[P.dpos[k]] == 0.0) return fail(l2g::SolverReFactor, "schedule check: zero pivot");
+    run(P.backward);
+    // the stand-alone forward program must agree with the fused one: solve L y = b again
+    {
+        std::vector<double> y2(m, 0.0), keep = xs;
+        for (int f = 0; f < m; ++f) y2[P.pinv[f]] = b[f];
+        xs = y2;
+        run(P.forward);
+        run(P.backward);
+        double dmax = 0.0, amax = 0.0;
+        for (int k = 0; k < m; ++k) {
+            dmax = std::max(dmax, std::fabs(xs[k] - keep[k]));
+            amax = std::max(amax, std::fabs(keep[k]));
         }
+        if (dmax > 1e-9 * std::max(1.0, amax))
+            return fail(-1, "schedule check: fused and stand-alone forward substitutions disagree");
+        xs = keep;
+    }
     for (int v = 0; v < m; ++v) x[v] = xs[P.qinv[v]];
     if (info) {
         std::memset(info, 0, sizeof(*info));
@@ -975,9 +1000,9 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         info->levels_refactor = P.levels_refactor;
         info->levels_forward = P.levels_fwd;
         info->levels_backward = P.levels_bwd;
-        info->groups_refactor = (int)P.phases.size();
-        info->groups_forward = (int)P.fwd_groups.size();
-        info->groups_backward = (int)P.bwd_groups.size();
+        info->groups_refactor = P.factor.nphases();
+        info->groups_forward = P.forward.nphases();
+        info->groups_backward = P.backward.nphases();
         info->flops_refactor = P.flops_refactor;
     }
     return 0;

@@ -9,13 +9,12 @@
 //   solve      forward / backward substitution                 (KLUSolver.cpp:61-69 contract)
 //   update     Va, Vm, V and the convergence test              BaseNRSingleSlackAlgo.tpp:129-162,
 //                                                              BaseNRAlgo.tpp:136-167
-// Refactorisation: right-looking by elimination level; the update groups (pivot c, column j)
-// of a level are spread over the CTA's threads in conflict-free phases, one barrier per
-// phase, no atomics, so the result is deterministic.  Solves: row oriented and level
-// scheduled with 1..32 lanes per row; levels with one or two rows run as a chain on warp 0
-// with the next row's indices prefetched.  LU values live in shared memory when they fit,
-// else in the CTA's global slab (L2 resident).  The mixed form (FP32 LU) refines every
-// Newton step once against the FP64 Jacobian, computed on the fly from dS/dV.
+// The refactorisation (right-looking, by elimination level, with the forward substitution
+// of the right-hand side fused in) and the substitutions run as phase programs: flat lists
+// of independent operations, coloured on the host into conflict-free phases, one barrier
+// per phase, no atomics -- the result is deterministic.  LU values live in shared memory
+// when they fit, else in the CTA's global slab (L2 resident).  The mixed form (FP32 LU)
+// refines every Newton step once against the FP64 Jacobian, computed on the fly from dS/dV.
 #include "pf_engine.cuh"
 
 namespace l2g {
@@ -27,12 +26,6 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double cabs2(double2 a) { return sqrt(a.x * a.x + a.y * a.y); }
-
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v, int width) {
-    for (int o = width >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, width);
-    return v;
-}
 
 struct Shared {
     double red[32];
@@ -129,12 +122,23 @@ __device__ void mismatch(const DevPlan &P, Shared &S, const double2 *__restrict_
     const double sa = S.slack_absorbed;
     for (int r = threadIdx.x; r < P.n; r += blockDim.x) {
         double2 s = make_double2(0.0, 0.0);
-        const int p1 = P.Rp[r + 1];
-        for (int p = P.Rp[r]; p < p1; ++p) {
-            const double2 y = ybus_value(P, S, p);
-            const double2 v = V[P.Rj[p]];
-            s.x += y.x * v.x - y.y * v.y;
-            s.y += y.x * v.y + y.y * v.x;
+        const int p0 = P.Rp[r], p1 = P.Rp[r + 1];
+        for (int p = p0; p < p1; p += 4) {
+            // indices first, then values: the loads of four entries are in flight together
+            int c[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) c[u] = p + u < p1 ? P.Rj[p + u] : -1;
+            double2 y[4], vv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                y[u] = c[u] >= 0 ? ybus_value(P, S, p + u) : make_double2(0.0, 0.0);
+                vv[u] = c[u] >= 0 ? V[c[u]] : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                s.x += y[u].x * vv[u].x - y[u].y * vv[u].y;
+                s.y += y[u].x * vv[u].y + y[u].y * vv[u].x;
+            }
         }
         Ibus[r] = s;
         const double2 vr = V[r];
@@ -187,96 +191,101 @@ __device__ void jacobian_fill(const DevPlan &P, Shared &S, const double2 *__rest
     }
 }
 
-// Right-looking refactorisation in conflict-free phases; sets S.piv_err on a zero pivot.
-template <typename LT>
-__device__ void refactor(const DevPlan &P, Shared &S, LT *lu) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    for (int ph = 0; ph < P.nphases; ++ph) {
-        const int4 Q = P.phases[ph];
-        const int lanes = P.ph_lanes[ph];
-        for (int e = Q.z + tid; e < Q.w; e += nt) {
-            const int2 dv = P.divs[e];
-            lu[dv.x] = lu[dv.x] / lu[dv.y];
-        }
-        const int per_warp = 32 / lanes;
-        const int sub = lane & (lanes - 1);
-        const int nslots = nw * per_warp;
-        for (int g = Q.x + warp * per_warp + lane / lanes; g < Q.y; g += nslots) {
-            const int4 G = P.grp[g];
-            const int lc = P.grp_lc[g];
-            const LT f = lu[G.y] / lu[G.z];  // U(c, j) / U(c, c)
-            const int *d = P.dst + G.w;
-            for (int s = sub; s < lc; s += lanes) lu[d[s]] -= lu[G.x + s] * f;
-        }
-        __syncthreads();
+template <typename LT, typename XT>
+__device__ __forceinline__ void run_op(const int4 o, LT *lu, XT *v) {
+    const int kind = (unsigned)o.w >> 28;
+    const int w = o.w & 0x0fffffff;
+    switch (kind) {
+        case 0: lu[o.x] -= lu[o.y] * (lu[o.z] / lu[w]); break;
+        case 1: lu[o.x] = lu[o.x] / lu[w]; break;
+        case 2: v[o.x] -= (XT)lu[o.y] * v[o.z] / (XT)lu[w]; break;
+        case 3: v[o.x] -= (XT)lu[o.y] * v[o.z]; break;
+        case 4: v[o.x] = v[o.x] / (XT)lu[w]; break;
+        default: break;  // padding
     }
-    int zero = 0;
-    for (int k = tid; k < P.m; k += nt) zero |= lu[P.dpos[k]] == (LT)0;
-    if (zero) S.piv_err = 1;
-    __syncthreads();
 }
 
-// Row-oriented, level-scheduled substitution.  upper == false: x_i -= L(i,:) x (unit
-// diagonal); upper == true: x_i = (x_i - U(i,:) x) / U(i,i).
-template <typename LT, typename XT, bool upper>
-__device__ void tri_solve(const DevPlan &P, const LT *lu, XT *x) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int4 *desc = upper ? P.bwd_desc : P.fwd_desc;
-    const int2 *pc = upper ? P.urow_pc : P.lrow_pc;
-    const int4 *groups = upper ? P.bwd_groups : P.fwd_groups;
-    const int ng = upper ? P.nbwd : P.nfwd;
-    for (int g = 0; g < ng; ++g) {
-        const int4 G = groups[g];
-        if (G.z == 0) {
-            const int lanes = G.w;
-            const int per_warp = 32 / lanes;
-            const int sub = lane & (lanes - 1);
-            const int slot = lane / lanes;
-            for (int base = G.x + warp * per_warp; base < G.y; base += nw * per_warp) {
-                const int t = base + slot;
-                XT s = (XT)0;
-                int4 d = make_int4(-1, 0, 0, 0);
-                if (t < G.y) {
-                    d = desc[t];
-                    for (int e = sub; e < d.z; e += lanes) {
-                        const int2 q = pc[d.y + e];
-                        s += (XT)lu[q.x] * x[q.y];
-                    }
-                }
-                s = warp_sum(s, lanes);
-                if (d.x >= 0 && sub == 0) {
-                    if (upper) x[d.x] = (x[d.x] - s) / (XT)lu[d.w];
-                    else x[d.x] -= s;
-                }
-            }
-        } else if (warp == 0) {
-            // chain: one row after the other; the next row's descriptor and first 32
-            // entries are loaded while the current row is reduced
-            int4 dn = desc[G.x];
-            int2 qn = lane < dn.z ? pc[dn.y + lane] : make_int2(0, 0);
-            for (int t = G.x; t < G.y; ++t) {
-                const int4 d = dn;
-                const int2 q = qn;
-                if (t + 1 < G.y) {
-                    dn = desc[t + 1];
-                    qn = lane < dn.z ? pc[dn.y + lane] : make_int2(0, 0);
-                }
-                XT s = lane < d.z ? (XT)lu[q.x] * x[q.y] : (XT)0;
-                for (int e = lane + 32; e < d.z; e += 32) {
-                    const int2 q2 = pc[d.y + e];
-                    s += (XT)lu[q2.x] * x[q2.y];
-                }
-                s = warp_sum(s, 32);
-                if (lane == 0) {
-                    if (upper) x[d.x] = (x[d.x] - s) / (XT)lu[d.w];
-                    else x[d.x] -= s;
-                }
-                __syncwarp();
-            }
+// Runs a phase program: one barrier per phase.  In phase p, thread t < sw[p] runs the
+// operations sb[p] + t, sb[p] + t + sw[p], ... (bounds and widths staged in shared memory).
+//
+// Latency hiding: a thread holds the first two operations of the current phase and of the
+// next one in registers and loads those of the next-but-one phase while it works; inside a
+// phase it loads two operations ahead.  A register that still waits for its load must not
+// be copied (the copy would stall on the load), so the three register pairs rotate roles
+// through a loop unrolled by three, and inside a phase each register is reloaded right
+// after its operation has consumed it.
+struct OpPair {
+    int4 a, b;
+};
+
+template <typename LT, typename XT>
+__device__ __forceinline__ void load_first2(const int4 *__restrict__ ops, const int *sb, const int *sw, int nph,
+                                            int p, OpPair &r) {
+    r.a = make_int4(0, 0, 0, 7 << 28);
+    r.b = r.a;
+    if (p < nph) {
+        const int w = sw[p];
+        if ((int)threadIdx.x < w) {
+            const int k = sb[p] + threadIdx.x, e = sb[p + 1];
+            if (k < e) r.a = ops[k];
+            if (k + w < e) r.b = ops[k + w];
         }
-        __syncthreads();
     }
+}
+
+struct Trace {
+    unsigned long long *buf;
+    int cap, n;
+    __device__ __forceinline__ void mark() {
+        if (buf != nullptr && threadIdx.x == 0 && n < cap) buf[n++] = clock64();
+    }
+};
+
+template <typename LT, typename XT>
+__device__ __forceinline__ void run_phase(const int4 *__restrict__ ops, const int *sb, const int *sw, int nph,
+                                          int p, OpPair &cur, OpPair &pre, LT *lu, XT *v, Trace &tr) {
+    load_first2<LT, XT>(ops, sb, sw, nph, p + 2, pre);
+    const int w = sw[p];
+    if ((int)threadIdx.x < w) {
+        const int e = sb[p + 1];
+        int k = sb[p] + threadIdx.x;
+        for (;;) {
+            if (k >= e) break;
+            run_op<LT, XT>(cur.a, lu, v);
+            if (k + 2 * w < e) cur.a = ops[k + 2 * w];
+            k += w;
+            if (k >= e) break;
+            run_op<LT, XT>(cur.b, lu, v);
+            if (k + 2 * w < e) cur.b = ops[k + 2 * w];
+            k += w;
+        }
+    }
+    __syncthreads();
+    tr.mark();
+}
+
+template <typename LT, typename XT>
+__device__ void run_program(const int4 *__restrict__ ops, const int *sb, const int *sw, int nph, LT *lu, XT *v,
+                            Trace &tr) {
+    if (nph <= 0) return;
+    OpPair A, B, C;
+    load_first2<LT, XT>(ops, sb, sw, nph, 0, A);
+    load_first2<LT, XT>(ops, sb, sw, nph, 1, B);
+    for (int p = 0; p < nph; p += 3) {
+        run_phase<LT, XT>(ops, sb, sw, nph, p, A, C, lu, v, tr);
+        if (p + 1 >= nph) break;
+        run_phase<LT, XT>(ops, sb, sw, nph, p + 1, B, A, lu, v, tr);
+        if (p + 2 >= nph) break;
+        run_phase<LT, XT>(ops, sb, sw, nph, p + 2, C, B, lu, v, tr);
+    }
+}
+
+template <typename LT>
+__device__ void check_pivots(const DevPlan &P, Shared &S, const LT *lu) {
+    int zero = 0;
+    for (int k = threadIdx.x; k < P.m; k += blockDim.x) zero |= lu[P.dpos[k]] == (LT)0;
+    if (zero) S.piv_err = 1;
+    __syncthreads();
 }
 
 // FP64 residual of the Newton system, F - J dx, written as the next right-hand side.
@@ -328,6 +337,31 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
     double *dxg = Va + n;
     const size_t bus_bytes = (((size_t)n * 64 + (size_t)m * 8) + 255) & ~(size_t)255;
     LT *lu = LU_SMEM ? reinterpret_cast<LT *>(dyn + xbytes) : reinterpret_cast<LT *>(slab + bus_bytes);
+    // phase bounds of the three programs, staged once per launch
+    int *sb_fac = reinterpret_cast<int *>(dyn + xbytes + (LU_SMEM ? (((size_t)P.nnzLU * sizeof(LT) + 15) & ~(size_t)15) : 0));
+    int *sb_bwd = sb_fac + P.fac_nph + 1;
+    int *sb_fwd = sb_bwd + P.bwd_nph + 1;
+    int *sw_fac = sb_fwd + P.fwd_nph + 1;
+    int *sw_bwd = sw_fac + P.fac_nph;
+    int *sw_fwd = sw_bwd + P.bwd_nph;
+    for (int i = tid; i <= P.fac_nph; i += blockDim.x) sb_fac[i] = P.fac_base[i];
+    for (int i = tid; i <= P.bwd_nph; i += blockDim.x) sb_bwd[i] = P.bwd_base[i];
+    for (int i = tid; i <= P.fwd_nph; i += blockDim.x) sb_fwd[i] = P.fwd_base[i];
+    for (int i = tid; i < P.fac_nph; i += blockDim.x) sw_fac[i] = P.fac_width[i];
+    for (int i = tid; i < P.bwd_nph; i += blockDim.x) sw_bwd[i] = P.bwd_width[i];
+    for (int i = tid; i < P.fwd_nph; i += blockDim.x) sw_fwd[i] = P.fwd_width[i];
+    __syncthreads();
+    // per-phase SM cycles, measured by thread 0 between the barriers that end each phase
+    unsigned long long pc[kPhaseSlots] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const bool prof = A.phase_cycles != nullptr && tid == 0;
+    int traced = 0;
+    unsigned long long tmark = prof ? clock64() : 0;
+#define L2G_MARK(slot)                                  \
+    if (prof) {                                          \
+        const unsigned long long t_ = clock64();        \
+        pc[slot] += t_ - tmark;                         \
+        tmark = t_;                                     \
+    }
 
     for (;;) {
         if (tid == 0) S.job = atomicAdd(A.job_counter, 1);
@@ -379,28 +413,39 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
             __syncthreads();
             double norm;
             int bad;
+            L2G_MARK(6);
             mismatch<XT>(P, S, V, Ibus, Fbus, Sb, x, norm, bad);
+            L2G_MARK(0);
             bool conv = !bad && norm < A.tol;
             int it = 0, err = 0;
             double *Jout = (A.Jout && inst == A.j_inst) ? A.Jout : nullptr;
+            Trace tr{(A.trace != nullptr && blockIdx.x == 0 && traced == 0) ? A.trace : nullptr, A.trace_cap, 0};
+            traced = 1;
             while (!conv && it < A.max_iter) {
                 ++it;
                 jacobian_fill<LT>(P, S, V, Ibus, lu, Jout);
                 __syncthreads();
-                refactor<LT>(P, S, lu);
+                L2G_MARK(1);
+                // refactorisation with the forward substitution of the right-hand side fused in
+                const bool refine_now = REFINE && norm < A.refine_below;
+                tr.mark();
+                run_program<LT, XT>(P.fac_ops, sb_fac, sw_fac, P.fac_nph, lu, x, tr);
+                check_pivots<LT>(P, S, lu);
+                L2G_MARK(2);
                 if (S.piv_err) {
                     err = 6;  // SolverReFactor
                     break;
                 }
-                tri_solve<LT, XT, false>(P, lu, x);
-                tri_solve<LT, XT, true>(P, lu, x);
-                if (REFINE) {
+                run_program<LT, XT>(P.bwd_ops, sb_bwd, sw_bwd, P.bwd_nph, lu, x, tr);
+                L2G_MARK(4);
+                if (refine_now) {
                     for (int k = tid; k < m; k += blockDim.x) dxg[k] = (double)x[k];
                     __syncthreads();
                     newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, x);
                     __syncthreads();
-                    tri_solve<LT, XT, false>(P, lu, x);
-                    tri_solve<LT, XT, true>(P, lu, x);
+                    run_program<LT, XT>(P.fwd_ops, sb_fwd, sw_fwd, P.fwd_nph, lu, x, tr);
+                    run_program<LT, XT>(P.bwd_ops, sb_bwd, sw_bwd, P.bwd_nph, lu, x, tr);
+                    L2G_MARK(5);
                 }
                 // voltage update
                 double lmin = 1.0;
@@ -415,8 +460,8 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
                         va = atan2(v.y, v.x);
                     }
                     const int ia = P.xVa[b], im = P.xVm[b];
-                    if (ia >= 0) va -= REFINE ? dxg[ia] + (double)x[ia] : (double)x[ia];
-                    if (im >= 0) vm -= REFINE ? dxg[im] + (double)x[im] : (double)x[im];
+                    if (ia >= 0) va -= refine_now ? dxg[ia] + (double)x[ia] : (double)x[ia];
+                    if (im >= 0) vm -= refine_now ? dxg[im] + (double)x[im] : (double)x[im];
                     double sn, cs;
                     sincos(va, &sn, &cs);
                     V[b] = make_double2(vm * cs, vm * sn);
@@ -426,7 +471,7 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
                 }
                 if (P.distributed) {
                     const double dxs =
-                        REFINE ? dxg[P.xSlack] + (double)x[P.xSlack] : (double)x[P.xSlack];
+                        refine_now ? dxg[P.xSlack] + (double)x[P.xSlack] : (double)x[P.xSlack];
                     const double vmin = block_min(S, lmin);  // contains barriers
                     if (tid == 0) S.slack_absorbed -= dxs;
                     if (vmin < 0.0) {
@@ -438,7 +483,11 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
                     }
                 }
                 __syncthreads();
+                tr.mark();
+                tr.buf = nullptr;
+                L2G_MARK(6);
                 mismatch<XT>(P, S, V, Ibus, Fbus, Sb, x, norm, bad);
+                L2G_MARK(0);
                 if (bad) {
                     err = 3;  // InifiniteValue
                     break;
@@ -451,6 +500,7 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
             if (tid == 0) {
                 A.iters[inst] = it;
                 A.errs[inst] = err;
+                pc[7] += 1;
             }
             __syncthreads();
             if (A.chain && err != 0) {
@@ -464,6 +514,9 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
         }
         __syncthreads();
     }
+    if (prof)
+        for (int i = 0; i < kPhaseSlots; ++i) A.phase_cycles[(size_t)blockIdx.x * kPhaseSlots + i] = pc[i];
+#undef L2G_MARK
 }
 
 template <typename LT, typename XT, bool SM, bool RF>
@@ -498,7 +551,9 @@ size_t slab_bytes(const DevPlan &P, int lu_bytes, bool lu_in_smem) {
 
 size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem) {
     size_t xb = ((size_t)P.m * x_bytes + 15) & ~(size_t)15;
-    return xb + (lu_in_smem ? (size_t)P.nnzLU * lu_bytes : 0);
+    size_t lb = lu_in_smem ? (((size_t)P.nnzLU * lu_bytes + 15) & ~(size_t)15) : 0;
+    size_t bb = (size_t)(2 * (P.fac_nph + P.bwd_nph + P.fwd_nph) + 3) * sizeof(int);
+    return xb + lb + bb;
 }
 
 cudaError_t launch_nr_batch(const DevPlan &P, const BatchArgs &A, int precision, int threads, int grid,

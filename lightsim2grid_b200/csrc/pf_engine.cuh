@@ -24,20 +24,13 @@ struct DevPlan {
     const int *xP, *xQ, *xVa, *xVm;
     int xSlack;
     const double *wJ;        // distributed slack: J(P(r), 0) per bus (0 if none)
-    // right-looking refactorisation
-    const int4 *grp;         // per update group: L(:,c) start, U(c,j) position, pivot position, dst offset
-    const int *grp_lc;       // per update group: rows of L(:,c)
-    const int *dst;
-    const int4 *phases;      // group range, division range
-    const int *ph_lanes;
-    int nphases;
-    const int2 *divs;        // (L entry, pivot) per division
+    // phase programs (see pf_plan.hpp): operations as int4 (x, y, z, w | kind << 28) and
+    // phase boundaries; factor includes the forward substitution of the right-hand side
+    const int4 *fac_ops, *bwd_ops, *fwd_ops;
+    const int *fac_base, *bwd_base, *fwd_base;
+    const int *fac_width, *bwd_width, *fwd_width;
+    int fac_nph, bwd_nph, fwd_nph;
     const int *dpos;         // pivot position per column (m)
-    // triangular solves: rows in level order as (row, first entry, entries, diagonal)
-    const int4 *fwd_desc, *bwd_desc;
-    const int2 *lrow_pc, *urow_pc;  // (LU position, column) per entry
-    const int4 *fwd_groups, *bwd_groups;
-    int nfwd, nbwd;
 };
 
 // One batch launch.
@@ -66,7 +59,16 @@ struct BatchArgs {
     long long slab_bytes;
     int lu_in_smem;
     int refine;               // FP32 LU only: one FP64-residual refinement of every Newton step
+    double refine_below;      // ... taken when ||F||_inf before the step is below this
+    unsigned long long *phase_cycles;  // optional, kPhaseSlots per CTA: SM cycles per phase
+    unsigned long long *trace;         // optional: CTA 0, first Newton iteration of its first
+                                       // instance: clock after every phase of every program
+    int trace_cap;
 };
+
+// phase_cycles slots: mismatch, J fill, refactorisation, forward, backward, refinement,
+// update, instances
+constexpr int kPhaseSlots = 8;
 
 constexpr int kMaxOverrides = 32;
 

@@ -80,53 +80,80 @@ std::vector<int> minimum_degree(int m, const std::vector<int> &Ap, const std::ve
     return order;
 }
 
-int lanes_for(int maxlen) {
-    if (maxlen <= 2) return 1;
-    if (maxlen <= 4) return 2;
-    if (maxlen <= 8) return 4;
-    if (maxlen <= 16) return 8;
-    if (maxlen <= 32) return 16;
-    return 32;
-}
+// Builds one phase program, level after level.  All operations of a level that write the
+// same value form a cluster and run on one thread, in the order they were added (so there
+// are no write conflicts, no atomics and a deterministic summation order); clusters are
+// spread over the threads longest-first onto the least loaded thread.  A phase is stored
+// with stride `width` (threads that have work): thread t < width runs operations
+// base + t, base + t + width, ...; shorter threads are padded with empty operations.
+struct ProgramBuilder {
+    Plan::Program &prog;
+    int nt;
+    std::vector<int> ops;          // 4 ints per operation of the current level
+    std::vector<long long> key;    // written value: space (0 lu, 1 v) and index
 
-// Groups items by level: each level becomes a wide group, except runs of consecutive
-// levels with at most `chain_max` items, which become one chain group.
-void make_groups(const std::vector<int> &level, const std::vector<int> &itemlen, int chain_max,
-                 std::vector<int> &order, std::vector<LevelGroup> &groups, int &nlevels, bool solve) {
-    int m = (int)level.size();
-    nlevels = 0;
-    for (int v : level) nlevels = std::max(nlevels, v + 1);
-    std::vector<int> cnt(nlevels + 1, 0);
-    for (int v : level) cnt[v + 1]++;
-    for (int l = 0; l < nlevels; ++l) cnt[l + 1] += cnt[l];
-    order.assign(m, 0);
-    std::vector<int> fillp(cnt.begin(), cnt.end() - 1);
-    for (int i = 0; i < m; ++i) order[fillp[level[i]]++] = i;
-    // within a level, longest items first (better balance of the round-robin)
-    for (int l = 0; l < nlevels; ++l)
-        std::stable_sort(order.begin() + cnt[l], order.begin() + cnt[l + 1],
-                         [&](int a, int b) { return itemlen[a] > itemlen[b]; });
-    groups.clear();
-    int l = 0;
-    while (l < nlevels) {
-        int sz = cnt[l + 1] - cnt[l];
-        if (sz <= chain_max) {
-            int l2 = l;
-            int maxlen = 0;
-            while (l2 < nlevels && cnt[l2 + 1] - cnt[l2] <= chain_max) {
-                for (int t = cnt[l2]; t < cnt[l2 + 1]; ++t) maxlen = std::max(maxlen, itemlen[order[t]]);
-                ++l2;
-            }
-            groups.push_back({cnt[l], cnt[l2], 1, solve ? lanes_for(maxlen) : 32});
-            l = l2;
-        } else {
-            int maxlen = 0;
-            for (int t = cnt[l]; t < cnt[l + 1]; ++t) maxlen = std::max(maxlen, itemlen[order[t]]);
-            groups.push_back({cnt[l], cnt[l + 1], 0, solve ? lanes_for(maxlen) : 32});
-            ++l;
-        }
+    ProgramBuilder(Plan::Program &p, int threads) : prog(p), nt(threads) {
+        prog.ops.clear();
+        prog.base.assign(1, 0);
+        prog.width.clear();
     }
-}
+    void begin() {
+        ops.clear();
+        key.clear();
+    }
+    void add(int x, int y, int z, int w, int kind) {
+        ops.push_back(x);
+        ops.push_back(y);
+        ops.push_back(z);
+        ops.push_back(w | (kind << 28));
+        key.push_back(((long long)(kind == 0 ? 0 : 1) << 32) | (long long)x);
+    }
+    void end() {
+        const int n = (int)key.size();
+        if (n == 0) return;
+        std::vector<int> idx(n);
+        for (int i = 0; i < n; ++i) idx[i] = i;
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return key[a] < key[b]; });
+        struct Cl { int first, count; };
+        std::vector<Cl> cl;
+        for (int i = 0; i < n;) {
+            int j = i;
+            while (j < n && key[idx[j]] == key[idx[i]]) ++j;
+            cl.push_back({i, j - i});
+            i = j;
+        }
+        std::stable_sort(cl.begin(), cl.end(), [](const Cl &a, const Cl &b) { return a.count > b.count; });
+        const int width = std::min<int>(nt, (int)cl.size());
+        std::vector<std::vector<int>> per(width);
+        std::vector<std::pair<int, int>> heap;  // (load, thread), min-heap
+        for (int t = 0; t < width; ++t) heap.push_back({0, t});
+        auto cmp = [](const std::pair<int, int> &a, const std::pair<int, int> &b) {
+            return a.first != b.first ? a.first > b.first : a.second > b.second;
+        };
+        std::make_heap(heap.begin(), heap.end(), cmp);
+        for (const Cl &c : cl) {
+            std::pop_heap(heap.begin(), heap.end(), cmp);
+            auto &h = heap.back();
+            for (int q = 0; q < c.count; ++q) per[h.second].push_back(idx[c.first + q]);
+            h.first += c.count;
+            std::push_heap(heap.begin(), heap.end(), cmp);
+        }
+        int len = 0;
+        for (auto &v : per) len = std::max(len, (int)v.size());
+        for (int j = 0; j < len; ++j)
+            for (int t = 0; t < width; ++t) {
+                if (j < (int)per[t].size()) {
+                    const int o = per[t][j];
+                    prog.ops.insert(prog.ops.end(), ops.begin() + 4 * o, ops.begin() + 4 * o + 4);
+                } else {
+                    const int none[4] = {0, 0, 0, 7 << 28};
+                    prog.ops.insert(prog.ops.end(), none, none + 4);
+                }
+            }
+        prog.width.push_back(width);
+        prog.base.push_back((int)(prog.ops.size() / 4));
+    }
+};
 
 }  // namespace
 
@@ -434,155 +461,118 @@ int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, con
         for (int t = 0; t < P.lcount[k]; ++t) P.Urow_k[P.lstart[k] + t] = Lrows[k][t];
     }
 
-    // ---------------------------------------------------------------- refactorisation schedule
-    // levels: a pivot can be applied once every pivot updating its column is done
-    std::vector<int> level(m, 0);
-    P.flops_refactor = 0;
-    for (int k = 0; k < m; ++k) {
-        int lv = 0;
-        for (int c : Ucols[k]) lv = std::max(lv, level[c] + 1);
-        level[k] = lv;
-        for (int c : Ucols[k]) P.flops_refactor += P.lcount[c];
+    // ---------------------------------------------------------------- phase programs
+    if (P.nnzLU >= (1 << 28) || m >= (1 << 28)) {
+        msg = "build_plan: LU too large for the operation encoding";
+        return SolverAnalyze;
     }
-    P.colleve = level;
-    int nlev = 0;
-    for (int v : level) nlev = std::max(nlev, v + 1);
-    P.levels_refactor = nlev;
     // U row lists: for pivot c, the columns j > c with U(c, j) != 0 and the position of U(c, j)
     std::vector<std::vector<std::pair<int, int>>> urows(m);
     for (int k = 0; k < m; ++k)
         for (size_t t = 0; t < Ucols[k].size(); ++t) urows[Ucols[k][t]].push_back({k, P.colstart[k] + (int)t});
-    std::vector<std::vector<int>> bylevel(nlev);
-    for (int k = 0; k < m; ++k) bylevel[level[k]].push_back(k);
-    std::vector<int> rowpos(m, -1);
-    std::vector<uint64_t> used(P.nnzLU, 0);  // phases of the current level writing an entry
-    std::vector<int> used_level(P.nnzLU, -1);
-    std::vector<int> pend_div;               // pivots whose divisions are pending
-    for (int l = 0; l < nlev; ++l) {
-        // the groups of this level
-        struct G { int c, j, upos; };
-        std::vector<G> gs;
-        for (int c : bylevel[l])
-            for (auto &e : urows[c]) gs.push_back({c, e.first, e.second});
-        // greedy colouring into conflict-free phases (first fit in group order)
-        std::vector<std::vector<int>> ph_groups;
-        std::vector<std::vector<int>> gdst(gs.size());
-        for (size_t g = 0; g < gs.size(); ++g) {
-            const int c = gs[g].c, j = gs[g].j;
-            for (int p = P.colstart[j]; p < P.colstart[j + 1]; ++p) rowpos[P.Urow_k[p]] = p;
-            for (int s = 0; s < P.lcount[c]; ++s) {
-                int d = rowpos[Lrows[c][s]];
-                if (d < 0) {
-                    msg = "build_plan: internal error, LU pattern is not closed";
-                    return SolverAnalyze;
-                }
-                gdst[g].push_back(d);
-            }
-            for (int p = P.colstart[j]; p < P.colstart[j + 1]; ++p) rowpos[P.Urow_k[p]] = -1;
-            uint64_t busy = 0;
-            for (int d : gdst[g]) {
-                if (used_level[d] != l) {
-                    used_level[d] = l;
-                    used[d] = 0;
-                }
-                busy |= used[d];
-            }
-            int ph = 0;
-            while (ph < 64 && ((busy >> ph) & 1u)) ++ph;
-            if (ph == 64) {
-                msg = "build_plan: more than 64 conflicting update phases in one level";
-                return SolverAnalyze;
-            }
-            for (int d : gdst[g]) used[d] |= (uint64_t)1 << ph;
-            if ((int)ph_groups.size() <= ph) ph_groups.resize(ph + 1);
-            ph_groups[ph].push_back((int)g);
-        }
-        if (ph_groups.empty()) ph_groups.resize(1);  // a level with no updates still divides
-        for (size_t ph = 0; ph < ph_groups.size(); ++ph) {
-            Plan::Phase Q;
-            Q.gbeg = (int)P.grp_lstart.size();
-            int maxlc = 0;
-            // longest groups first: better balance of the round-robin
-            std::stable_sort(ph_groups[ph].begin(), ph_groups[ph].end(), [&](int a, int b) {
-                return P.lcount[gs[a].c] > P.lcount[gs[b].c];
-            });
-            for (int g : ph_groups[ph]) {
-                const int c = gs[g].c;
-                P.grp_lstart.push_back(P.lstart[c]);
-                P.grp_lcount.push_back(P.lcount[c]);
-                P.grp_upos.push_back(gs[g].upos);
-                P.grp_dpos.push_back(P.dpos[c]);
-                P.grp_dst.push_back((int)P.dst.size());
-                P.dst.insert(P.dst.end(), gdst[g].begin(), gdst[g].end());
-                maxlc = std::max(maxlc, P.lcount[c]);
-            }
-            Q.gend = (int)P.grp_lstart.size();
-            Q.dbeg = (int)P.div_pos.size();
-            if (ph == 0) {
-                for (int c : pend_div)
-                    for (int t = 0; t < P.lcount[c]; ++t) {
-                        P.div_pos.push_back(P.lstart[c] + t);
-                        P.div_dpos.push_back(P.dpos[c]);
-                    }
-                pend_div.clear();
-            }
-            Q.dend = (int)P.div_pos.size();
-            Q.lanes = lanes_for(maxlc);
-            P.phases.push_back(Q);
-        }
-        pend_div = bylevel[l];
-    }
-    {
-        // trailing phase: divisions of the last level, and the pivot check of every column
-        Plan::Phase Q;
-        Q.gbeg = Q.gend = (int)P.grp_lstart.size();
-        Q.dbeg = (int)P.div_pos.size();
-        for (int c : pend_div)
-            for (int t = 0; t < P.lcount[c]; ++t) {
-                P.div_pos.push_back(P.lstart[c] + t);
-                P.div_dpos.push_back(P.dpos[c]);
-            }
-        Q.dend = (int)P.div_pos.size();
-        Q.lanes = 1;
-        P.phases.push_back(Q);
-    }
+    // L row lists: for row i, the columns k < i with L(i, k) != 0
+    std::vector<std::vector<int>> lrows(m);
+    for (int k = 0; k < m; ++k)
+        for (int i : Lrows[k]) lrows[i].push_back(k);
 
-    // ---------------------------------------------------------------- triangular solves
+    // refactorisation levels: a pivot is applied once every pivot updating its column is done
+    std::vector<int> level(m, 0);
+    P.flops_refactor = 0;
+    int nlev = 0;
+    for (int k = 0; k < m; ++k) {
+        int lv = 0;
+        for (int c : Ucols[k]) lv = std::max(lv, level[c] + 1);
+        level[k] = lv;
+        nlev = std::max(nlev, lv + 1);
+        for (int c : Ucols[k]) P.flops_refactor += P.lcount[c];
+    }
+    P.colleve = level;
+    P.levels_refactor = nlev;
+    // level of the fused forward push of pivot k: its L column final (level[k]) and y(k)
+    // final (every push into it done).  L columns are kept undivided; consumers divide by
+    // the pivot.
+    std::vector<int> plev(m, 0);
+    int nplev = nlev;
+    for (int k = 0; k < m; ++k) {
+        int lv = level[k];
+        for (int kp : lrows[k]) lv = std::max(lv, plev[kp] + 1);
+        plev[k] = lv;
+        nplev = std::max(nplev, lv + 1);
+    }
+    std::vector<std::vector<int>> bylevel(nlev), bypush(nplev);
+    for (int k = 0; k < m; ++k) {
+        bylevel[level[k]].push_back(k);
+        if (opt.fuse_forward) bypush[plev[k]].push_back(k);
+    }
+    std::vector<int> rowpos(m, -1);
     {
-        std::vector<std::vector<std::pair<int, int>>> lr(m), ur(m);
+        ProgramBuilder B(P.factor, opt.threads);
+        for (int l = 0; l < nplev; ++l) {
+            B.begin();
+            if (l < nlev)
+                for (int c : bylevel[l])
+                    for (auto &e : urows[c]) {
+                        const int j = e.first;
+                        for (int p = P.colstart[j]; p < P.colstart[j + 1]; ++p) rowpos[P.Urow_k[p]] = p;
+                        for (int t = 0; t < P.lcount[c]; ++t) {
+                            int d = rowpos[Lrows[c][t]];
+                            if (d < 0) {
+                                msg = "build_plan: internal error, LU pattern is not closed";
+                                return SolverAnalyze;
+                            }
+                            B.add(d, P.lstart[c] + t, e.second, P.dpos[c], 0);
+                        }
+                        for (int p = P.colstart[j]; p < P.colstart[j + 1]; ++p) rowpos[P.Urow_k[p]] = -1;
+                    }
+            for (int k : bypush[l])
+                for (int t = 0; t < P.lcount[k]; ++t) B.add(Lrows[k][t], P.lstart[k] + t, k, P.dpos[k], 2);
+            B.end();
+        }
+    }
+    {
+        // backward substitution U z = y, from the last pivot: blevel(k) = 1 + max over U(k, j)
+        std::vector<int> blev(m, 0);
+        int nb = 0;
+        for (int k = m - 1; k >= 0; --k) {
+            int lv = 0;
+            for (auto &e : urows[k]) lv = std::max(lv, blev[e.first] + 1);
+            blev[k] = lv;
+            nb = std::max(nb, lv + 1);
+        }
+        std::vector<std::vector<int>> byb(nb);
+        for (int k = 0; k < m; ++k) byb[blev[k]].push_back(k);
+        P.levels_bwd = nb;
+        ProgramBuilder B(P.backward, opt.threads);
+        for (int l = 0; l <= nb; ++l) {
+            B.begin();
+            if (l >= 1)
+                for (int k : byb[l - 1]) B.add(k, 0, 0, P.dpos[k], 4);
+            if (l < nb)
+                for (int k : byb[l])
+                    for (int p = P.colstart[k]; p < P.dpos[k]; ++p) B.add(P.Urow_k[p], p, k, P.dpos[k], 2);
+            B.end();
+        }
+    }
+    {
+        // forward substitution L y = b on its own: flevel(k) = 1 + max over L(k, k')
+        std::vector<int> flev(m, 0);
+        int nf = 0;
         for (int k = 0; k < m; ++k) {
-            for (int t = 0; t < P.lcount[k]; ++t) lr[Lrows[k][t]].push_back({k, P.lstart[k] + t});
-            for (size_t t = 0; t < Ucols[k].size(); ++t) ur[Ucols[k][t]].push_back({k, P.colstart[k] + (int)t});
-        }
-        P.lrow_ptr.assign(m + 1, 0);
-        P.urow_ptr.assign(m + 1, 0);
-        std::vector<int> lvL(m, 0), lvU(m, 0), lenL(m), lenU(m);
-        for (int i = 0; i < m; ++i) {
             int lv = 0;
-            for (auto &e : lr[i]) {
-                P.lrow_col.push_back(e.first);
-                P.lrow_pos.push_back(e.second);
-                lv = std::max(lv, lvL[e.first] + 1);
-            }
-            lvL[i] = lv;
-            lenL[i] = (int)lr[i].size();
-            P.lrow_ptr[i + 1] = (int)P.lrow_col.size();
+            for (int kp : lrows[k]) lv = std::max(lv, flev[kp] + 1);
+            flev[k] = lv;
+            nf = std::max(nf, lv + 1);
         }
-        for (int i = 0; i < m; ++i) {
-            for (auto &e : ur[i]) {
-                P.urow_col.push_back(e.first);
-                P.urow_pos.push_back(e.second);
-            }
-            lenU[i] = (int)ur[i].size();
-            P.urow_ptr[i + 1] = (int)P.urow_col.size();
+        std::vector<std::vector<int>> byf(nf);
+        for (int k = 0; k < m; ++k) byf[flev[k]].push_back(k);
+        P.levels_fwd = nf;
+        ProgramBuilder B(P.forward, opt.threads);
+        for (int l = 0; l < nf; ++l) {
+            B.begin();
+            for (int k : byf[l])
+                for (int t = 0; t < P.lcount[k]; ++t) B.add(Lrows[k][t], P.lstart[k] + t, k, P.dpos[k], 2);
+            B.end();
         }
-        for (int i = m - 1; i >= 0; --i) {
-            int lv = 0;
-            for (auto &e : ur[i]) lv = std::max(lv, lvU[e.first] + 1);
-            lvU[i] = lv;
-        }
-        make_groups(lvL, lenL, opt.chain_max_items, P.fwd_order, P.fwd_groups, P.levels_fwd, true);
-        make_groups(lvU, lenU, opt.chain_max_items, P.bwd_order, P.bwd_groups, P.levels_bwd, true);
     }
 
     // ---------------------------------------------------------------- J fill maps

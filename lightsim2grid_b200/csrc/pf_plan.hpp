@@ -9,9 +9,8 @@
 //     threshold-partial-pivoting Gilbert-Peierls factorisation of the first Jacobian --
 //     the same contract as the reference's KLU::initialize (src/linear_solvers/KLUSolver.cpp:24-45):
 //     later Jacobians are refactorised with these pivots;
-//   * the device schedules: the LU value layout, the per-column update lists of the
-//     left-looking refactorisation and the level sets of the refactorisation and of both
-//     triangular solves.
+//   * the device schedules: the LU value layout and the phase programs of the
+//     refactorisation and of both triangular solves.
 #pragma once
 
 #include <complex>
@@ -35,16 +34,6 @@ enum Err : int {
     SolverSolve = 7,
     NotInitError = 8,
     LicenseError = 9
-};
-
-// One group of elimination levels.  kind 0: a "wide" level, its items are spread over
-// all warps and a block barrier follows.  kind 1: a chain of levels with few items each,
-// run by warp 0 alone, in order, with warp barriers only.
-struct LevelGroup {
-    int begin;   // first item (index into the item order array)
-    int end;     // one past the last item
-    int kind;    // 0 wide, 1 chain
-    int lanes;   // lanes cooperating on one item (solves only): 1, 2, 4, 8, 16 or 32
 };
 
 struct Plan {
@@ -78,26 +67,29 @@ struct Plan {
     std::vector<int> dpos;            // per step: position of the diagonal
     std::vector<int> lstart, lcount;  // per step: L part (rows > k, ascending)
     std::vector<int> Urow_k;          // per LU position: row (step numbering)
-    // Right-looking refactorisation.  An update group (c, j) applies pivot c to column j:
-    // A(i, j) -= A(i, c) * U(c, j) / U(c, c) for every row i of L(:, c).  Groups of one
-    // elimination level are independent except when they write the same entry; they are
-    // coloured into conflict-free phases.  The divisions L(:, c) /= U(c, c) of a level run
-    // at the start of the next level's first phase (they touch no entry that phase uses).
-    std::vector<int> grp_lstart, grp_lcount, grp_upos, grp_dpos, grp_dst;  // per group
-    std::vector<int> dst;             // destination positions, grp_dst[g] .. + grp_lcount[g]
-    struct Phase {
-        int gbeg, gend;               // update groups
-        int dbeg, dend;               // division entries
-        int lanes;                    // lanes per group (1..32)
+    // Phase programs.  A program is a sequence of phases; a phase is a list of independent
+    // operations (no two write the same value, none reads a value another one writes), run
+    // by all threads of a CTA, with a barrier between phases.  The L columns are kept
+    // undivided (L(i,c) * U(c,c)); every consumer divides by the pivot.
+    // Operation (x, y, z, w | kind<<28):
+    //   kind 0  lu[x] -= lu[y] * (lu[z] / lu[w])   right-looking update of column j by pivot c:
+    //                                              y = undivided L(i,c), z = U(c,j), w = U(c,c)
+    //   kind 2  v[x]  -= lu[y] * v[z] / lu[w]      push of an undivided column / value
+    //   kind 4  v[x]  /= lu[w]                     division by a pivot
+    //   kind 7  nothing (padding)
+    // Operations writing the same value run on the same thread (see ProgramBuilder).
+    // `factor`: refactorisation by elimination level with the forward substitution of the
+    // right-hand side fused in; `backward`: U z = y; `forward`: L y = b on its own (second
+    // solve of a refinement).
+    struct Program {
+        std::vector<int> ops;          // 4 ints per operation; kind 7 = empty slot
+        std::vector<int> base;         // phase p = operations [base[p], base[p+1])
+        std::vector<int> width;        // phase p: threads with work (the operation stride)
+        int nphases() const { return (int)base.size() - 1; }
+        int nops() const { return (int)(ops.size() / 4); }
     };
-    std::vector<Phase> phases;
-    std::vector<int> div_pos, div_dpos;  // L entry and its pivot, per division entry
+    Program factor, backward, forward;
     std::vector<int> colleve;         // elimination level per column
-    // triangular solves (row oriented)
-    std::vector<int> lrow_ptr, lrow_col, lrow_pos;   // L(i, k < i)
-    std::vector<int> urow_ptr, urow_col, urow_pos;   // U(i, k > i)
-    std::vector<int> fwd_order, bwd_order;
-    std::vector<LevelGroup> fwd_groups, bwd_groups;
     // J fill
     std::vector<int> ytarget;         // 4 per CSR position: LU position or -1
     std::vector<int> yjpos;           // 4 per CSR position: J CSC position or -1
@@ -117,8 +109,8 @@ struct Plan {
 
 struct PlanOptions {
     double pivot_threshold = 1e-3;    // diagonal preference of the first factorisation
-    int chain_max_items = 2;          // solve levels with at most this many rows join a chain
-    int warps = 16;                   // warps per CTA the schedules are sized for
+    bool fuse_forward = true;         // fuse the forward substitution into the refactorisation
+    int threads = 512;                // CTA size the phase programs are laid out for
 };
 
 // Builds a plan.  Ybus CSC (n x n, complex), V0 and Sbus (used for the first

@@ -23,7 +23,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--lu-placement", type=int, default=0)
-    ap.add_argument("--chain-max", type=int, default=0)
+    ap.add_argument("--fuse-forward", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     args = ap.parse_args()
 
@@ -40,7 +40,7 @@ def main():
     nb = g.nb_powerline() if args.cases <= 0 else min(args.cases, g.nb_powerline())
     coeffs = [g.branch_coeffs([b]) for b in range(nb)]
     plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, threads=args.threads,
-                lu_placement=args.lu_placement, chain_max_items=args.chain_max, max_ctas_per_sm=args.ctas_per_sm)
+                lu_placement=args.lu_placement, fuse_forward=args.fuse_forward, max_ctas_per_sm=args.ctas_per_sm)
     lib = plan._lib
     cp = np.zeros(nb + 1, np.int32)
     rows, cols, vals = [], [], []
@@ -83,11 +83,24 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
+    cyc = np.zeros(8)
+    assert lib.pf_batch_device_phase_cycles(plan.handle, nat.ctypes.byref(b), stream.cuda_stream,
+                                            nat.ptr(cyc, nat.f64p)) == 0, nat.last_error(lib)
+    names = ["mismatch", "jfill", "refactor", "forward", "backward", "refine", "update", "instances"]
+    tot = cyc[:7].sum()
+    phase_share = {k: round(float(v / tot), 4) for k, v in zip(names[:7], cyc[:7])}
+    tr = np.zeros(2048)
+    ntr = lib.pf_batch_device_phase_trace(plan.handle, nat.ctypes.byref(b), stream.cuda_stream,
+                                          nat.ptr(tr, nat.f64p), 2048)
+    assert ntr >= 0, nat.last_error(lib)
+    trace = np.diff(tr[:ntr]).astype(int).tolist()
     it = bufs[8].cpu().numpy()
     er = bufs[9].cpu().numpy()
     out = {"grid": args.grid, "cases": ns, "precision": args.precision, "ms": times,
            "converged": int((er == 0).sum()), "iterations": int(it.sum()),
-           "pf_per_s": float((er == 0).sum() / (np.mean(times) * 1e-3)), "plan": plan.info()}
+           "pf_per_s": float((er == 0).sum() / (np.mean(times) * 1e-3)),
+           "cycles_per_iteration_per_cta": float(tot / max(1, int(it.sum()))), "phase_share": phase_share,
+           "plan": plan.info(), "phase_trace_cycles": trace}
     print(json.dumps(out))
 
 

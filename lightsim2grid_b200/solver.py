@@ -94,7 +94,8 @@ class Plan:
     """Owns one native plan (pattern, ordering, pivots, device schedules)."""
 
     def __init__(self, Ybus, V0, Sbus, slack_ids, slack_weights, pv, pq, distributed=False, precision=0,
-                 threads=0, lu_placement=0, chain_max_items=0, fp64_fallback=0, max_ctas_per_sm=0, refine=0):
+                 threads=0, lu_placement=0, fuse_forward=0, fp64_fallback=0, max_ctas_per_sm=0, refine=0,
+                 refine_threshold=0.0):
         self._lib = nat.load()
         Y = canonical_csc(Ybus)
         n = Y.shape[0]
@@ -116,9 +117,9 @@ class Plan:
         self.pv, self.pq = nat.as_i32(pv), nat.as_i32(pq)
         self.distributed, self.precision = bool(distributed), int(precision)
         opt = nat.PfOptions(precision=self.precision, threads=int(threads), lu_placement=int(lu_placement),
-                            chain_max_items=int(chain_max_items), pivot_threshold=0.0,
+                            fuse_forward=int(fuse_forward), pivot_threshold=0.0,
                             fp64_fallback=int(fp64_fallback), max_ctas_per_sm=int(max_ctas_per_sm),
-                            refine=int(refine))
+                            refine=int(refine), refine_threshold=float(refine_threshold))
         h = nat.ctypes.c_void_p()
         rc = self._lib.pf_plan_create(
             n, nat.ptr(self.Yp, nat.i32p), nat.ptr(self.Yi, nat.i32p), nat.cptr(self.Yx), nat.cptr(V0),
