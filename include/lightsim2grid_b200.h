@@ -132,6 +132,19 @@ int pf_batch_ts(pf_plan *plan, int nsteps, const double *Sbus_ri, const double *
    host synchronisation; capturable in a CUDA graph once the plan exists. */
 int pf_batch_device(pf_plan *plan, const pf_device_batch *batch, void *stream);
 
+/* pf_batch_device without any allocation, for callers that cannot let the library call
+   cudaMalloc (work issued during CUDA-graph stream capture, hosts that own the device-memory
+   budget through their own allocator, plugin hosts that forbid allocation on work calls).
+   No counterpart in the reference.  The kernel's working memory comes from a 32 MiB
+   file-scope device array held on every GPU that loads the library until exit; a plan whose
+   per-CTA working memory does not fit is rejected with an error, otherwise the launch uses as
+   many CTAs as fit.  The first call on a device looks the array's address up
+   (cudaGetSymbolAddress) -- make it before any stream capture.  The array is shared by all
+   calls and keeps the previous call's contents; the job counter is cleared before each launch.
+   Calls whose kernels overlap on the GPU race on the array: keep them on one stream.  Calls no
+   cudaMalloc, cudaFree or allocating library routine. */
+int pf_batch_device_noalloc(pf_plan *plan, const pf_device_batch *batch, void *stream);
+
 /* pf_batch_device, synchronously, with per-phase SM-cycle counters: out[0..7] = cycles summed
    over CTAs spent in mismatch, J fill, refactorisation, forward substitution, backward
    substitution, refinement (mixed form), voltage update / start-up, and the number of

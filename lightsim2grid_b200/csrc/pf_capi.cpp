@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 
+#include "pf_capi_internal.hpp"
 #include "pf_engine.cuh"
 #include "pf_plan.hpp"
 
@@ -379,18 +380,23 @@ void release(pf_plan *pl) {
     pl->stream = nullptr;
 }
 
-// launches the kernel for a batch whose device buffers are set up in `a` (no sync)
-int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
-    a.scratch = static_cast<unsigned char *>(pl->scratch.p);
+// Launches the kernel for a batch whose device buffers are set up in `a` (no sync), with
+// the per-CTA slabs in `scratch` (`scratch_bytes` long) and the job counter at `counter`.
+// The number of CTAs is bounded by the slabs that fit in the scratch.
+int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, unsigned char *scratch,
+                size_t scratch_bytes, int *counter) {
+    a.scratch = scratch;
     a.slab_bytes = (long long)pl->slab;
-    a.job_counter = static_cast<int *>(pl->counter.p);
+    a.job_counter = counter;
     a.lu_in_smem = pl->lu_in_smem ? 1 : 0;
     a.refine = (precision == 1 && pl->refine) ? 1 : 0;
     a.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
     if (a.njobs <= 0) return 0;
-    cudaError_t e = cudaMemsetAsync(pl->counter.p, 0, sizeof(int), st);
+    if (scratch_bytes < pl->slab) return fail(-1, "launch: the scratch memory holds no CTA slab");
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
     int grid = std::min(pl->grid, a.njobs);
+    grid = std::min<long long>(grid, (long long)(scratch_bytes / pl->slab));
     // the FP64 re-run of a mixed plan uses the FP64 kernel with this plan's layout:
     // LU bytes differ, so recompute shared memory and slab use for that precision
     size_t smem = pl->smem;
@@ -406,10 +412,8 @@ int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
             need = l2g::smem_bytes(pl->dp, lub, lub, false);
             slab = l2g::slab_bytes(pl->dp, lub, false);
         }
-        if (slab > pl->slab) {
-            // FP64 needs a larger slab than the plan reserved: fewer CTAs
-            grid = std::max(1, std::min(grid, (int)((pl->slab * (size_t)pl->grid) / slab)));
-        }
+        if (slab > scratch_bytes) return fail(-1, "launch: the scratch memory holds no FP64 CTA slab");
+        grid = std::max(1, std::min(grid, (int)(scratch_bytes / slab)));
         a.slab_bytes = (long long)slab;
         a.lu_in_smem = in ? 1 : 0;
         smem = need;
@@ -420,6 +424,11 @@ int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
     e = l2g::launch_nr_batch(pl->dp, a, precision, pl->threads, grid, smem, st);
     if (e != cudaSuccess) return cuda_fail(e, "launch: kernel");
     return 0;
+}
+
+int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
+    return launch_into(pl, a, precision, st, static_cast<unsigned char *>(pl->scratch.p),
+                       pl->slab * (size_t)pl->grid, static_cast<int *>(pl->counter.p));
 }
 
 template <typename T>
@@ -546,6 +555,50 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
 }
 
 }  // namespace
+
+// ------------------------------------------------------------------ internal (pf_capi_internal.hpp)
+namespace l2g {
+
+BatchArgs device_args(const pf_device_batch *b) {
+    BatchArgs a{};
+    a.n_inst = b->n_inst;
+    a.V0 = static_cast<const double2 *>(b->V0);
+    a.v0_stride = b->v0_stride;
+    a.Sbus = static_cast<const double2 *>(b->Sbus);
+    a.sbus_stride = b->sbus_stride;
+    a.ovr_ptr = b->ovr_ptr;
+    a.ovr_pos = b->ovr_pos;
+    a.ovr_val = static_cast<const double2 *>(b->ovr_val);
+    a.max_iter = b->max_iter;
+    a.tol = b->tol;
+    a.job_first = b->job_first;
+    a.job_count = b->job_count;
+    a.njobs = b->njobs;
+    a.chain = b->chain;
+    a.Vout = static_cast<double2 *>(b->Vout);
+    a.iters = b->iters;
+    a.errs = b->errs;
+    a.Jout = nullptr;
+    a.j_inst = -1;
+    return a;
+}
+
+int batch_device_with_scratch(pf_plan *pl, const pf_device_batch *b, void *stream, void *scratch,
+                              size_t scratch_bytes) {
+    if (!pl || !b) return fail(-1, "pf_batch_device_noalloc: null argument");
+    const size_t head = 256;  // job counter
+    if (scratch_bytes <= head) return fail(-1, "pf_batch_device_noalloc: scratch too small");
+    unsigned char *base = static_cast<unsigned char *>(scratch);
+    l2g::BatchArgs a = l2g::device_args(b);
+    return launch_into(pl, a, pl->precision, static_cast<cudaStream_t>(stream), base + head, scratch_bytes - head,
+                       reinterpret_cast<int *>(base));
+}
+
+size_t plan_slab_bytes(const pf_plan *pl) { return pl ? pl->slab : 0; }
+
+void set_last_error(const std::string &msg) { g_err = msg; }
+
+}  // namespace l2g
 
 extern "C" {
 
@@ -819,35 +872,13 @@ int pf_batch_ts(pf_plan *pl, int nsteps, const double *Sbus_ri, const double *V0
     return 0;
 }
 
-static l2g::BatchArgs device_args(const pf_device_batch *b) {
-    l2g::BatchArgs a{};
-    a.n_inst = b->n_inst;
-    a.V0 = static_cast<const double2 *>(b->V0);
-    a.v0_stride = b->v0_stride;
-    a.Sbus = static_cast<const double2 *>(b->Sbus);
-    a.sbus_stride = b->sbus_stride;
-    a.ovr_ptr = b->ovr_ptr;
-    a.ovr_pos = b->ovr_pos;
-    a.ovr_val = static_cast<const double2 *>(b->ovr_val);
-    a.max_iter = b->max_iter;
-    a.tol = b->tol;
-    a.job_first = b->job_first;
-    a.job_count = b->job_count;
-    a.njobs = b->njobs;
-    a.chain = b->chain;
-    a.Vout = static_cast<double2 *>(b->Vout);
-    a.iters = b->iters;
-    a.errs = b->errs;
-    a.Jout = nullptr;
-    a.j_inst = -1;
-    return a;
-}
 
 static int batch_device_impl(pf_plan *pl, const pf_device_batch *b, void *stream, unsigned long long *cycles) {
-    l2g::BatchArgs a = device_args(b);
+    l2g::BatchArgs a = l2g::device_args(b);
     a.phase_cycles = cycles;
     return launch(pl, a, pl->precision, static_cast<cudaStream_t>(stream));
 }
+
 
 int pf_batch_device(pf_plan *pl, const pf_device_batch *b, void *stream) {
     if (!pl || !b) return fail(-1, "pf_batch_device: null argument");
@@ -861,7 +892,7 @@ int pf_batch_device_phase_trace(pf_plan *pl, const pf_device_batch *b, void *str
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     e = cudaMemsetAsync(pl->cycles.p, 0, (size_t)cap * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return cuda_fail(e, "pf_batch_device_phase_trace: memset");
-    l2g::BatchArgs a = device_args(b);
+    l2g::BatchArgs a = l2g::device_args(b);
     a.trace = static_cast<unsigned long long *>(pl->cycles.p);
     a.trace_cap = cap;
     int rc = launch(pl, a, pl->precision, st);

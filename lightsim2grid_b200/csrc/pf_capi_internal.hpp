@@ -1,0 +1,26 @@
+// Internal interfaces between the translation units behind the C ABI (not part of the ABI).
+#pragma once
+
+#include <cstddef>
+#include <string>
+
+#include "../../include/lightsim2grid_b200.h"
+#include "pf_engine.cuh"
+
+namespace l2g {
+
+// Kernel arguments of a device-resident batch (scratch, counter and variant not yet set).
+BatchArgs device_args(const pf_device_batch *b);
+
+// pf_batch_device with caller-provided scratch: the first 256 bytes hold the job counter,
+// the rest the per-CTA slabs (the grid shrinks to the slabs that fit).  Allocates nothing.
+int batch_device_with_scratch(pf_plan *pl, const pf_device_batch *b, void *stream, void *scratch,
+                              size_t scratch_bytes);
+
+// Bytes of one CTA slab of the plan's kernel.
+size_t plan_slab_bytes(const pf_plan *pl);
+
+// Sets the message returned by pf_last_error on this thread.
+void set_last_error(const std::string &msg);
+
+}  // namespace l2g

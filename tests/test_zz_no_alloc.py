@@ -1,0 +1,95 @@
+"""pf_batch_device_noalloc: the batch entry point for callers that cannot let the library
+allocate device memory (work issued during CUDA-graph capture, hosts that own the memory
+budget, plugin hosts that forbid allocation on work calls).
+
+It must give the same answer as pf_batch_device on the same device-resident inputs, call
+after call, although its working memory is a static array shared by every call.  This file
+is collected last so that a failure here cannot hide any other test.
+"""
+import numpy as np
+import pytest
+
+from conftest import grid_problem
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_batch(plan, c, ncases, dev):
+    import torch
+    from lightsim2grid_b200 import _native as nat
+
+    g = c["grid"]
+    coeffs = [g.branch_coeffs([b]) for b in range(min(ncases, g.nb_powerline()))]
+    cp = np.zeros(len(coeffs) + 1, np.int32)
+    rows, cols, vals = [], [], []
+    for k, lst in enumerate(coeffs):
+        cp[k + 1] = cp[k] + len(lst)
+        for (r, cc, y) in lst:
+            rows.append(r)
+            cols.append(cc)
+            vals.append(y)
+    rows, cols, vals = nat.as_i32(rows), nat.as_i32(cols), nat.as_c128(vals).ravel()
+    solv = np.zeros(len(coeffs), np.int32)
+    optr = np.zeros(len(coeffs) + 1, np.int32)
+    opos = np.zeros(int(cp[-1]), np.int32)
+    oval = np.zeros(int(cp[-1]), np.complex128)
+    lib = plan._lib
+    nw = lib.pf_n1_prepare(plan.handle, len(coeffs), nat.ptr(cp, nat.i32p), nat.ptr(rows, nat.i32p),
+                           nat.ptr(cols, nat.i32p), nat.cptr(vals), nat.ptr(solv, nat.i32p), nat.ptr(optr, nat.i32p),
+                           nat.ptr(opos, nat.i32p), nat.cptr(oval), int(cp[-1]))
+    assert nw >= 0, nat.last_error(lib)
+    ns = int(solv.sum())
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    n = c["Ybus"].shape[0]
+    keep = dict(V0=t(nat.as_c128(c["V0"]).ravel().view(np.float64)), S=t(nat.as_c128(c["Sbus"]).ravel().view(np.float64)),
+                optr=t(optr[:ns + 1]), opos=t(opos[:nw]), oval=t(oval[:nw].view(np.float64)),
+                jf=t(np.arange(ns, dtype=np.int32)), jc=t(np.ones(ns, np.int32)))
+
+    def outputs():
+        return (torch.full((ns * n * 2,), float("nan"), dtype=torch.float64, device=dev),
+                torch.full((ns,), -7, dtype=torch.int32, device=dev), torch.full((ns,), -7, dtype=torch.int32, device=dev))
+
+    def desc(out):
+        Vout, it, er = out
+        return nat.PfDeviceBatch(n_inst=ns, V0=keep["V0"].data_ptr(), v0_stride=0, Sbus=keep["S"].data_ptr(),
+                                 sbus_stride=0, ovr_ptr=keep["optr"].data_ptr(), ovr_pos=keep["opos"].data_ptr(),
+                                 ovr_val=keep["oval"].data_ptr(), max_iter=10, tol=1e-8, chain=0,
+                                 job_first=keep["jf"].data_ptr(), job_count=keep["jc"].data_ptr(), njobs=ns,
+                                 Vout=Vout.data_ptr(), iters=it.data_ptr(), errs=er.data_ptr())
+
+    return ns, keep, outputs, desc
+
+
+@pytest.mark.parametrize("name,ncases,precision", [("grid118", 186, 0), ("grid118", 186, 1), ("grid2848", 400, 1)])
+def test_noalloc_matches_allocating_entry_point_twice(name, ncases, precision):
+    import torch
+    from lightsim2grid_b200 import Plan, _native as nat
+
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    c = grid_problem(name)
+    plan = Plan(c["Ybus"], c["V0"], c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=precision)
+    lib = plan._lib
+    ns, keep, outputs, desc = _device_batch(plan, c, ncases, dev)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    ref = outputs()
+    b = desc(ref)
+    assert lib.pf_batch_device(plan.handle, nat.ctypes.byref(b), stream) == 0, nat.last_error(lib)
+    torch.cuda.synchronize()
+    V_ref = ref[0].cpu().numpy()
+    it_ref, er_ref = ref[1].cpu().numpy(), ref[2].cpu().numpy()
+    assert np.all(er_ref >= 0) and np.any(er_ref == 0)
+
+    for call in range(2):  # two calls in a row share (and reuse) the static working memory
+        out = outputs()
+        b = desc(out)
+        rc = lib.pf_batch_device_noalloc(plan.handle, nat.ctypes.byref(b), stream)
+        assert rc == 0, nat.last_error(lib)
+        torch.cuda.synchronize()
+        V = out[0].cpu().numpy()
+        it, er = out[1].cpu().numpy(), out[2].cpu().numpy()
+        assert np.array_equal(er, er_ref), call
+        assert np.array_equal(it, it_ref), call
+        ok = np.repeat(er_ref == 0, V.size // ns)
+        assert np.abs(V[ok] - V_ref[ok]).max() <= 1e-10, call
