@@ -71,7 +71,8 @@ struct pf_plan {
     void *d_dbl = nullptr;
     l2g::DevPlan dp{};
     // device work buffers
-    DevBuf scratch, counter, V0, Sbus, optr, opos, oval, jfirst, jcount, Vout, iters, errs, Jout, cycles;
+    DevBuf scratch, counter, V0, Sbus, optr, opos, oval, jfirst, jcount, Vout, iters, errs, Jout, cycles, Vcase,
+        casemap;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // host state
@@ -259,6 +260,15 @@ int upload(pf_plan *pl) {
     size_t ofo = push(bi, P.factor.ops), ofb = push(bi, P.factor.base), ofw = push(bi, P.factor.width);
     size_t obo = push(bi, P.backward.ops), obb = push(bi, P.backward.base), obw = push(bi, P.backward.width);
     size_t owo = push(bi, P.forward.ops), owb = push(bi, P.forward.base), oww = push(bi, P.forward.width);
+    // packed operations for the shared-memory LU layout (always fit when the LU does)
+    const bool compact = l2g::compact_fits(P);
+    std::vector<unsigned> cf, cb, cw;
+    if (compact) {
+        l2g::compact_ops(P.factor, P.m, cf);
+        l2g::compact_ops(P.backward, P.m, cb);
+        l2g::compact_ops(P.forward, P.m, cw);
+    }
+    size_t ocf = push(bi, cf), ocb = push(bi, cb), ocw = push(bi, cw);
     size_t odpos = push(bi, P.dpos);
     std::vector<double> rx(2 * (size_t)P.nnzY);
     for (int i = 0; i < P.nnzY; ++i) {
@@ -319,6 +329,12 @@ int upload(pf_plan *pl) {
     d.fac_width = I(ofw);
     d.bwd_width = I(obw);
     d.fwd_width = I(oww);
+    auto U2 = [&](size_t o) { return reinterpret_cast<const uint2 *>(bI + o); };
+    d.compact = compact ? 1 : 0;
+    d.lu_offset = l2g::compact_lu_offset(P.m);
+    d.fac_cops = compact ? U2(ocf) : nullptr;
+    d.bwd_cops = compact ? U2(ocb) : nullptr;
+    d.fwd_cops = compact ? U2(ocw) : nullptr;
     d.fac_nph = P.factor.nphases();
     d.bwd_ops = I4(obo);
     d.bwd_base = I(obb);
@@ -346,7 +362,7 @@ int configure(pf_plan *pl) {
     const size_t static_smem = 2048;  // Shared struct of the kernel, rounded up
     size_t sm_in = l2g::smem_bytes(pl->dp, lub, xb, true);
     size_t sm_out = l2g::smem_bytes(pl->dp, lub, xb, false);
-    bool fits = sm_in + static_smem <= (size_t)optin;
+    bool fits = pl->dp.compact && sm_in + static_smem <= (size_t)optin;
     if (pl->opt.lu_placement == 1 && !fits) return fail(-1, "pf_plan_create: LU does not fit in shared memory");
     if (sm_out + static_smem > (size_t)optin)
         return fail(-1, "pf_plan_create: the solve vector does not fit in shared memory");
@@ -368,7 +384,8 @@ int configure(pf_plan *pl) {
 
 void release(pf_plan *pl) {
     for (DevBuf *b : {&pl->scratch, &pl->counter, &pl->V0, &pl->Sbus, &pl->optr, &pl->opos, &pl->oval,
-                      &pl->jfirst, &pl->jcount, &pl->Vout, &pl->iters, &pl->errs, &pl->Jout, &pl->cycles})
+                      &pl->jfirst, &pl->jcount, &pl->Vout, &pl->iters, &pl->errs, &pl->Jout, &pl->cycles,
+                      &pl->Vcase, &pl->casemap})
         b->release();
     if (pl->d_int) cudaFree(pl->d_int);
     if (pl->d_dbl) cudaFree(pl->d_dbl);
@@ -407,7 +424,7 @@ int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, u
         size_t slab = l2g::slab_bytes(pl->dp, lub, in);
         int optin = 0;
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, pl->device);
-        if (in && need + 2048 > (size_t)optin) {
+        if (in && (need + 2048 > (size_t)optin || !pl->dp.compact)) {
             in = false;
             need = l2g::smem_bytes(pl->dp, lub, lub, false);
             slab = l2g::slab_bytes(pl->dp, lub, false);
@@ -536,8 +553,9 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
         }
     }
     double t2 = now();
-    if ((e = cudaMemcpyAsync(Vout, pl->Vout.p, (size_t)n_inst * n * sizeof(cplx), cudaMemcpyDeviceToHost, st)) !=
-        cudaSuccess)
+    if (Vout &&
+        (e = cudaMemcpyAsync(Vout, pl->Vout.p, (size_t)n_inst * n * sizeof(cplx), cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess)
         return cuda_fail(e, "batch: download");
     if (want_J) {
         pl->lastJ.resize(pl->P.Ji.size());
@@ -798,16 +816,39 @@ int pf_batch_n1(pf_plan *pl, int ncases, const int *case_ptr, const int *coef_ro
     oval.resize(std::max(w, 1));
     std::vector<int> jf(ns), jc(ns, 1);
     for (int i = 0; i < ns; ++i) jf[i] = i;
-    std::vector<cplx> vout((size_t)std::max(ns, 1) * n);
     std::vector<int> it(std::max(ns, 1)), er(std::max(ns, 1));
     double t1 = now();
+    cplx *Vo = reinterpret_cast<cplx *>(V_out_ri);
     if (ns > 0) {
         int rc = run_batch(pl, ns, reinterpret_cast<const cplx *>(V0_ri), 0, reinterpret_cast<const cplx *>(Sbus_ri),
-                           0, optr, opos, oval, jf, jc, 0, max_iter, tol, vout.data(), it.data(), er.data(), false);
+                           0, optr, opos, oval, jf, jc, 0, max_iter, tol, nullptr, it.data(), er.data(), false);
         if (rc) return rc;
     }
-    cplx *Vo = reinterpret_cast<cplx *>(V_out_ri);
-    std::fill(Vo, Vo + (size_t)ncases * n, cplx(0.0, 0.0));
+    // result rows in case order, on the device, then one copy into the caller's array
+    {
+        cudaStream_t st = pl->stream;
+        std::vector<int> map(ncases, -1);
+        for (int i = 0; i < ns; ++i) map[idx[i]] = i;
+        cudaError_t e;
+        if ((e = pl->casemap.ensure((size_t)std::max(ncases, 1) * sizeof(int))) != cudaSuccess)
+            return cuda_fail(e, "pf_batch_n1: alloc");
+        if ((e = pl->Vcase.ensure((size_t)std::max(ncases, 1) * n * sizeof(cplx))) != cudaSuccess)
+            return cuda_fail(e, "pf_batch_n1: alloc");
+        if (ns == 0 && (e = pl->errs.ensure(sizeof(int))) != cudaSuccess) return cuda_fail(e, "pf_batch_n1: alloc");
+        if (ns == 0 && (e = pl->Vout.ensure(sizeof(cplx))) != cudaSuccess) return cuda_fail(e, "pf_batch_n1: alloc");
+        if ((e = cudaMemcpyAsync(pl->casemap.p, map.data(), (size_t)ncases * sizeof(int), cudaMemcpyHostToDevice,
+                                 st)) != cudaSuccess)
+            return cuda_fail(e, "pf_batch_n1: upload");
+        if ((e = l2g::launch_scatter_case_rows(static_cast<const double2 *>(pl->Vout.p),
+                                               static_cast<const int *>(pl->errs.p),
+                                               static_cast<const int *>(pl->casemap.p), ncases, n,
+                                               static_cast<double2 *>(pl->Vcase.p), pl->num_sms, st)) != cudaSuccess)
+            return cuda_fail(e, "pf_batch_n1: scatter");
+        if ((e = cudaMemcpyAsync(Vo, pl->Vcase.p, (size_t)ncases * n * sizeof(cplx), cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess)
+            return cuda_fail(e, "pf_batch_n1: download");
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "pf_batch_n1: download");
+    }
     for (int c = 0; c < ncases; ++c) {
         converged[c] = 0;
         iters[c] = 0;
@@ -818,7 +859,6 @@ int pf_batch_n1(pf_plan *pl, int ncases, const int *case_ptr, const int *coef_ro
         iters[c] = it[i];
         errs[c] = er[i];
         converged[c] = er[i] == 0;
-        if (er[i] == 0) std::memcpy(Vo + (size_t)c * n, vout.data() + (size_t)i * n, sizeof(cplx) * n);
     }
     pl->timers[0] = now() - t0;
     pl->timers[1] = t1 - t0;
@@ -992,18 +1032,50 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
             const int W = pr.ops[4 * o + 3] & 0x0fffffff, kind = (unsigned)pr.ops[4 * o + 3] >> 28;
             switch (kind) {
                 case 0: lu[X] -= lu[Y] * (lu[Z] / lu[W]); break;
-                case 1: lu[X] = lu[X] / lu[W]; break;
                 case 2: xs[X] -= lu[Y] * xs[Z] / lu[W]; break;
-                case 3: xs[X] -= lu[Y] * xs[Z]; break;
-                case 4: xs[X] = xs[X] / lu[W]; break;
                 default: break;
             }
         }
+    };
+    // the same programs in the packed form of the shared-memory layout, one index space
+    std::vector<double> s0;
+    if (l2g::compact_fits(P)) {
+        const int L = l2g::compact_lu_offset(m);
+        s0.assign((size_t)L + P.nnzLU, 0.0);
+        for (int k = 0; k < m; ++k) s0[k] = xs[k];
+        for (int p = 0; p < P.nnzLU; ++p) s0[(size_t)L + p] = lu[p];
+    }
+    auto run_packed = [&](const l2g::Plan::Program &pr) {
+        std::vector<unsigned> c;
+        l2g::compact_ops(pr, m, c);
+        for (size_t o = 0; o < c.size(); o += 2) {
+            const unsigned X = c[o] & 0xffffu, Y = c[o] >> 16, Z = c[o + 1] & 0xffffu, W = c[o + 1] >> 16;
+            if (X == (unsigned)m) continue;  // empty slot (scratch)
+            s0[X] -= s0[Y] * (s0[Z] / s0[W]);
+        }
+    };
+    auto scale = [&](std::vector<double> &v, const double *u) {
+        for (int k = 0; k < m; ++k) v[k] = v[k] / u[P.dpos[k]];
     };
     run(P.factor);
     for (int k = 0; k < m; ++k)
         if (lu[P.dpos[k]] == 0.0) return fail(l2g::SolverReFactor, "schedule check: zero pivot");
     run(P.backward);
+    scale(xs, lu.data());
+    if (!s0.empty()) {
+        const int L = l2g::compact_lu_offset(m);
+        run_packed(P.factor);
+        run_packed(P.backward);
+        std::vector<double> xc(s0.begin(), s0.begin() + m);
+        scale(xc, s0.data() + L);
+        double dmax = 0.0, amax = 0.0;
+        for (int k = 0; k < m; ++k) {
+            dmax = std::max(dmax, std::fabs(xc[k] - xs[k]));
+            amax = std::max(amax, std::fabs(xs[k]));
+        }
+        if (dmax > 1e-9 * std::max(1.0, amax))
+            return fail(-1, "schedule check: packed and unpacked programs disagree");
+    }
     // the stand-alone forward program must agree with the fused one: solve L y = b again
     {
         std::vector<double> y2(m, 0.0), keep = xs;
@@ -1011,6 +1083,7 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         xs = y2;
         run(P.forward);
         run(P.backward);
+        scale(xs, lu.data());
         double dmax = 0.0, amax = 0.0;
         for (int k = 0; k < m; ++k) {
             dmax = std::max(dmax, std::fabs(xs[k] - keep[k]));

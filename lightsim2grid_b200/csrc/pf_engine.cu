@@ -191,46 +191,30 @@ __device__ void jacobian_fill(const DevPlan &P, Shared &S, const double2 *__rest
     }
 }
 
+// a / b: correctly rounded in FP64; in FP32 (mixed form) the reciprocal-based quotient
+// (within 2 ulp), whose error the FP64-residual refinement of the Newton step absorbs
+__device__ __forceinline__ double lu_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float lu_div(float a, float b) { return __fdividef(a, b); }
+
 template <typename LT, typename XT>
 __device__ __forceinline__ void run_op(const int4 o, LT *lu, XT *v) {
-    const int kind = (unsigned)o.w >> 28;
+    const unsigned kind = (unsigned)o.w >> 28;
     const int w = o.w & 0x0fffffff;
-    switch (kind) {
-        case 0: lu[o.x] -= lu[o.y] * (lu[o.z] / lu[w]); break;
-        case 1: lu[o.x] = lu[o.x] / lu[w]; break;
-        case 2: v[o.x] -= (XT)lu[o.y] * v[o.z] / (XT)lu[w]; break;
-        case 3: v[o.x] -= (XT)lu[o.y] * v[o.z]; break;
-        case 4: v[o.x] = v[o.x] / (XT)lu[w]; break;
-        default: break;  // padding
+    if (kind == 0u) {
+        lu[o.x] -= lu[o.y] * lu_div(lu[o.z], lu[w]);
+    } else if (kind == 2u) {
+        v[o.x] -= lu_div((XT)lu[o.y] * v[o.z], (XT)lu[w]);
     }
+    // kind 7: empty slot
 }
 
-// Runs a phase program: one barrier per phase.  In phase p, thread t < sw[p] runs the
-// operations sb[p] + t, sb[p] + t + sw[p], ... (bounds and widths staged in shared memory).
-//
-// Latency hiding: a thread holds the first two operations of the current phase and of the
-// next one in registers and loads those of the next-but-one phase while it works; inside a
-// phase it loads two operations ahead.  A register that still waits for its load must not
-// be copied (the copy would stall on the load), so the three register pairs rotate roles
-// through a loop unrolled by three, and inside a phase each register is reloaded right
-// after its operation has consumed it.
-struct OpPair {
-    int4 a, b;
-};
-
-template <typename LT, typename XT>
-__device__ __forceinline__ void load_first2(const int4 *__restrict__ ops, const int *sb, const int *sw, int nph,
-                                            int p, OpPair &r) {
-    r.a = make_int4(0, 0, 0, 7 << 28);
-    r.b = r.a;
-    if (p < nph) {
-        const int w = sw[p];
-        if ((int)threadIdx.x < w) {
-            const int k = sb[p] + threadIdx.x, e = sb[p + 1];
-            if (k < e) r.a = ops[k];
-            if (k + w < e) r.b = ops[k + w];
-        }
-    }
+// Packed operation of the shared-memory layout: s[x] -= s[y] * s[z] / s[w] over the one
+// index space of the solve vector and the LU (empty slots write a scratch element).
+template <typename T>
+__device__ __forceinline__ void run_op_packed(const uint2 o, T *s) {
+    const T y = s[o.x >> 16], z = s[o.y & 0xffffu], w = s[o.y >> 16];
+    T *px = s + (o.x & 0xffffu);
+    *px -= y * lu_div(z, w);
 }
 
 struct Trace {
@@ -241,22 +225,67 @@ struct Trace {
     }
 };
 
-template <typename LT, typename XT>
-__device__ __forceinline__ void run_phase(const int4 *__restrict__ ops, const int *sb, const int *sw, int nph,
-                                          int p, OpPair &cur, OpPair &pre, LT *lu, XT *v, Trace &tr) {
-    load_first2<LT, XT>(ops, sb, sw, nph, p + 2, pre);
+// Runs a phase program: one barrier per phase.  In phase p, thread t < sw[p] runs the
+// operations sb[p] + t, sb[p] + t + sw[p], ... (bounds and widths staged in shared memory).
+//
+// Latency hiding: a block barrier also waits for the thread's global loads still in flight,
+// so operation loads are not carried across more than the next barrier.  A thread loads the
+// first two operations of phase p + 1 when phase p starts (they arrive while phase p works),
+// and inside a phase it keeps four operations in flight.  The two register pairs swap roles
+// from phase to phase through a loop unrolled by two (a register still waiting for its load
+// is never copied).
+template <typename OP>
+struct OpPair {
+    OP a, b;
+};
+
+template <typename OP>
+__device__ __forceinline__ OP empty_op();
+template <>
+__device__ __forceinline__ int4 empty_op<int4>() { return make_int4(0, 0, 0, 7 << 28); }
+
+template <typename OP>
+__device__ __forceinline__ void load_first2(const OP *__restrict__ ops, const int *sb, const int *sw, int nph,
+                                            int p, OpPair<OP> &r, OP none) {
+    r.a = none;
+    r.b = none;
+    if (p < nph) {
+        const int w = sw[p];
+        if ((int)threadIdx.x < w) {
+            const int k = sb[p] + threadIdx.x, e = sb[p + 1];
+            if (k < e) r.a = ops[k];
+            if (k + w < e) r.b = ops[k + w];
+        }
+    }
+}
+
+template <typename OP, typename F>
+__device__ __forceinline__ void run_phase(const OP *__restrict__ ops, const int *sb, const int *sw, int nph, int p,
+                                          OpPair<OP> &cur, OpPair<OP> &nxt, OP none, F &&apply, Trace &tr) {
+    load_first2<OP>(ops, sb, sw, nph, p + 1, nxt, none);
     const int w = sw[p];
     if ((int)threadIdx.x < w) {
         const int e = sb[p + 1];
         int k = sb[p] + threadIdx.x;
+        OP c = none, d = none;
+        if (k + 2 * w < e) c = ops[k + 2 * w];
+        if (k + 3 * w < e) d = ops[k + 3 * w];
         for (;;) {
             if (k >= e) break;
-            run_op<LT, XT>(cur.a, lu, v);
-            if (k + 2 * w < e) cur.a = ops[k + 2 * w];
+            apply(cur.a);
+            if (k + 4 * w < e) cur.a = ops[k + 4 * w];
             k += w;
             if (k >= e) break;
-            run_op<LT, XT>(cur.b, lu, v);
-            if (k + 2 * w < e) cur.b = ops[k + 2 * w];
+            apply(cur.b);
+            if (k + 4 * w < e) cur.b = ops[k + 4 * w];
+            k += w;
+            if (k >= e) break;
+            apply(c);
+            if (k + 4 * w < e) c = ops[k + 4 * w];
+            k += w;
+            if (k >= e) break;
+            apply(d);
+            if (k + 4 * w < e) d = ops[k + 4 * w];
             k += w;
         }
     }
@@ -264,20 +293,39 @@ __device__ __forceinline__ void run_phase(const int4 *__restrict__ ops, const in
     tr.mark();
 }
 
-template <typename LT, typename XT>
-__device__ void run_program(const int4 *__restrict__ ops, const int *sb, const int *sw, int nph, LT *lu, XT *v,
+template <typename OP, typename F>
+__device__ void run_program(const OP *__restrict__ ops, const int *sb, const int *sw, int nph, OP none, F &&apply,
                             Trace &tr) {
     if (nph <= 0) return;
-    OpPair A, B, C;
-    load_first2<LT, XT>(ops, sb, sw, nph, 0, A);
-    load_first2<LT, XT>(ops, sb, sw, nph, 1, B);
-    for (int p = 0; p < nph; p += 3) {
-        run_phase<LT, XT>(ops, sb, sw, nph, p, A, C, lu, v, tr);
+    OpPair<OP> A, B;
+    load_first2<OP>(ops, sb, sw, nph, 0, A, none);
+    for (int p = 0; p < nph; p += 2) {
+        run_phase<OP>(ops, sb, sw, nph, p, A, B, none, apply, tr);
         if (p + 1 >= nph) break;
-        run_phase<LT, XT>(ops, sb, sw, nph, p + 1, B, A, lu, v, tr);
-        if (p + 2 >= nph) break;
-        run_phase<LT, XT>(ops, sb, sw, nph, p + 2, C, B, lu, v, tr);
+        run_phase<OP>(ops, sb, sw, nph, p + 1, B, A, none, apply, tr);
     }
+}
+
+// One program over the LU layout of the kernel variant: packed operations over the shared
+// index space, or int4 operations over the global LU and the shared solve vector.
+template <typename LT, typename XT, bool LU_SMEM>
+__device__ __forceinline__ void run_lu_program(const uint2 *cops, const int4 *ops, const int *sb, const int *sw,
+                                               int nph, int m, LT *lu, XT *x, Trace &tr) {
+    if constexpr (LU_SMEM) {
+        static_assert(sizeof(LT) == sizeof(XT), "the packed layout needs one element type");
+        const uint2 none = make_uint2((unsigned)m | ((unsigned)m << 16), (unsigned)m | ((unsigned)m << 16));
+        run_program<uint2>(cops, sb, sw, nph, none, [x](const uint2 o) { run_op_packed<XT>(o, x); }, tr);
+    } else {
+        run_program<int4>(ops, sb, sw, nph, empty_op<int4>(), [lu, x](const int4 o) { run_op<LT, XT>(o, lu, x); },
+                          tr);
+    }
+}
+
+// z(k) / U(k, k): the backward program keeps z undivided
+template <typename LT, typename XT>
+__device__ __forceinline__ void scale_by_pivots(const DevPlan &P, const LT *lu, XT *x) {
+    for (int k = threadIdx.x; k < P.m; k += blockDim.x) x[k] = lu_div(x[k], (XT)lu[P.dpos[k]]);
+    __syncthreads();
 }
 
 template <typename LT>
@@ -326,7 +374,8 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
     __shared__ Shared S;
     const int tid = threadIdx.x;
     const int n = P.n, m = P.m;
-    const size_t xbytes = ((size_t)m * sizeof(XT) + 15) & ~(size_t)15;
+    // shared layout: x | LU (LU_SMEM: one index space, LU at element lu_offset) | phase tables
+    const size_t xbytes = LU_SMEM ? (size_t)P.lu_offset * sizeof(XT) : (((size_t)m * sizeof(XT) + 15) & ~(size_t)15);
     XT *x = reinterpret_cast<XT *>(dyn);
     unsigned char *slab = A.scratch + (size_t)blockIdx.x * (size_t)A.slab_bytes;
     double2 *V = reinterpret_cast<double2 *>(slab);
@@ -429,22 +478,24 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
                 // refactorisation with the forward substitution of the right-hand side fused in
                 const bool refine_now = REFINE && norm < A.refine_below;
                 tr.mark();
-                run_program<LT, XT>(P.fac_ops, sb_fac, sw_fac, P.fac_nph, lu, x, tr);
+                run_lu_program<LT, XT, LU_SMEM>(P.fac_cops, P.fac_ops, sb_fac, sw_fac, P.fac_nph, m, lu, x, tr);
                 check_pivots<LT>(P, S, lu);
                 L2G_MARK(2);
                 if (S.piv_err) {
                     err = 6;  // SolverReFactor
                     break;
                 }
-                run_program<LT, XT>(P.bwd_ops, sb_bwd, sw_bwd, P.bwd_nph, lu, x, tr);
+                run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, sb_bwd, sw_bwd, P.bwd_nph, m, lu, x, tr);
+                scale_by_pivots<LT, XT>(P, lu, x);
                 L2G_MARK(4);
                 if (refine_now) {
                     for (int k = tid; k < m; k += blockDim.x) dxg[k] = (double)x[k];
                     __syncthreads();
                     newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, x);
                     __syncthreads();
-                    run_program<LT, XT>(P.fwd_ops, sb_fwd, sw_fwd, P.fwd_nph, lu, x, tr);
-                    run_program<LT, XT>(P.bwd_ops, sb_bwd, sw_bwd, P.bwd_nph, lu, x, tr);
+                    run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, sb_fwd, sw_fwd, P.fwd_nph, m, lu, x, tr);
+                    run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, sb_bwd, sw_bwd, P.bwd_nph, m, lu, x, tr);
+                    scale_by_pivots<LT, XT>(P, lu, x);
                     L2G_MARK(5);
                 }
                 // voltage update
@@ -541,7 +592,27 @@ int occupancy_variant(int threads, size_t smem) {
     return nb;
 }
 
+// Result rows in case order: row c = the converged voltages of compact instance map[c], or
+// zeros (islanded case, map[c] < 0, or an instance that did not converge).
+__global__ void scatter_case_rows(const double2 *__restrict__ src, const int *__restrict__ errs,
+                                  const int *__restrict__ map, int ncases, int n, double2 *__restrict__ dst) {
+    const long long total = (long long)ncases * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / n), b = (int)(t - (long long)c * n);
+        const int i = map[c];
+        dst[t] = (i >= 0 && errs[i] == 0) ? src[(long long)i * n + b] : make_double2(0.0, 0.0);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_scatter_case_rows(const double2 *src, const int *errs, const int *map, int ncases, int n,
+                                     double2 *dst, int num_sms, cudaStream_t st) {
+    if (ncases <= 0) return cudaSuccess;
+    scatter_case_rows<<<num_sms * 8, 256, 0, st>>>(src, errs, map, ncases, n, dst);
+    return cudaGetLastError();
+}
 
 size_t slab_bytes(const DevPlan &P, int lu_bytes, bool lu_in_smem) {
     size_t bus = (((size_t)P.n * 64 + (size_t)P.m * 8) + 255) & ~(size_t)255;
@@ -550,7 +621,7 @@ size_t slab_bytes(const DevPlan &P, int lu_bytes, bool lu_in_smem) {
 }
 
 size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem) {
-    size_t xb = ((size_t)P.m * x_bytes + 15) & ~(size_t)15;
+    size_t xb = lu_in_smem ? (size_t)P.lu_offset * x_bytes : (((size_t)P.m * x_bytes + 15) & ~(size_t)15);
     size_t lb = lu_in_smem ? (((size_t)P.nnzLU * lu_bytes + 15) & ~(size_t)15) : 0;
     size_t bb = (size_t)(2 * (P.fac_nph + P.bwd_nph + P.fwd_nph) + 3) * sizeof(int);
     return xb + lb + bb;

@@ -30,6 +30,9 @@ struct DevPlan {
     const int *fac_base, *bwd_base, *fwd_base;
     const int *fac_width, *bwd_width, *fwd_width;
     int fac_nph, bwd_nph, fwd_nph;
+    // packed operations of the shared-memory layout (x and LU in one index space)
+    int compact, lu_offset;
+    const uint2 *fac_cops, *bwd_cops, *fwd_cops;
     const int *dpos;         // pivot position per column (m)
 };
 
@@ -80,6 +83,10 @@ size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem);
 // A.lu_in_smem and A.refine select the kernel variant.
 cudaError_t launch_nr_batch(const DevPlan &P, const BatchArgs &A, int precision, int threads, int grid,
                             size_t smem, cudaStream_t stream);
+// Copies the converged result rows of a compacted batch into case order (zero rows for
+// cases with map[c] < 0 or errs[map[c]] != 0).
+cudaError_t launch_scatter_case_rows(const double2 *src, const int *errs, const int *map, int ncases, int n,
+                                     double2 *dst, int num_sms, cudaStream_t st);
 // Resident CTAs per SM for a configuration (0 if it cannot launch).
 int nr_occupancy(int precision, bool lu_in_smem, bool refine, int threads, size_t smem);
 

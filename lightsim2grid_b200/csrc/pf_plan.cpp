@@ -157,6 +157,28 @@ struct ProgramBuilder {
 
 }  // namespace
 
+int compact_lu_offset(int m) { return (m + 1 + 3) & ~3; }
+
+bool compact_fits(const Plan &P) { return (long long)compact_lu_offset(P.m) + P.nnzLU <= 65536; }
+
+void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out) {
+    const unsigned L = (unsigned)compact_lu_offset(m), dummy = (unsigned)m;
+    const int n = pr.nops();
+    out.resize(2 * (size_t)n);
+    for (int o = 0; o < n; ++o) {
+        const unsigned x = (unsigned)pr.ops[4 * o], y = (unsigned)pr.ops[4 * o + 1], z = (unsigned)pr.ops[4 * o + 2];
+        const unsigned w = (unsigned)pr.ops[4 * o + 3] & 0x0fffffffu, kind = (unsigned)pr.ops[4 * o + 3] >> 28;
+        unsigned X = dummy, Y = dummy, Z = dummy, W = dummy;
+        if (kind == 0u) {
+            X = L + x; Y = L + y; Z = L + z; W = L + w;
+        } else if (kind == 2u) {
+            X = x; Y = L + y; Z = z; W = L + w;
+        }
+        out[2 * (size_t)o] = X | (Y << 16);
+        out[2 * (size_t)o + 1] = Z | (W << 16);
+    }
+}
+
 void host_jacobian(const Plan &P, const cplx *Yx, const cplx *V, std::vector<double> &Jx) {
     const int n = P.n;
     std::vector<cplx> Ibus(n, 0.0), dVm(P.nnzY), dVa(P.nnzY);
@@ -542,14 +564,13 @@ int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, con
         std::vector<std::vector<int>> byb(nb);
         for (int k = 0; k < m; ++k) byb[blev[k]].push_back(k);
         P.levels_bwd = nb;
+        // z(k) is kept undivided by U(k, k): a push divides by the pivot, and one scaling pass
+        // after the program divides every z(k) (no per-pivot division operations)
         ProgramBuilder B(P.backward, opt.threads);
-        for (int l = 0; l <= nb; ++l) {
+        for (int l = 0; l < nb; ++l) {
             B.begin();
-            if (l >= 1)
-                for (int k : byb[l - 1]) B.add(k, 0, 0, P.dpos[k], 4);
-            if (l < nb)
-                for (int k : byb[l])
-                    for (int p = P.colstart[k]; p < P.dpos[k]; ++p) B.add(P.Urow_k[p], p, k, P.dpos[k], 2);
+            for (int k : byb[l])
+                for (int p = P.colstart[k]; p < P.dpos[k]; ++p) B.add(P.Urow_k[p], p, k, P.dpos[k], 2);
             B.end();
         }
     }

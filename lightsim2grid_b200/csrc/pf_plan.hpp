@@ -82,7 +82,11 @@ struct Plan {
     // right-hand side fused in; `backward`: U z = y; `forward`: L y = b on its own (second
     // solve of a refinement).
     struct Program {
-        std::vector<int> ops;          // 4 ints per operation; kind 7 = empty slot
+        // 4 ints per operation (x, y, z, w | kind << 28):
+        //   kind 0: LU[x] -= LU[y] * LU[z] / LU[w]   (refactorisation update, L kept undivided)
+        //   kind 2: v[x]  -= LU[y] * v[z] / LU[w]    (substitution push)
+        //   kind 7: empty slot
+        std::vector<int> ops;
         std::vector<int> base;         // phase p = operations [base[p], base[p+1])
         std::vector<int> width;        // phase p: threads with work (the operation stride)
         int nphases() const { return (int)base.size() - 1; }
@@ -118,6 +122,13 @@ struct PlanOptions {
 int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, const cplx *V0, const cplx *Sbus,
                const int *slack_ids, int nslack, const double *weights, const int *pv, int npv, const int *pq,
                int npq, bool distributed, const PlanOptions &opt, std::string &msg);
+
+// Operations packed for a shared-memory LU: the solve vector and the LU share one index
+// space (v[k] -> k, a scratch slot for empty operations -> m, LU[i] -> lu_offset + i) with
+// 16 bits per index, so every operation is  s[x] -= s[y] * s[z] / s[w]  (8 bytes).
+int compact_lu_offset(int m);
+bool compact_fits(const Plan &P);
+void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out);  // 2 words per op
 
 // Host evaluation of the Jacobian values (J CSC order) at V for Ybus values Yx (CSC order).
 void host_jacobian(const Plan &P, const cplx *Yx, const cplx *V, std::vector<double> &Jx);

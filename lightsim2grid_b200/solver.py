@@ -210,7 +210,7 @@ class Plan:
             rows, cols, vals = np.zeros(1, np.int32), np.zeros(1, np.int32), np.zeros(1, np.complex128)
         V0 = nat.as_c128(V0).ravel()
         Sbus = nat.as_c128(Sbus).ravel()
-        Vout = np.zeros((ncases, self.n), dtype=np.complex128)
+        Vout = np.empty((ncases, self.n), dtype=np.complex128)  # every row is written
         conv = np.zeros(max(ncases, 1), dtype=np.int32)
         iters = np.zeros(max(ncases, 1), dtype=np.int32)
         errs = np.zeros(max(ncases, 1), dtype=np.int32)
