@@ -145,6 +145,19 @@ int pf_batch_device(pf_plan *plan, const pf_device_batch *batch, void *stream);
    cudaMalloc, cudaFree or allocating library routine. */
 int pf_batch_device_noalloc(pf_plan *plan, const pf_device_batch *batch, void *stream);
 
+/* pf_batch_device with working memory supplied by the caller: `scratch` (device memory,
+   256-byte aligned, `scratch_bytes` long) holds the launch's job counter and per-CTA slabs
+   (pf_scratch_bytes gives the size for a number of CTAs; the launch uses as many CTAs as fit).
+   Launches of one plan on different streams with disjoint scratch may overlap on the GPU: the
+   plan's device data is only read.  Used by the serving loop, which admits requests against a
+   device-memory budget.  No counterpart in the reference (its solvers own their memory). */
+int pf_batch_device_scratch(pf_plan *plan, const pf_device_batch *batch, void *scratch, long long scratch_bytes,
+                            void *stream);
+
+/* Scratch bytes pf_batch_device_scratch needs to run `ctas` CTAs at once (at most the plan's
+   grid); < 0 on error. */
+long long pf_scratch_bytes(const pf_plan *plan, int ctas);
+
 /* pf_batch_device, synchronously, with per-phase SM-cycle counters: out[0..7] = cycles summed
    over CTAs spent in mismatch, J fill, refactorisation, forward substitution, backward
    substitution, refinement (mixed form), voltage update / start-up, and the number of

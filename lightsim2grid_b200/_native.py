@@ -49,7 +49,8 @@ class PfDeviceBatch(ctypes.Structure):
 SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_get", "pf_set_ybus_values",
            "pf_solve", "pf_get_J", "pf_batch_n1", "pf_n1_prepare", "pf_batch_ts", "pf_batch_device", "pf_timers",
            "pf_host_jacobian_pattern", "pf_host_schedule_solve", "pf_batch_device_phase_cycles",
-           "pf_batch_device_phase_trace", "pf_batch_device_noalloc")
+           "pf_batch_device_phase_trace", "pf_batch_device_noalloc", "pf_batch_device_scratch",
+           "pf_scratch_bytes")
 
 
 def load(path=None):
@@ -96,6 +97,11 @@ def load(path=None):
                                                 f64p, ctypes.c_int]
     lib.pf_batch_device_noalloc.restype = ctypes.c_int
     lib.pf_batch_device_noalloc.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfDeviceBatch), ctypes.c_void_p]
+    lib.pf_batch_device_scratch.restype = ctypes.c_int
+    lib.pf_batch_device_scratch.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfDeviceBatch), ctypes.c_void_p,
+                                            ctypes.c_longlong, ctypes.c_void_p]
+    lib.pf_scratch_bytes.restype = ctypes.c_longlong
+    lib.pf_scratch_bytes.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.pf_timers.restype = ctypes.c_int
     lib.pf_timers.argtypes = [ctypes.c_void_p, f64p, ctypes.c_int]
     lib.pf_host_jacobian_pattern.restype = ctypes.c_int

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -603,9 +604,11 @@ BatchArgs device_args(const pf_device_batch *b) {
 
 int batch_device_with_scratch(pf_plan *pl, const pf_device_batch *b, void *stream, void *scratch,
                               size_t scratch_bytes) {
-    if (!pl || !b) return fail(-1, "pf_batch_device_noalloc: null argument");
+    if (!pl || !b || !scratch) return fail(-1, "batch with scratch: null argument");
+    if (reinterpret_cast<uintptr_t>(scratch) % 256 != 0)
+        return fail(-1, "batch with scratch: scratch not 256-byte aligned");
     const size_t head = 256;  // job counter
-    if (scratch_bytes <= head) return fail(-1, "pf_batch_device_noalloc: scratch too small");
+    if (scratch_bytes < head + pl->slab) return fail(-1, "batch with scratch: scratch holds no CTA slab");
     unsigned char *base = static_cast<unsigned char *>(scratch);
     l2g::BatchArgs a = l2g::device_args(b);
     return launch_into(pl, a, pl->precision, static_cast<cudaStream_t>(stream), base + head, scratch_bytes - head,
@@ -919,6 +922,18 @@ static int batch_device_impl(pf_plan *pl, const pf_device_batch *b, void *stream
     return launch(pl, a, pl->precision, static_cast<cudaStream_t>(stream));
 }
 
+
+int pf_batch_device_scratch(pf_plan *plan, const pf_device_batch *batch, void *scratch, long long scratch_bytes,
+                            void *stream) {
+    if (scratch_bytes <= 0) return fail(-1, "pf_batch_device_scratch: scratch too small");
+    return l2g::batch_device_with_scratch(plan, batch, stream, scratch, (size_t)scratch_bytes);
+}
+
+long long pf_scratch_bytes(const pf_plan *plan, int ctas) {
+    if (!plan || ctas <= 0) return fail(-1, "pf_scratch_bytes: invalid argument");
+    const int c = std::min(ctas, plan->grid);
+    return 256 + (long long)plan->slab * c;
+}
 
 int pf_batch_device(pf_plan *pl, const pf_device_batch *b, void *stream) {
     if (!pl || !b) return fail(-1, "pf_batch_device: null argument");
