@@ -14,6 +14,11 @@ Arms:
   --impl reference   the CPU restatement of the reference's loop (oracle/, the reference
                      itself cannot be built here) on all host threads, same metric.
 
+The ``serve`` object is the serving leg: Poisson arrivals (2,000 requests/s, 10 s by
+default) over six synthetic grids of 14 to 6,515 buses, half single power flows with
+perturbed injections and half N-1 batches of 8 to 64 outages, continuously batched on the
+GPU; it reports p50/p99 latency and throughput.
+
 Multi-GPU (torchrun): every rank runs the whole batch on its own GPU (replicas; the cases
 are independent and nothing is exchanged); value = total converged PFs / max-over-ranks time.
 """
@@ -27,6 +32,10 @@ import threading
 import time
 
 import numpy as np
+
+# the serving leg runs one stream per in-flight request: give them 32 hardware queues
+# (must be set before CUDA starts)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
@@ -166,6 +175,39 @@ def _cpu_oracle_n1(g, Vn, coeffs, threads):
     dt = time.perf_counter() - t0
     nconv = sum(int(r[2].sum()) for r in res)
     return nconv, dt
+
+
+SERVE_GRIDS = ("grid14", "grid118", "grid300", "grid1354", "grid2848", "grid6515")
+
+
+def _serve(seconds, rate, device):
+    """Serving leg: Poisson arrivals at `rate` requests/s for `seconds` over the six synthetic
+    grids (14 to 6,515 buses); half the requests are one power flow with injections scaled by
+    U[0.9, 1.1] per bus, half an N-1 batch of 8 to 64 outages; mixed precision, tol 1e-8."""
+    from lightsim2grid_b200 import synthetic
+    from lightsim2grid_b200.serving import PowerFlowServer, latency_stats, make_requests
+
+    grids = {g: synthetic.make_named_grid(g)[0] for g in SERVE_GRIDS}
+    budget, slots = 4 << 30, 32
+    srv = PowerFlowServer(grids, device=device, hbm_budget=budget, slots=slots, precision=1, max_iter=MAX_ITER,
+                          tol=TOL)
+    nb = {k: v.n_bus for k, v in grids.items()}
+    nbr = {k: v.nb_powerline() for k, v in grids.items()}
+    srv.serve(make_requests(nb, rate=rate, duration=min(1.0, seconds), seed=12345, branches_of=nbr))  # warm-up
+    reqs = make_requests(nb, rate=rate, duration=seconds, seed=2024, branches_of=nbr)
+    done = srv.serve(reqs, realtime=True)
+    st = latency_stats(done)
+    per = {}
+    for g in SERVE_GRIDS:
+        lat = np.array([r.latency for r in done if r.grid == g])
+        if lat.size:
+            per[g] = {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)}
+    st.update({"duration_s": seconds, "arrival_rate": rate, "grids": list(SERVE_GRIDS), "per_grid": per,
+               "slots": slots, "hbm_budget_bytes": budget, "peak_inflight": srv.last.peak_inflight,
+               "peak_bytes": srv.last.peak_bytes, "rejected": len(srv.last.rejected),
+               "latency": "arrival to result in pinned host memory (host clock)",
+               "kernel_launches": len([r for r in done if r.ninst > 0])})
+    return st
 
 
 def _host_threads():
@@ -332,16 +374,20 @@ def run_ours(args):
     if traffic_per_unit is not None:
         traffic = float(traffic_per_unit * float(np.sum(mixed["iters"])))
 
-    # e2e through the host C-ABI (host buffers, copies in the timed region)
+    # e2e through the host C-ABI (host buffers, copies in the timed region); results land in
+    # pinned host arrays, inputs are the host coefficient arrays
     plan_e2e = mixed["plan"]
+    nc = len(coeffs)
+    pinned = (torch.empty(nc * n * 2, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(nc, n),
+              *(torch.empty(nc, dtype=torch.int32, pin_memory=True).numpy() for _ in range(3)))
     for _ in range(max(1, min(args.warmup, 2))):
-        plan_e2e.batch_n1_arrays(cp, rows, cols, vals, Vn, S, MAX_ITER, TOL)
+        plan_e2e.batch_n1_arrays(cp, rows, cols, vals, Vn, S, MAX_ITER, TOL, out=pinned)
     torch.cuda.synchronize()
     e2e_times, e2e_conv = [], 0
     ke = max(2, min(args.steps, 5))
     for _ in range(ke):
         t0 = time.perf_counter()
-        Vout, conv, iters, errs = plan_e2e.batch_n1_arrays(cp, rows, cols, vals, Vn, S, MAX_ITER, TOL)
+        Vout, conv, iters, errs = plan_e2e.batch_n1_arrays(cp, rows, cols, vals, Vn, S, MAX_ITER, TOL, out=pinned)
         e2e_times.append(time.perf_counter() - t0)
         e2e_conv = int(conv.sum())
     e2e_t = float(np.mean(e2e_times))
@@ -352,6 +398,10 @@ def run_ours(args):
     ns = mixed["ns"]
     h2d = 2 * n * 16 + (ns + 1) * 4 + int(cp[-1]) * (4 + 16) + 2 * ns * 4
     d2h = ns * n * 16 + 2 * ns * 4
+
+    serve = None
+    if ws == 1 and args.serve_seconds > 0:
+        serve = _serve(args.serve_seconds, args.serve_rate, dev)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -396,13 +446,14 @@ def run_ours(args):
             "e2e": {"value": ws * e2e_conv / e2e_t, "unit": "PF/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_t,
                     "path": "Plan.batch_n1_arrays -> pf_batch_n1 (host buffers; islanding check, uploads, kernel, "
-                            "download of all voltages)"},
+                            "download of all voltages into pinned host arrays)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "nr_batch_kernel<float,float>",
                          "algorithmic_bytes_per_launch": mixed["abytes"],
                          "algorithmic_bytes_per_instance_iteration": mixed["per_it"],
                          "kernel_ms": 1e3 * kt},
+            "serve": serve if serve is not None else {"skipped": "serving is measured at n_gpus = 1"},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": args.steps,
@@ -424,6 +475,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline leg")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="serving leg duration (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving leg arrival rate (requests/s)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -17,6 +17,10 @@
 // refines every Newton step once against the FP64 Jacobian, computed on the fly from dS/dV.
 #include "pf_engine.cuh"
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 namespace l2g {
 
 namespace {
@@ -570,11 +574,33 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const
 #undef L2G_MARK
 }
 
+// Raises a kernel's dynamic shared-memory limit to everything the device allows, once per
+// kernel and device (launches then pass their own size; setting the attribute on every
+// launch would make concurrent launches on other streams wait on the driver).
+cudaError_t allow_max_smem(const void *fn) {
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({fn, dev})) return cudaSuccess;
+    int optin = 0;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, fn);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    if (e != cudaSuccess) return e;
+    done.insert({fn, dev});
+    return cudaSuccess;
+}
+
 template <typename LT, typename XT, bool SM, bool RF>
 cudaError_t launch_variant(const DevPlan &P, const BatchArgs &A, int threads, int grid, size_t smem,
                            cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(nr_batch_kernel<LT, XT, SM, RF>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_max_smem(reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF>));
     if (e != cudaSuccess) return e;
     nr_batch_kernel<LT, XT, SM, RF><<<grid, threads, smem, st>>>(P, A);
     return cudaGetLastError();
@@ -583,9 +609,7 @@ cudaError_t launch_variant(const DevPlan &P, const BatchArgs &A, int threads, in
 template <typename LT, typename XT, bool SM, bool RF>
 int occupancy_variant(int threads, size_t smem) {
     int nb = 0;
-    if (cudaFuncSetAttribute(nr_batch_kernel<LT, XT, SM, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-        return 0;
+    if (allow_max_smem(reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF>)) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, nr_batch_kernel<LT, XT, SM, RF>, threads, smem) !=
         cudaSuccess)
         return 0;

@@ -25,6 +25,9 @@ def main():
     ap.add_argument("--lu-placement", type=int, default=0)
     ap.add_argument("--fuse-forward", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
+    ap.add_argument("--refine", type=int, default=0, help="0 default (on), 1 on, 2 off")
+    ap.add_argument("--refine-threshold", type=float, default=0.0)
+    ap.add_argument("--check", action="store_true", help="compare the voltages with an FP64 plan's")
     args = ap.parse_args()
 
     import torch
@@ -40,7 +43,8 @@ def main():
     nb = g.nb_powerline() if args.cases <= 0 else min(args.cases, g.nb_powerline())
     coeffs = [g.branch_coeffs([b]) for b in range(nb)]
     plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, threads=args.threads,
-                lu_placement=args.lu_placement, fuse_forward=args.fuse_forward, max_ctas_per_sm=args.ctas_per_sm)
+                lu_placement=args.lu_placement, fuse_forward=args.fuse_forward, max_ctas_per_sm=args.ctas_per_sm,
+                refine=args.refine, refine_threshold=args.refine_threshold)
     lib = plan._lib
     cp = np.zeros(nb + 1, np.int32)
     rows, cols, vals = [], [], []
@@ -96,7 +100,27 @@ def main():
     trace = np.diff(tr[:ntr]).astype(int).tolist()
     it = bufs[8].cpu().numpy()
     er = bufs[9].cpu().numpy()
-    out = {"grid": args.grid, "cases": ns, "precision": args.precision, "ms": times,
+    check = None
+    if args.check:
+        ref = Plan(Y, Vn, S, sl, w, pv, pq, precision=0)
+        Vf = torch.zeros_like(bufs[7])
+        itf = torch.zeros_like(bufs[8])
+        erf = torch.zeros_like(bufs[9])
+        b2 = nat.PfDeviceBatch(n_inst=ns, V0=bufs[0].data_ptr(), v0_stride=0, Sbus=bufs[1].data_ptr(), sbus_stride=0,
+                               ovr_ptr=bufs[2].data_ptr(), ovr_pos=bufs[3].data_ptr(), ovr_val=bufs[4].data_ptr(),
+                               max_iter=10, tol=1e-8, chain=0, job_first=bufs[5].data_ptr(),
+                               job_count=bufs[6].data_ptr(), njobs=ns, Vout=Vf.data_ptr(), iters=itf.data_ptr(),
+                               errs=erf.data_ptr())
+        assert ref._lib.pf_batch_device(ref.handle, nat.ctypes.byref(b2), stream.cuda_stream) == 0
+        torch.cuda.synchronize()
+        ef = erf.cpu().numpy()
+        both = (er == 0) & (ef == 0)
+        Vm = bufs[7].cpu().numpy().view(np.complex128).reshape(ns, -1)
+        Vr = Vf.cpu().numpy().view(np.complex128).reshape(ns, -1)
+        check = {"flags_equal": bool(np.array_equal(er == 0, ef == 0)),
+                 "max_abs_dV_vs_fp64": float(np.abs(Vm[both] - Vr[both]).max()) if both.any() else None,
+                 "iterations_fp64": int(itf.cpu().numpy().sum())}
+    out = {"grid": args.grid, "cases": ns, "precision": args.precision, "ms": times, "check": check,
            "converged": int((er == 0).sum()), "iterations": int(it.sum()),
            "pf_per_s": float((er == 0).sum() / (np.mean(times) * 1e-3)),
            "cycles_per_iteration_per_cta": float(tot / max(1, int(it.sum()))), "phase_share": phase_share,

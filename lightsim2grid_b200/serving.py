@@ -16,6 +16,10 @@ module serves both request kinds for many grids at once:
 
 ``Dispatcher`` holds the admission policy and bookkeeping and runs against any executor;
 ``CudaExecutor`` launches through the C ABI (``pf_batch_device_scratch``).
+
+CUDA maps streams onto ``CUDA_DEVICE_MAX_CONNECTIONS`` hardware queues (8 unless set), and
+launches that share a queue wait for one another; a serving process sets it to 32 before
+CUDA starts (``configure_process``) so that a short request is not queued behind a long one.
 """
 import collections
 import time
@@ -26,6 +30,13 @@ from . import _native as nat
 from .solver import Plan
 
 PF, N1 = "pf", "n1"
+
+
+def configure_process():
+    """Call before the process first uses CUDA: 32 hardware queues for the streams."""
+    import os
+
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 
 class Request:
@@ -88,6 +99,7 @@ class Dispatcher:
         self.rejected = []
         self.peak_bytes = 0
         self.peak_inflight = 0
+        self.host_s = {"submit": 0.0, "launch": 0.0, "poll": 0.0}  # host seconds spent per step
 
     def submit(self, req):
         req.nbytes = self.ex.bytes_needed(req)
@@ -100,7 +112,7 @@ class Dispatcher:
         n = 0
         while self.pending and len(self.inflight) < self.slots:
             req = self.pending[0]
-            if self.in_use + req.nbytes > self.budget:
+            if self.in_use + req.nbytes > self.budget or not self.ex.reserve(req):
                 break
             self.pending.popleft()
             self.in_use += req.nbytes
@@ -132,13 +144,21 @@ class Dispatcher:
         i, total = 0, len(reqs)
         while len(self.done) + len(self.rejected) < total:
             t = now()
+            h0 = clock()
             while i < total and (not realtime or reqs[i].arrival <= t):
                 if not realtime:
                     reqs[i].arrival = t
                 self.submit(reqs[i])
                 i += 1
+            h1 = clock()
             self.admit(t)
-            if not self.complete(now) and not self.inflight and not self.pending and i < total:
+            h2 = clock()
+            finished = self.complete(now)
+            h3 = clock()
+            self.host_s["submit"] += h1 - h0
+            self.host_s["launch"] += h2 - h1
+            self.host_s["poll"] += h3 - h2
+            if not finished and not self.inflight and not self.pending and i < total:
                 # idle until the next arrival
                 wait = reqs[i].arrival - now()
                 if wait > 0:
@@ -201,13 +221,11 @@ class GridService:
     def n1_overrides(self, branches):
         """(solvable mask, ovr_ptr, ovr_pos, ovr_val) for the given branches, compacted."""
         branches = np.asarray(branches, np.int64)
+        lens = (self.cptr[branches + 1] - self.cptr[branches]).astype(np.int64)
         cp = np.zeros(branches.size + 1, np.int32)
-        idx = []
-        for k, b in enumerate(branches):
-            a, e = self.cptr[b], self.cptr[b + 1]
-            cp[k + 1] = cp[k] + (e - a)
-            idx.extend(range(a, e))
-        idx = np.asarray(idx, np.int64)
+        np.cumsum(lens, out=cp[1:])
+        starts = np.repeat(self.cptr[branches].astype(np.int64) - cp[:-1], lens)
+        idx = starts + np.arange(int(cp[-1]), dtype=np.int64)
         rows, cols = np.ascontiguousarray(self.rows[idx]), np.ascontiguousarray(self.cols[idx])
         vals = np.ascontiguousarray(self.vals[idx]) if idx.size else np.zeros(1, np.complex128)
         if idx.size == 0:
@@ -227,109 +245,159 @@ class GridService:
         return solv.astype(bool), optr[:ns + 1].copy(), opos[:nw].copy(), oval[:nw].copy()
 
 
-class CudaExecutor:
-    """Runs each admitted request as its own launch on its own stream slot: inputs are copied
-    from the slot's pinned host buffer, the kernel runs with working memory sized for the
-    request, results are copied back to the slot's pinned output buffer; ``poll`` reports
-    finished requests.  Pinned buffers are sized once for the largest grid and
-    ``max_instances`` instances."""
+def _align(n, a=256):
+    return (int(n) + a - 1) // a * a
 
-    def __init__(self, services, device, slots, max_instances=64):
+
+class DeviceArena:
+    """First-fit allocator over one device allocation of ``nbytes`` (the serving budget):
+    every request's inputs, outputs and kernel working memory live in one region of it, so
+    serving allocates no device memory after start-up."""
+
+    def __init__(self, nbytes, device):
+        import torch
+
+        self.size = _align(nbytes)
+        self.buf = torch.empty(self.size, dtype=torch.uint8, device=device)
+        self.base = self.buf.data_ptr()
+        self.holes = [(0, self.size)]  # (offset, size), sorted by offset, coalesced
+
+    def alloc(self, n):
+        n = _align(n)
+        for i, (o, sz) in enumerate(self.holes):
+            if sz >= n:
+                if sz == n:
+                    del self.holes[i]
+                else:
+                    self.holes[i] = (o + n, sz - n)
+                return o
+        return None
+
+    def release(self, o, n):
+        n = _align(n)
+        h = self.holes
+        i = 0
+        while i < len(h) and h[i][0] < o:
+            i += 1
+        h.insert(i, (o, n))
+        if i + 1 < len(h) and h[i][0] + h[i][1] == h[i + 1][0]:
+            h[i] = (h[i][0], h[i][1] + h[i + 1][1])
+            del h[i + 1]
+        if i > 0 and h[i - 1][0] + h[i - 1][1] == h[i][0]:
+            h[i - 1] = (h[i - 1][0], h[i - 1][1] + h[i][1])
+            del h[i]
+
+    def free_bytes(self):
+        return sum(sz for _, sz in self.holes)
+
+
+class CudaExecutor:
+    """Runs each admitted request as its own launch on its own stream slot.  A request's
+    device region (from the arena) holds its inputs, outputs and the kernel's working memory;
+    inputs are copied from the slot's pinned host buffer, results back to the slot's pinned
+    output buffer; ``poll`` reports finished requests.  Pinned buffers are sized once for the
+    largest grid and ``max_instances`` instances."""
+
+    def __init__(self, services, device, slots, arena, max_instances=64):
         import torch
 
         self.torch = torch
         self.sv = services
         self.device = device
+        self.arena = arena
         self.max_k = int(max_instances)
         nmax = max(s.n for s in services.values())
         in_bytes = max(nmax * 16, self.max_k * 4 * 24 + 8 * (self.max_k + 1)) + 1024
         out_bytes = self.max_k * nmax * 16 + 16 * self.max_k + 1024
         self.free = [(torch.cuda.Stream(device), torch.empty(in_bytes, dtype=torch.uint8, pin_memory=True),
                       torch.empty(out_bytes, dtype=torch.uint8, pin_memory=True)) for _ in range(slots)]
+        # job lists (instance j = job j) shared by every launch: read only
+        self.jf = torch.arange(self.max_k, dtype=torch.int32, device=device)
+        self.jc = torch.ones(self.max_k, dtype=torch.int32, device=device)
         self.active = {}
         self.prepared = {}
 
     def bytes_needed(self, req):
+        """Region layout: [scratch | outputs (V, iters, errs) | inputs]; returns its size."""
         s = self.sv[req.grid]
         if req.kind == PF:
             k, ov = 1, None
+            inputs = [_align(s.n * 16)]
         else:
             ov = s.n1_overrides(req.branches)
             k = int(ov[0].sum())
+            inputs = [_align(4 * (k + 1)), _align(4 * max(ov[2].size, 1)), _align(16 * max(ov[3].size, 1))]
         if k > self.max_k:
             raise ValueError("request {} has {} instances (at most {})".format(req.rid, k, self.max_k))
         req.ninst = k
-        self.prepared[req.rid] = ov
         ctas = max(1, min(k, s.grid_ctas))
-        scratch = int(s.plan._lib.pf_scratch_bytes(s.plan.handle, ctas))
-        nb = scratch + k * s.n * 16 + 16 * k + 8 * (k + 1)
-        nb += s.n * 16 if req.kind == PF else ov[2].size * 20 + 4 * (k + 1)
-        return nb
+        scratch = _align(s.plan._lib.pf_scratch_bytes(s.plan.handle, ctas)) if k else 0
+        outs = _align(k * s.n * 16 + 8 * k)
+        self.prepared[req.rid] = [ov, scratch, outs, inputs, None]
+        return scratch + outs + sum(inputs)
 
-    @staticmethod
-    def _put(pin, off, arr):
-        """Copies a numpy array into the pinned buffer at byte offset `off` (16-aligned)."""
-        b = np.ascontiguousarray(arr).view(np.uint8).ravel()
-        pin.numpy()[off:off + b.size] = b
-        return off, b.size, (off + b.size + 15) & ~15
+    def reserve(self, req):
+        prep = self.prepared[req.rid]
+        o = self.arena.alloc(req.nbytes)
+        if o is None:
+            return False
+        prep[4] = o
+        return True
 
     def launch(self, req):
         torch = self.torch
         s = self.sv[req.grid]
-        ov = self.prepared.pop(req.rid, None)
+        ov, scratch, outs, inputs, off = self.prepared.pop(req.rid)
         st, pin_in, pin_out = self.free.pop()
-        dev = self.device
         k = req.ninst
-        keep = {}
+        buf, base = self.arena.buf, self.arena.base
         with torch.cuda.stream(st):
             if k == 0:
                 ev = torch.cuda.Event()
                 ev.record(st)
-                self.active[req.rid] = (req, (st, pin_in, pin_out), ev, keep)
+                self.active[req.rid] = (req, (st, pin_in, pin_out), ev, off)
                 return
+            o_scr, o_out = off, off + scratch
+            o_in = o_out + outs
+            pin = pin_in.numpy()
 
-            def upload(name, arr, dtype):
-                nonlocal off
-                o, nb, off = self._put(pin_in, off, arr)
-                t = torch.empty(nb, dtype=torch.uint8, device=dev)
-                t.copy_(pin_in[o:o + nb], non_blocking=True)
-                keep[name] = t
-                return t.data_ptr()
+            def upload(arr, size):
+                nonlocal o_in
+                b = np.ascontiguousarray(arr).view(np.uint8).ravel()
+                p0 = o_in - (off + scratch + outs)
+                pin[p0:p0 + b.size] = b
+                buf[o_in:o_in + b.size].copy_(pin_in[p0:p0 + b.size], non_blocking=True)
+                ptr = base + o_in
+                o_in += size
+                return ptr
 
-            off = 0
             if req.kind == PF:
-                sbus = upload("S", (s.Sbase * req.scale).astype(np.complex128), np.complex128)
+                sbus = upload((s.Sbase * req.scale).astype(np.complex128), inputs[0])
                 optr_d = opos_d = oval_d = 0
             else:
                 solv, optr, opos, oval = ov
-                optr_d = upload("optr", optr, np.int32)
-                opos_d = upload("opos", opos if opos.size else np.zeros(1, np.int32), np.int32)
-                oval_d = upload("oval", oval if oval.size else np.zeros(1, np.complex128), np.complex128)
+                optr_d = upload(optr, inputs[0])
+                opos_d = upload(opos if opos.size else np.zeros(1, np.int32), inputs[1])
+                oval_d = upload(oval if oval.size else np.zeros(1, np.complex128), inputs[2])
                 sbus = s.Sbase_dev.data_ptr()
-            ctas = max(1, min(k, s.grid_ctas))
-            sb = int(s.plan._lib.pf_scratch_bytes(s.plan.handle, ctas))
-            keep["scratch"] = torch.empty(sb, dtype=torch.uint8, device=dev)
-            keep["jf"] = torch.arange(k, dtype=torch.int32, device=dev)
-            keep["jc"] = torch.ones(k, dtype=torch.int32, device=dev)
-            keep["out"] = torch.empty(k * s.n * 16 + 8 * k, dtype=torch.uint8, device=dev)
-            vo = keep["out"].data_ptr()
+            vo = base + o_out
             b = nat.PfDeviceBatch(n_inst=k, V0=s.Vbase_dev.data_ptr(), v0_stride=0, Sbus=sbus, sbus_stride=0,
                                   ovr_ptr=optr_d, ovr_pos=opos_d, ovr_val=oval_d, max_iter=s.max_iter, tol=s.tol,
-                                  chain=0, job_first=keep["jf"].data_ptr(), job_count=keep["jc"].data_ptr(),
+                                  chain=0, job_first=self.jf.data_ptr(), job_count=self.jc.data_ptr(),
                                   njobs=k, Vout=vo, iters=vo + k * s.n * 16, errs=vo + k * s.n * 16 + 4 * k)
-            rc = s.plan._lib.pf_batch_device_scratch(s.plan.handle, nat.ctypes.byref(b), keep["scratch"].data_ptr(),
-                                                     sb, st.cuda_stream)
+            rc = s.plan._lib.pf_batch_device_scratch(s.plan.handle, nat.ctypes.byref(b), base + o_scr, scratch,
+                                                     st.cuda_stream)
             if rc != 0:
                 raise RuntimeError(nat.last_error(s.plan._lib))
             nout = k * s.n * 16 + 8 * k
-            pin_out[:nout].copy_(keep["out"], non_blocking=True)
+            pin_out[:nout].copy_(buf[o_out:o_out + nout], non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(st)
-        self.active[req.rid] = (req, (st, pin_in, pin_out), ev, keep)
+        self.active[req.rid] = (req, (st, pin_in, pin_out), ev, off)
 
     def poll(self):
         fin = []
-        for rid, (req, slot, ev, keep) in list(self.active.items()):
+        for rid, (req, slot, ev, off) in list(self.active.items()):
             if not ev.query():
                 continue
             s = self.sv[req.grid]
@@ -346,6 +414,7 @@ class CudaExecutor:
                 req.errs = raw[nv + 4 * k:nv + 8 * k].view(np.int32).copy()
                 req.converged = req.errs == 0
                 req.V[~req.converged] = 0.0
+            self.arena.release(off, req.nbytes)
             del self.active[rid]
             self.free.append(slot)
             fin.append(rid)
@@ -355,7 +424,7 @@ class CudaExecutor:
 class PowerFlowServer:
     """Grids served from one GPU.  ``grids``: name -> GridModel."""
 
-    def __init__(self, grids, device=None, hbm_budget=4 << 30, slots=32, precision=1, max_iter=10, tol=1e-8,
+    def __init__(self, grids, device=None, hbm_budget=2 << 30, slots=32, precision=1, max_iter=10, tol=1e-8,
                  max_instances=64, **plan_options):
         import torch
 
@@ -366,7 +435,8 @@ class PowerFlowServer:
 
     def executor(self):
         if getattr(self, "_ex", None) is None:
-            self._ex = CudaExecutor(self.services, self.device, self.slots, self.max_instances)
+            self.arena = DeviceArena(self.hbm_budget, self.device)
+            self._ex = CudaExecutor(self.services, self.device, self.slots, self.arena, self.max_instances)
         return self._ex
 
     def serve(self, requests, realtime=True):

@@ -201,7 +201,10 @@ class Plan:
                 vals.append(y)
         return self.batch_n1_arrays(cptr_, rows, cols, vals, V0, Sbus, max_iter, tol)
 
-    def batch_n1_arrays(self, case_ptr, rows, cols, vals, V0, Sbus, max_iter, tol):
+    def batch_n1_arrays(self, case_ptr, rows, cols, vals, V0, Sbus, max_iter, tol, out=None):
+        """N-1 batch from flat coefficient arrays.  ``out``: optional ``(V[ncases, n] complex128,
+        conv, iters, errs int32[ncases])`` arrays to write into (e.g. views of pinned host memory,
+        which the device copies into at full bus speed); fresh arrays otherwise."""
         case_ptr = nat.as_i32(case_ptr)
         ncases = case_ptr.size - 1
         rows, cols = nat.as_i32(rows), nat.as_i32(cols)
@@ -210,10 +213,18 @@ class Plan:
             rows, cols, vals = np.zeros(1, np.int32), np.zeros(1, np.int32), np.zeros(1, np.complex128)
         V0 = nat.as_c128(V0).ravel()
         Sbus = nat.as_c128(Sbus).ravel()
-        Vout = np.empty((ncases, self.n), dtype=np.complex128)  # every row is written
-        conv = np.zeros(max(ncases, 1), dtype=np.int32)
-        iters = np.zeros(max(ncases, 1), dtype=np.int32)
-        errs = np.zeros(max(ncases, 1), dtype=np.int32)
+        if out is not None:
+            Vout, conv, iters, errs = out
+            ok = (Vout.dtype == np.complex128 and Vout.shape == (ncases, self.n) and Vout.flags.c_contiguous
+                  and all(a.dtype == np.int32 and a.size >= max(ncases, 1) and a.flags.c_contiguous
+                          for a in (conv, iters, errs)))
+            if not ok:
+                raise ValueError("out arrays must be V[ncases, n] complex128 and three int32[ncases], contiguous")
+        else:
+            Vout = np.empty((ncases, self.n), dtype=np.complex128)  # every row is written
+            conv = np.zeros(max(ncases, 1), dtype=np.int32)
+            iters = np.zeros(max(ncases, 1), dtype=np.int32)
+            errs = np.zeros(max(ncases, 1), dtype=np.int32)
         rc = self._lib.pf_batch_n1(self._h, ncases, nat.ptr(case_ptr, nat.i32p), nat.ptr(rows, nat.i32p),
                                    nat.ptr(cols, nat.i32p), nat.cptr(vals), nat.cptr(V0), nat.cptr(Sbus),
                                    int(max_iter), float(tol), nat.cptr(Vout), nat.ptr(conv, nat.i32p),

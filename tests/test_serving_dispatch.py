@@ -29,6 +29,9 @@ class FakeExecutor:
         req.ninst = 1 if req.kind == PF else len(req.branches)
         return req.ninst * 1000
 
+    def reserve(self, req):
+        return True
+
     def launch(self, req):
         self.order.append(req.rid)
         self.running[req.rid] = self.clock.t + 2e-3 * req.ninst
@@ -104,3 +107,34 @@ def test_request_generator_is_seeded_and_shaped():
             assert r.branches.max() < nbr[r.grid]
     frac_pf = np.mean([r.kind == PF for r in r1])
     assert 0.4 < frac_pf < 0.6
+
+
+def test_device_arena_first_fit_and_coalescing():
+    """The serving arena on a CPU buffer: random allocations never overlap, stay aligned and
+    inside the arena, and freeing everything coalesces back to one hole."""
+    from lightsim2grid_b200.serving import DeviceArena
+
+    a = DeviceArena(1 << 20, "cpu")
+    rng = np.random.default_rng(4)
+    live = {}
+    for step in range(2000):
+        if live and (rng.random() < 0.45 or len(live) > 40):
+            key = list(live)[int(rng.integers(len(live)))]
+            o, n = live.pop(key)
+            a.release(o, n)
+        else:
+            n = int(rng.integers(1, 60000))
+            o = a.alloc(n)
+            if o is None:
+                assert a.free_bytes() < 1 << 20
+                continue
+            assert o % 256 == 0 and o + n <= a.size
+            for (p, m) in live.values():
+                assert o + n <= p or p + m <= o
+            live[step] = (o, n)
+        # holes sorted, disjoint, coalesced
+        h = a.holes
+        assert all(h[i][0] + h[i][1] < h[i + 1][0] for i in range(len(h) - 1))
+    for o, n in live.values():
+        a.release(o, n)
+    assert a.holes == [(0, a.size)]
