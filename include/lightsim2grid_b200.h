@@ -154,6 +154,23 @@ int pf_batch_device_noalloc(pf_plan *plan, const pf_device_batch *batch, void *s
 int pf_batch_device_scratch(pf_plan *plan, const pf_device_batch *batch, void *scratch, long long scratch_bytes,
                             void *stream);
 
+/* One launch over several plans (grids of different sizes), config "uneven-size batched N-1":
+   batch i belongs to plans[i] (device-resident inputs and outputs, as for pf_batch_device;
+   its job fields are ignored).  The launch's job list lives in device memory: job j runs
+   instances [job_first[j], job_first[j] + job_count[j]) of segment job_seg[j]; CTAs take jobs
+   in list order, so put the costly ones first.  The plans must share device, precision,
+   refinement and LU placement; the launch uses the largest thread count, shared-memory layout
+   and slab among them.  pf_multi_create uploads the segment table and allocates the scratch
+   once; pf_multi_launch is asynchronous, allocates nothing and can be captured in a CUDA graph.
+   No counterpart in the reference (one solver object per grid). */
+typedef struct pf_multi pf_multi;
+int pf_multi_create(pf_plan *const *plans, const pf_device_batch *batches, int nseg, const int *job_seg,
+                    const int *job_first, const int *job_count, int njobs, pf_multi **out);
+int pf_multi_launch(pf_multi *multi, void *stream);
+int pf_multi_info(const pf_multi *multi, int *threads, int *grid, long long *shared_bytes,
+                  long long *scratch_bytes);
+void pf_multi_destroy(pf_multi *multi);
+
 /* Scratch bytes pf_batch_device_scratch needs to run `ctas` CTAs at once (at most the plan's
    grid); < 0 on error. */
 long long pf_scratch_bytes(const pf_plan *plan, int ctas);

@@ -50,7 +50,7 @@ SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_g
            "pf_solve", "pf_get_J", "pf_batch_n1", "pf_n1_prepare", "pf_batch_ts", "pf_batch_device", "pf_timers",
            "pf_host_jacobian_pattern", "pf_host_schedule_solve", "pf_batch_device_phase_cycles",
            "pf_batch_device_phase_trace", "pf_batch_device_noalloc", "pf_batch_device_scratch",
-           "pf_scratch_bytes")
+           "pf_scratch_bytes", "pf_multi_create", "pf_multi_launch", "pf_multi_info", "pf_multi_destroy")
 
 
 def load(path=None):
@@ -102,6 +102,17 @@ def load(path=None):
                                             ctypes.c_longlong, ctypes.c_void_p]
     lib.pf_scratch_bytes.restype = ctypes.c_longlong
     lib.pf_scratch_bytes.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.pf_multi_create.restype = ctypes.c_int
+    lib.pf_multi_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(PfDeviceBatch), ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_void_p)]
+    lib.pf_multi_launch.restype = ctypes.c_int
+    lib.pf_multi_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    lib.pf_multi_info.restype = ctypes.c_int
+    lib.pf_multi_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+    lib.pf_multi_destroy.restype = None
+    lib.pf_multi_destroy.argtypes = [ctypes.c_void_p]
     lib.pf_timers.restype = ctypes.c_int
     lib.pf_timers.argtypes = [ctypes.c_void_p, f64p, ctypes.c_int]
     lib.pf_host_jacobian_pattern.restype = ctypes.c_int

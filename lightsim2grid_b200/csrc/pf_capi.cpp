@@ -86,6 +86,17 @@ struct pf_plan {
     bool graph_symmetric = true;
 };
 
+// A launch over several plans (pf_multi_create): segment table, scratch and job lists.
+struct pf_multi {
+    std::vector<pf_plan *> plans;
+    int device = 0, precision = 0, threads = 0, grid = 0, num_sms = 0;
+    bool lu_in_smem = false, refine = false;
+    size_t smem = 0, slab = 0;
+    DevBuf segs, scratch, counter;
+    l2g::Segment seg0{};
+    l2g::MultiArgs M{};
+};
+
 namespace {
 
 // ------------------------------------------------------------------ islanding check
@@ -1125,6 +1136,108 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         info->flops_refactor = P.flops_refactor;
     }
     return 0;
+}
+
+
+int pf_multi_create(pf_plan *const *plans, const pf_device_batch *batches, int nseg, const int *job_seg,
+                    const int *job_first, const int *job_count, int njobs, pf_multi **out) {
+    if (!out || !plans || !batches || nseg <= 0 || njobs < 0 || (njobs > 0 && (!job_seg || !job_first || !job_count)))
+        return fail(-1, "pf_multi_create: invalid argument");
+    *out = nullptr;
+    pf_multi *mp = new pf_multi();
+    for (int i = 0; i < nseg; ++i) {
+        pf_plan *pl = plans[i];
+        if (!pl) {
+            delete mp;
+            return fail(-1, "pf_multi_create: null plan");
+        }
+        if (i == 0) {
+            mp->device = pl->device;
+            mp->precision = pl->precision;
+            mp->refine = pl->refine;
+            mp->lu_in_smem = pl->lu_in_smem;
+            mp->num_sms = pl->num_sms;
+        } else if (pl->device != mp->device || pl->precision != mp->precision || pl->refine != mp->refine ||
+                   pl->lu_in_smem != mp->lu_in_smem) {
+            delete mp;
+            return fail(-1, "pf_multi_create: plans differ in device, precision, refinement or LU placement");
+        }
+        mp->plans.push_back(pl);
+        mp->threads = std::max(mp->threads, pl->threads);
+        mp->smem = std::max(mp->smem, pl->smem);
+        mp->slab = std::max(mp->slab, pl->slab);
+    }
+    int occ = l2g::nr_occupancy(mp->precision, mp->lu_in_smem, mp->refine, mp->threads, mp->smem);
+    if (occ <= 0) {
+        delete mp;
+        return fail(-1, "pf_multi_create: the plans' largest layout cannot be launched");
+    }
+    mp->grid = std::max(1, std::min(mp->num_sms * occ, std::max(njobs, 1)));
+    cudaError_t e;
+    if ((e = mp->scratch.ensure(mp->slab * (size_t)mp->grid)) != cudaSuccess ||
+        (e = mp->counter.ensure(256)) != cudaSuccess ||
+        (e = mp->segs.ensure(sizeof(l2g::Segment) * (size_t)nseg)) != cudaSuccess) {
+        for (DevBuf *b : {&mp->scratch, &mp->counter, &mp->segs}) b->release();
+        delete mp;
+        return cuda_fail(e, "pf_multi_create: allocation");
+    }
+    std::vector<l2g::Segment> host(nseg);
+    for (int i = 0; i < nseg; ++i) {
+        pf_plan *pl = plans[i];
+        l2g::Segment &sg = host[i];
+        sg.P = pl->dp;
+        sg.A = l2g::device_args(&batches[i]);
+        sg.A.scratch = static_cast<unsigned char *>(mp->scratch.p);
+        sg.A.slab_bytes = (long long)mp->slab;
+        sg.A.job_counter = nullptr;  // jobs come from the launch's list
+        sg.A.lu_in_smem = mp->lu_in_smem ? 1 : 0;
+        sg.A.refine = mp->refine ? 1 : 0;
+        sg.A.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
+    }
+    e = cudaMemcpy(mp->segs.p, host.data(), sizeof(l2g::Segment) * (size_t)nseg, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        for (DevBuf *b : {&mp->scratch, &mp->counter, &mp->segs}) b->release();
+        delete mp;
+        return cuda_fail(e, "pf_multi_create: upload");
+    }
+    mp->seg0 = host[0];
+    mp->M.segs = static_cast<const l2g::Segment *>(mp->segs.p);
+    mp->M.job_seg = job_seg;
+    mp->M.job_first = job_first;
+    mp->M.job_count = job_count;
+    mp->M.njobs = njobs;
+    mp->M.job_counter = static_cast<int *>(mp->counter.p);
+    *out = mp;
+    return 0;
+}
+
+int pf_multi_launch(pf_multi *mp, void *stream) {
+    if (!mp) return fail(-1, "pf_multi_launch: null argument");
+    if (mp->M.njobs <= 0) return 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(mp->counter.p, 0, sizeof(int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_multi_launch: counter reset");
+    l2g::BatchArgs a0 = mp->seg0.A;
+    a0.phase_cycles = nullptr;
+    a0.trace = nullptr;
+    e = l2g::launch_nr_batch(mp->seg0.P, a0, mp->precision, mp->threads, mp->grid, mp->smem, st, mp->M);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_multi_launch: kernel");
+    return 0;
+}
+
+int pf_multi_info(const pf_multi *mp, int *threads, int *grid, long long *shared_bytes, long long *scratch_bytes) {
+    if (!mp) return fail(-1, "pf_multi_info: null argument");
+    if (threads) *threads = mp->threads;
+    if (grid) *grid = mp->grid;
+    if (shared_bytes) *shared_bytes = (long long)mp->smem;
+    if (scratch_bytes) *scratch_bytes = (long long)(mp->slab * (size_t)mp->grid);
+    return 0;
+}
+
+void pf_multi_destroy(pf_multi *mp) {
+    if (!mp) return;
+    for (DevBuf *b : {&mp->scratch, &mp->counter, &mp->segs}) b->release();
+    delete mp;
 }
 
 }  // extern "C"

@@ -372,206 +372,277 @@ __device__ void newton_residual(const DevPlan &P, Shared &S, const double2 *__re
     }
 }
 
+// Where one plan's data lives for a CTA: shared memory x | LU (LU_SMEM: one index space, LU at
+// element lu_offset) | phase tables, and the CTA's slab of the scratch memory.
+template <typename LT, typename XT>
+struct Layout {
+    XT *x;
+    LT *lu;
+    double2 *V, *Ibus, *Fbus;
+    double *Vm, *Va, *dxg;
+    int *sb_fac, *sb_bwd, *sb_fwd, *sw_fac, *sw_bwd, *sw_fwd;
+};
+
+template <typename LT, typename XT, bool LU_SMEM>
+__device__ __forceinline__ Layout<LT, XT> make_layout(const DevPlan &P, const BatchArgs &A, unsigned char *dyn) {
+    Layout<LT, XT> L;
+    const int n = P.n, m = P.m;
+    const size_t xbytes = LU_SMEM ? (size_t)P.lu_offset * sizeof(XT) : (((size_t)m * sizeof(XT) + 15) & ~(size_t)15);
+    L.x = reinterpret_cast<XT *>(dyn);
+    unsigned char *slab = A.scratch + (size_t)blockIdx.x * (size_t)A.slab_bytes;
+    L.V = reinterpret_cast<double2 *>(slab);
+    L.Ibus = L.V + n;
+    L.Fbus = L.Ibus + n;
+    L.Vm = reinterpret_cast<double *>(L.Fbus + n);
+    L.Va = L.Vm + n;
+    L.dxg = L.Va + n;
+    const size_t bus_bytes = (((size_t)n * 64 + (size_t)m * 8) + 255) & ~(size_t)255;
+    L.lu = LU_SMEM ? reinterpret_cast<LT *>(dyn + xbytes) : reinterpret_cast<LT *>(slab + bus_bytes);
+    L.sb_fac = reinterpret_cast<int *>(dyn + xbytes +
+                                       (LU_SMEM ? (((size_t)P.nnzLU * sizeof(LT) + 15) & ~(size_t)15) : 0));
+    L.sb_bwd = L.sb_fac + P.fac_nph + 1;
+    L.sb_fwd = L.sb_bwd + P.bwd_nph + 1;
+    L.sw_fac = L.sb_fwd + P.fwd_nph + 1;
+    L.sw_bwd = L.sw_fac + P.fac_nph;
+    L.sw_fwd = L.sw_bwd + P.bwd_nph;
+    return L;
+}
+
+// Phase bounds and widths of the three programs into shared memory (caller synchronises).
+template <typename LT, typename XT>
+__device__ __forceinline__ void stage_tables(const DevPlan &P, const Layout<LT, XT> &L) {
+    for (int i = threadIdx.x; i <= P.fac_nph; i += blockDim.x) L.sb_fac[i] = P.fac_base[i];
+    for (int i = threadIdx.x; i <= P.bwd_nph; i += blockDim.x) L.sb_bwd[i] = P.bwd_base[i];
+    for (int i = threadIdx.x; i <= P.fwd_nph; i += blockDim.x) L.sb_fwd[i] = P.fwd_base[i];
+    for (int i = threadIdx.x; i < P.fac_nph; i += blockDim.x) L.sw_fac[i] = P.fac_width[i];
+    for (int i = threadIdx.x; i < P.bwd_nph; i += blockDim.x) L.sw_bwd[i] = P.bwd_width[i];
+    for (int i = threadIdx.x; i < P.fwd_nph; i += blockDim.x) L.sw_fwd[i] = P.fwd_width[i];
+}
+
+// Per-phase SM cycles, measured by thread 0 between the barriers that end each phase.
+struct Prof {
+    bool on;
+    int traced;
+    unsigned long long tmark;
+    unsigned long long pc[kPhaseSlots];
+    __device__ __forceinline__ void start(bool o) {
+        on = o;
+        traced = 0;
+        tmark = o ? clock64() : 0;
+        for (int i = 0; i < kPhaseSlots; ++i) pc[i] = 0;
+    }
+    __device__ __forceinline__ void mark(int slot) {
+        if (on) {
+            const unsigned long long t = clock64();
+            pc[slot] += t - tmark;
+            tmark = t;
+        }
+    }
+};
+
+// One job: instances [first, first + count) of a batch, chained for a time series.
 template <typename LT, typename XT, bool LU_SMEM, bool REFINE>
-__global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P, const BatchArgs A) {
-    extern __shared__ __align__(16) unsigned char dyn[];
-    __shared__ Shared S;
+__device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, Shared &S, const Layout<LT, XT> &L,
+                                          int first, int count, Prof &pr) {
     const int tid = threadIdx.x;
     const int n = P.n, m = P.m;
-    // shared layout: x | LU (LU_SMEM: one index space, LU at element lu_offset) | phase tables
-    const size_t xbytes = LU_SMEM ? (size_t)P.lu_offset * sizeof(XT) : (((size_t)m * sizeof(XT) + 15) & ~(size_t)15);
-    XT *x = reinterpret_cast<XT *>(dyn);
-    unsigned char *slab = A.scratch + (size_t)blockIdx.x * (size_t)A.slab_bytes;
-    double2 *V = reinterpret_cast<double2 *>(slab);
-    double2 *Ibus = V + n;
-    double2 *Fbus = Ibus + n;
-    double *Vm = reinterpret_cast<double *>(Fbus + n);
-    double *Va = Vm + n;
-    double *dxg = Va + n;
-    const size_t bus_bytes = (((size_t)n * 64 + (size_t)m * 8) + 255) & ~(size_t)255;
-    LT *lu = LU_SMEM ? reinterpret_cast<LT *>(dyn + xbytes) : reinterpret_cast<LT *>(slab + bus_bytes);
-    // phase bounds of the three programs, staged once per launch
-    int *sb_fac = reinterpret_cast<int *>(dyn + xbytes + (LU_SMEM ? (((size_t)P.nnzLU * sizeof(LT) + 15) & ~(size_t)15) : 0));
-    int *sb_bwd = sb_fac + P.fac_nph + 1;
-    int *sb_fwd = sb_bwd + P.bwd_nph + 1;
-    int *sw_fac = sb_fwd + P.fwd_nph + 1;
-    int *sw_bwd = sw_fac + P.fac_nph;
-    int *sw_fwd = sw_bwd + P.bwd_nph;
-    for (int i = tid; i <= P.fac_nph; i += blockDim.x) sb_fac[i] = P.fac_base[i];
-    for (int i = tid; i <= P.bwd_nph; i += blockDim.x) sb_bwd[i] = P.bwd_base[i];
-    for (int i = tid; i <= P.fwd_nph; i += blockDim.x) sb_fwd[i] = P.fwd_base[i];
-    for (int i = tid; i < P.fac_nph; i += blockDim.x) sw_fac[i] = P.fac_width[i];
-    for (int i = tid; i < P.bwd_nph; i += blockDim.x) sw_bwd[i] = P.bwd_width[i];
-    for (int i = tid; i < P.fwd_nph; i += blockDim.x) sw_fwd[i] = P.fwd_width[i];
-    __syncthreads();
-    // per-phase SM cycles, measured by thread 0 between the barriers that end each phase
-    unsigned long long pc[kPhaseSlots] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const bool prof = A.phase_cycles != nullptr && tid == 0;
-    int traced = 0;
-    unsigned long long tmark = prof ? clock64() : 0;
-#define L2G_MARK(slot)                                  \
-    if (prof) {                                          \
-        const unsigned long long t_ = clock64();        \
-        pc[slot] += t_ - tmark;                         \
-        tmark = t_;                                     \
+    XT *x = L.x;
+    LT *lu = L.lu;
+    double2 *V = L.V, *Ibus = L.Ibus, *Fbus = L.Fbus;
+    double *Vm = L.Vm, *Va = L.Va, *dxg = L.dxg;
+    for (int step = 0; step < count; ++step) {
+        const int inst = first + step;
+        const double2 *Sb = A.Sbus + (long long)inst * A.sbus_stride;
+        if (step == 0 || !A.chain) {
+            const double2 *v0 = A.V0 + (long long)inst * A.v0_stride;
+            for (int b = tid; b < n; b += blockDim.x) {
+                const double2 v = v0[b];
+                V[b] = v;
+                Vm[b] = cabs2(v);
+                Va[b] = atan2(v.y, v.x);
+            }
+        } else {
+            for (int b = tid; b < n; b += blockDim.x) {
+                const double2 v = V[b];
+                Vm[b] = cabs2(v);
+                Va[b] = atan2(v.y, v.x);
+            }
+        }
+        if (tid == 0) {
+            int k0 = 0, k1 = 0;
+            if (A.ovr_ptr) {
+                k0 = A.ovr_ptr[inst];
+                k1 = A.ovr_ptr[inst + 1];
+            }
+            S.novr = min(k1 - k0, kMaxOverrides);
+            S.piv_err = 0;
+            S.slack_absorbed = 0.0;
+        }
+        __syncthreads();
+        if (tid < S.novr) {
+            const int k0 = A.ovr_ptr[inst];
+            S.opos[tid] = A.ovr_pos[k0 + tid];
+            S.oval[tid] = A.ovr_val[k0 + tid];
+        }
+        if (P.distributed) {
+            double ls = 0.0;
+            for (int b = tid; b < n; b += blockDim.x) ls += Sb[b].x;
+            const double tot = block_sum(S, ls);
+            if (tid == 0) S.slack_absorbed = tot;
+        }
+        __syncthreads();
+        double norm;
+        int bad;
+        pr.mark(6);
+        mismatch<XT>(P, S, V, Ibus, Fbus, Sb, x, norm, bad);
+        pr.mark(0);
+        bool conv = !bad && norm < A.tol;
+        int it = 0, err = 0;
+        double *Jout = (A.Jout && inst == A.j_inst) ? A.Jout : nullptr;
+        Trace tr{(A.trace != nullptr && blockIdx.x == 0 && pr.traced == 0) ? A.trace : nullptr, A.trace_cap, 0};
+        pr.traced = 1;
+        while (!conv && it < A.max_iter) {
+            ++it;
+            jacobian_fill<LT>(P, S, V, Ibus, lu, Jout);
+            __syncthreads();
+            pr.mark(1);
+            // refactorisation with the forward substitution of the right-hand side fused in
+            const bool refine_now = REFINE && norm < A.refine_below;
+            tr.mark();
+            run_lu_program<LT, XT, LU_SMEM>(P.fac_cops, P.fac_ops, L.sb_fac, L.sw_fac, P.fac_nph, m, lu, x, tr);
+            check_pivots<LT>(P, S, lu);
+            pr.mark(2);
+            if (S.piv_err) {
+                err = 6;  // SolverReFactor
+                break;
+            }
+            run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr);
+            scale_by_pivots<LT, XT>(P, lu, x);
+            pr.mark(4);
+            if (refine_now) {
+                for (int k = tid; k < m; k += blockDim.x) dxg[k] = (double)x[k];
+                __syncthreads();
+                newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, x);
+                __syncthreads();
+                run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr);
+                run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr);
+                scale_by_pivots<LT, XT>(P, lu, x);
+                pr.mark(5);
+            }
+            // voltage update
+            double lmin = 1.0;
+            for (int b = tid; b < n; b += blockDim.x) {
+                double vm, va;
+                if (P.distributed) {
+                    vm = Vm[b];
+                    va = Va[b];
+                } else {
+                    const double2 v = V[b];
+                    vm = cabs2(v);
+                    va = atan2(v.y, v.x);
+                }
+                const int ia = P.xVa[b], im = P.xVm[b];
+                if (ia >= 0) va -= refine_now ? dxg[ia] + (double)x[ia] : (double)x[ia];
+                if (im >= 0) vm -= refine_now ? dxg[im] + (double)x[im] : (double)x[im];
+                double sn, cs;
+                sincos(va, &sn, &cs);
+                V[b] = make_double2(vm * cs, vm * sn);
+                Vm[b] = vm;
+                Va[b] = va;
+                lmin = fmin(lmin, vm);
+            }
+            if (P.distributed) {
+                const double dxs =
+                    refine_now ? dxg[P.xSlack] + (double)x[P.xSlack] : (double)x[P.xSlack];
+                const double vmin = block_min(S, lmin);  // contains barriers
+                if (tid == 0) S.slack_absorbed -= dxs;
+                if (vmin < 0.0) {
+                    for (int b = tid; b < n; b += blockDim.x) {
+                        const double2 v = V[b];
+                        Vm[b] = cabs2(v);
+                        Va[b] = atan2(v.y, v.x);
+                    }
+                }
+            }
+            __syncthreads();
+            tr.mark();
+            tr.buf = nullptr;
+            pr.mark(6);
+            mismatch<XT>(P, S, V, Ibus, Fbus, Sb, x, norm, bad);
+            pr.mark(0);
+            if (bad) {
+                err = 3;  // InifiniteValue
+                break;
+            }
+            conv = norm < A.tol;
+        }
+        if (!conv && err == 0) err = 2;  // TooManyIterations
+        double2 *vo = A.Vout + (long long)inst * n;
+        for (int b = tid; b < n; b += blockDim.x) vo[b] = V[b];
+        if (tid == 0) {
+            A.iters[inst] = it;
+            A.errs[inst] = err;
+            pr.pc[7] += 1;
+        }
+        __syncthreads();
+        if (A.chain && err != 0) {
+            // the reference stops a time series at its first divergence
+            for (int s2 = step + 1 + tid; s2 < count; s2 += blockDim.x) {
+                A.iters[first + s2] = 0;
+                A.errs[first + s2] = 8;  // NotInitError: not computed
+            }
+            break;
+        }
     }
+}
 
+template <typename LT, typename XT, bool LU_SMEM, bool REFINE>
+__global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, const BatchArgs A0, const MultiArgs M) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ Shared S;
+    // the plan and batch of the current job, in shared memory: a launch of one plan (M.segs
+    // null) copies its parameters once; a launch over several plans copies the segment of a
+    // job when it differs from the CTA's previous one and restages the phase tables.  Both
+    // kinds run the same code, so an instance gives the same bits in either.
+    __shared__ __align__(16) Segment seg;
+    const int tid = threadIdx.x;
+    const bool multi = M.segs != nullptr;
+    int *const counter = multi ? M.job_counter : A0.job_counter;
+    const int njobs = multi ? M.njobs : A0.njobs;
+    Prof pr;
+    pr.start(A0.phase_cycles != nullptr && tid == 0);
+    int cur = -1;
+    Layout<LT, XT> L{};
     for (;;) {
-        if (tid == 0) S.job = atomicAdd(A.job_counter, 1);
+        if (tid == 0) S.job = atomicAdd(counter, 1);
         __syncthreads();
         const int job = S.job;
         __syncthreads();
-        if (job >= A.njobs) break;
-        const int first = A.job_first[job], count = A.job_count[job];
-        for (int step = 0; step < count; ++step) {
-            const int inst = first + step;
-            const double2 *Sb = A.Sbus + (long long)inst * A.sbus_stride;
-            if (step == 0 || !A.chain) {
-                const double2 *v0 = A.V0 + (long long)inst * A.v0_stride;
-                for (int b = tid; b < n; b += blockDim.x) {
-                    const double2 v = v0[b];
-                    V[b] = v;
-                    Vm[b] = cabs2(v);
-                    Va[b] = atan2(v.y, v.x);
-                }
-            } else {
-                for (int b = tid; b < n; b += blockDim.x) {
-                    const double2 v = V[b];
-                    Vm[b] = cabs2(v);
-                    Va[b] = atan2(v.y, v.x);
-                }
-            }
-            if (tid == 0) {
-                int k0 = 0, k1 = 0;
-                if (A.ovr_ptr) {
-                    k0 = A.ovr_ptr[inst];
-                    k1 = A.ovr_ptr[inst + 1];
-                }
-                S.novr = min(k1 - k0, kMaxOverrides);
-                S.piv_err = 0;
-                S.slack_absorbed = 0.0;
+        if (job >= njobs) break;
+        const int sj = multi ? M.job_seg[job] : 0;
+        if (sj != cur) {
+            if (multi) {
+                static_assert(sizeof(Segment) % sizeof(int4) == 0, "segment records are copied as int4");
+                const int4 *src = reinterpret_cast<const int4 *>(M.segs + sj);
+                int4 *dst = reinterpret_cast<int4 *>(&seg);
+                for (int i = tid; i < (int)(sizeof(Segment) / sizeof(int4)); i += blockDim.x) dst[i] = src[i];
+            } else if (tid == 0) {
+                seg.P = P0;
+                seg.A = A0;
             }
             __syncthreads();
-            if (tid < S.novr) {
-                const int k0 = A.ovr_ptr[inst];
-                S.opos[tid] = A.ovr_pos[k0 + tid];
-                S.oval[tid] = A.ovr_val[k0 + tid];
-            }
-            if (P.distributed) {
-                double ls = 0.0;
-                for (int b = tid; b < n; b += blockDim.x) ls += Sb[b].x;
-                const double tot = block_sum(S, ls);
-                if (tid == 0) S.slack_absorbed = tot;
-            }
+            cur = sj;
+            L = make_layout<LT, XT, LU_SMEM>(seg.P, seg.A, dyn);
+            stage_tables<LT, XT>(seg.P, L);
             __syncthreads();
-            double norm;
-            int bad;
-            L2G_MARK(6);
-            mismatch<XT>(P, S, V, Ibus, Fbus, Sb, x, norm, bad);
-            L2G_MARK(0);
-            bool conv = !bad && norm < A.tol;
-            int it = 0, err = 0;
-            double *Jout = (A.Jout && inst == A.j_inst) ? A.Jout : nullptr;
-            Trace tr{(A.trace != nullptr && blockIdx.x == 0 && traced == 0) ? A.trace : nullptr, A.trace_cap, 0};
-            traced = 1;
-            while (!conv && it < A.max_iter) {
-                ++it;
-                jacobian_fill<LT>(P, S, V, Ibus, lu, Jout);
-                __syncthreads();
-                L2G_MARK(1);
-                // refactorisation with the forward substitution of the right-hand side fused in
-                const bool refine_now = REFINE && norm < A.refine_below;
-                tr.mark();
-                run_lu_program<LT, XT, LU_SMEM>(P.fac_cops, P.fac_ops, sb_fac, sw_fac, P.fac_nph, m, lu, x, tr);
-                check_pivots<LT>(P, S, lu);
-                L2G_MARK(2);
-                if (S.piv_err) {
-                    err = 6;  // SolverReFactor
-                    break;
-                }
-                run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, sb_bwd, sw_bwd, P.bwd_nph, m, lu, x, tr);
-                scale_by_pivots<LT, XT>(P, lu, x);
-                L2G_MARK(4);
-                if (refine_now) {
-                    for (int k = tid; k < m; k += blockDim.x) dxg[k] = (double)x[k];
-                    __syncthreads();
-                    newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, x);
-                    __syncthreads();
-                    run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, sb_fwd, sw_fwd, P.fwd_nph, m, lu, x, tr);
-                    run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, sb_bwd, sw_bwd, P.bwd_nph, m, lu, x, tr);
-                    scale_by_pivots<LT, XT>(P, lu, x);
-                    L2G_MARK(5);
-                }
-                // voltage update
-                double lmin = 1.0;
-                for (int b = tid; b < n; b += blockDim.x) {
-                    double vm, va;
-                    if (P.distributed) {
-                        vm = Vm[b];
-                        va = Va[b];
-                    } else {
-                        const double2 v = V[b];
-                        vm = cabs2(v);
-                        va = atan2(v.y, v.x);
-                    }
-                    const int ia = P.xVa[b], im = P.xVm[b];
-                    if (ia >= 0) va -= refine_now ? dxg[ia] + (double)x[ia] : (double)x[ia];
-                    if (im >= 0) vm -= refine_now ? dxg[im] + (double)x[im] : (double)x[im];
-                    double sn, cs;
-                    sincos(va, &sn, &cs);
-                    V[b] = make_double2(vm * cs, vm * sn);
-                    Vm[b] = vm;
-                    Va[b] = va;
-                    lmin = fmin(lmin, vm);
-                }
-                if (P.distributed) {
-                    const double dxs =
-                        refine_now ? dxg[P.xSlack] + (double)x[P.xSlack] : (double)x[P.xSlack];
-                    const double vmin = block_min(S, lmin);  // contains barriers
-                    if (tid == 0) S.slack_absorbed -= dxs;
-                    if (vmin < 0.0) {
-                        for (int b = tid; b < n; b += blockDim.x) {
-                            const double2 v = V[b];
-                            Vm[b] = cabs2(v);
-                            Va[b] = atan2(v.y, v.x);
-                        }
-                    }
-                }
-                __syncthreads();
-                tr.mark();
-                tr.buf = nullptr;
-                L2G_MARK(6);
-                mismatch<XT>(P, S, V, Ibus, Fbus, Sb, x, norm, bad);
-                L2G_MARK(0);
-                if (bad) {
-                    err = 3;  // InifiniteValue
-                    break;
-                }
-                conv = norm < A.tol;
-            }
-            if (!conv && err == 0) err = 2;  // TooManyIterations
-            double2 *vo = A.Vout + (long long)inst * n;
-            for (int b = tid; b < n; b += blockDim.x) vo[b] = V[b];
-            if (tid == 0) {
-                A.iters[inst] = it;
-                A.errs[inst] = err;
-                pc[7] += 1;
-            }
-            __syncthreads();
-            if (A.chain && err != 0) {
-                // the reference stops a time series at its first divergence
-                for (int s2 = step + 1 + tid; s2 < count; s2 += blockDim.x) {
-                    A.iters[first + s2] = 0;
-                    A.errs[first + s2] = 8;  // NotInitError: not computed
-                }
-                break;
-            }
         }
+        const int first = multi ? M.job_first[job] : A0.job_first[job];
+        const int count = multi ? M.job_count[job] : A0.job_count[job];
+        solve_job<LT, XT, LU_SMEM, REFINE>(seg.P, seg.A, S, L, first, count, pr);
         __syncthreads();
     }
-    if (prof)
-        for (int i = 0; i < kPhaseSlots; ++i) A.phase_cycles[(size_t)blockIdx.x * kPhaseSlots + i] = pc[i];
-#undef L2G_MARK
+    if (pr.on)
+        for (int i = 0; i < kPhaseSlots; ++i) A0.phase_cycles[(size_t)blockIdx.x * kPhaseSlots + i] = pr.pc[i];
 }
 
 // Raises a kernel's dynamic shared-memory limit to everything the device allows, once per
@@ -598,11 +669,11 @@ cudaError_t allow_max_smem(const void *fn) {
 }
 
 template <typename LT, typename XT, bool SM, bool RF>
-cudaError_t launch_variant(const DevPlan &P, const BatchArgs &A, int threads, int grid, size_t smem,
-                           cudaStream_t st) {
+cudaError_t launch_variant(const DevPlan &P, const BatchArgs &A, const MultiArgs &M, int threads, int grid,
+                           size_t smem, cudaStream_t st) {
     cudaError_t e = allow_max_smem(reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF>));
     if (e != cudaSuccess) return e;
-    nr_batch_kernel<LT, XT, SM, RF><<<grid, threads, smem, st>>>(P, A);
+    nr_batch_kernel<LT, XT, SM, RF><<<grid, threads, smem, st>>>(P, A, M);
     return cudaGetLastError();
 }
 
@@ -652,17 +723,17 @@ size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem) 
 }
 
 cudaError_t launch_nr_batch(const DevPlan &P, const BatchArgs &A, int precision, int threads, int grid,
-                            size_t smem, cudaStream_t stream) {
+                            size_t smem, cudaStream_t stream, const MultiArgs &M) {
     const bool sm = A.lu_in_smem != 0;
     if (precision == 0) {
-        return sm ? launch_variant<double, double, true, false>(P, A, threads, grid, smem, stream)
-                  : launch_variant<double, double, false, false>(P, A, threads, grid, smem, stream);
+        return sm ? launch_variant<double, double, true, false>(P, A, M, threads, grid, smem, stream)
+                  : launch_variant<double, double, false, false>(P, A, M, threads, grid, smem, stream);
     }
     if (A.refine)
-        return sm ? launch_variant<float, float, true, true>(P, A, threads, grid, smem, stream)
-                  : launch_variant<float, float, false, true>(P, A, threads, grid, smem, stream);
-    return sm ? launch_variant<float, float, true, false>(P, A, threads, grid, smem, stream)
-              : launch_variant<float, float, false, false>(P, A, threads, grid, smem, stream);
+        return sm ? launch_variant<float, float, true, true>(P, A, M, threads, grid, smem, stream)
+                  : launch_variant<float, float, false, true>(P, A, M, threads, grid, smem, stream);
+    return sm ? launch_variant<float, float, true, false>(P, A, M, threads, grid, smem, stream)
+              : launch_variant<float, float, false, false>(P, A, M, threads, grid, smem, stream);
 }
 
 int nr_occupancy(int precision, bool lu_in_smem, bool refine, int threads, size_t smem) {

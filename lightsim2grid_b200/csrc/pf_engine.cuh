@@ -69,6 +69,23 @@ struct BatchArgs {
     int trace_cap;
 };
 
+// One segment of a launch over several plans: a plan and its batch (device memory).
+struct alignas(16) Segment {
+    DevPlan P;
+    BatchArgs A;
+};
+
+// Launch over several plans (segments): job j runs instances [job_first[j], job_first[j] +
+// job_count[j]) of segment job_seg[j].  segs == nullptr: a launch of one plan.
+struct MultiArgs {
+    const Segment *segs;
+    const int *job_seg;
+    const int *job_first;
+    const int *job_count;
+    int njobs;
+    int *job_counter;
+};
+
 // phase_cycles slots: mismatch, J fill, refactorisation, forward, backward, refinement,
 // update, instances
 constexpr int kPhaseSlots = 8;
@@ -82,7 +99,7 @@ size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem);
 // precision: 0 = FP64 LU and solves, 1 = FP32 LU and solves (FP64 mismatch and update).
 // A.lu_in_smem and A.refine select the kernel variant.
 cudaError_t launch_nr_batch(const DevPlan &P, const BatchArgs &A, int precision, int threads, int grid,
-                            size_t smem, cudaStream_t stream);
+                            size_t smem, cudaStream_t stream, const MultiArgs &M = MultiArgs{});
 // Copies the converged result rows of a compacted batch into case order (zero rows for
 // cases with map[c] < 0 or errs[map[c]] != 0).
 cudaError_t launch_scatter_case_rows(const double2 *src, const int *errs, const int *map, int ncases, int n,

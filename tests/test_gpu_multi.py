@@ -1,0 +1,80 @@
+"""Uneven-size batched N-1 in one graph-captured launch over three grids: per-instance
+convergence flags equal the oracle's (the reference's ContingencyAnalysis semantics,
+ContingencyAnalysis.cpp:166-233, islanded outages skipped), voltages within 1e-8 pu of the
+oracle, and bit-for-bit the results of one launch per grid."""
+import numpy as np
+import pytest
+
+from oracle.oracle import contingency_analysis
+
+pytestmark = pytest.mark.gpu
+
+TOL_ORACLE = 1e-8
+
+
+@pytest.fixture(scope="module")
+def uneven():
+    import torch
+
+    from lightsim2grid_b200 import synthetic
+    from lightsim2grid_b200.multi import build_uneven, draw_outages
+
+    dev = torch.device("cuda:0")
+    parts = [(nm, synthetic.make_named_grid(nm)[0], k) for nm, k in (("grid118", 50), ("grid1354", 100),
+                                                                        ("grid2848", 250))]
+    mb, cases = build_uneven(draw_outages(parts, seed=7), dev, precision=1)
+    st = torch.cuda.current_stream()
+    mb.launch(st.cuda_stream)
+    torch.cuda.synchronize()
+    for c in cases:
+        c.dev["er"].fill_(-1)
+    g = mb.capture()
+    g.replay()
+    torch.cuda.synchronize()
+    return mb, cases
+
+
+def test_flags_and_voltages_match_oracle(uneven):
+    mb, cases = uneven
+    for c in cases:
+        V, conv, it, er = c.results()
+        g = c.grid
+        coeffs = [g.branch_coeffs([int(b)]) for b in c.branches]
+        _, Vo, conv_o, _, _ = contingency_analysis(g.get_Ybus(), c.Sbase, c.Vbase, g.get_slack_ids(),
+                                                   g.get_slack_weights(), g.get_pv(), g.get_pq(), coeffs, 10, 1e-8)
+        assert np.array_equal(conv, conv_o.astype(bool)), c.name
+        assert conv.any()
+        assert np.abs(V[conv] - Vo[conv]).max() <= TOL_ORACLE, c.name
+        assert np.all(er[c.solvable] >= 0)  # every solvable instance was run
+
+
+def test_one_launch_equals_one_launch_per_grid(uneven):
+    import torch
+
+    from lightsim2grid_b200 import _native as nat
+
+    mb, cases = uneven
+    dev = torch.device("cuda:0")
+    st = torch.cuda.current_stream()
+    for c in cases:
+        V, conv, it, er = c.results()
+        k = c.ninst
+        jf = torch.arange(k, dtype=torch.int32, device=dev)
+        jc = torch.ones(k, dtype=torch.int32, device=dev)
+        Vs = torch.zeros(k * c.n * 2, dtype=torch.float64, device=dev)
+        its = torch.zeros(k, dtype=torch.int32, device=dev)
+        ers = torch.zeros(k, dtype=torch.int32, device=dev)
+        b = c.batch
+        b2 = nat.PfDeviceBatch(n_inst=k, V0=b.V0, v0_stride=0, Sbus=b.Sbus, sbus_stride=0, ovr_ptr=b.ovr_ptr,
+                               ovr_pos=b.ovr_pos, ovr_val=b.ovr_val, max_iter=b.max_iter, tol=b.tol, chain=0,
+                               job_first=jf.data_ptr(), job_count=jc.data_ptr(), njobs=k, Vout=Vs.data_ptr(),
+                               iters=its.data_ptr(), errs=ers.data_ptr())
+        lib = c.plan._lib
+        assert lib.pf_batch_device(c.plan.handle, nat.ctypes.byref(b2), st.cuda_stream) == 0, nat.last_error(lib)
+        torch.cuda.synchronize()
+        idx = np.flatnonzero(c.solvable)
+        assert np.array_equal(ers.cpu().numpy(), er[idx])
+        assert np.array_equal(its.cpu().numpy(), it[idx])
+        Vone = Vs.cpu().numpy().view(np.complex128).reshape(k, c.n)
+        ok = er[idx] == 0
+        assert np.array_equal(Vone[ok], V[idx][ok])
