@@ -186,7 +186,7 @@ def main(argv=None):
     ap.add_argument("--total", type=int, default=4096)
     ap.add_argument("--repeat", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--threads", type=int, default=512)
+    ap.add_argument("--threads", type=int, default=0, help="0: autotuned on a sample of the mix")
     ap.add_argument("--seed", type=int, default=4096)
     args = ap.parse_args(argv)
     import torch
@@ -198,7 +198,15 @@ def main(argv=None):
     counts = [args.total * w // sum(weights) for w in weights]
     counts[-1] += args.total - sum(counts)
     grids = [(nm, synthetic.make_named_grid(nm)[0], k) for nm, k in zip(names, counts)]
-    mb, cases = build_uneven(draw_outages(grids, args.seed), dev, precision=1, threads=args.threads)
+    tuning = None
+    threads = args.threads
+    if threads <= 0:
+        from .autotune import tune_uneven
+
+        sample = draw_outages([(nm, g, max(8, k // 8)) for nm, g, k in grids], args.seed + 1)
+        best, tuning = tune_uneven(sample, precision=1)
+        threads = best["threads"]
+    mb, cases = build_uneven(draw_outages(grids, args.seed), dev, precision=1, threads=threads)
     st = torch.cuda.current_stream()
     for _ in range(args.warmup):
         mb.launch(st.cuda_stream)
@@ -223,7 +231,7 @@ def main(argv=None):
                        "launch".format(args.total, "/".join(names)),
            "cases": {c.name: len(c.branches) for c in cases}, "solvable": {c.name: c.ninst for c in cases},
            "converged": conv, "ms": [1e3 * t for t in times], "converged_pf_per_s": tot / float(np.mean(times)),
-           "launch": mb.info()}
+           "launch": mb.info(), "autotune": tuning}
     print(json.dumps(out))
     return 0
 

@@ -189,10 +189,11 @@ def ar1_profiles(n_steps, n_series, seed=0, phi=0.9, sigma=0.03, daily=0.15, ste
     return (1.0 + e) * day[:, None]
 
 
-def time_series_injections(grid, n_steps, seed=0):
-    """Gen / load injections for a time series on ``grid`` (AR(1) x daily sinusoid)."""
-    m_gen = ar1_profiles(n_steps, grid.gen_bus.size, seed=seed)
-    m_load = ar1_profiles(n_steps, grid.load_bus.size, seed=seed + 1)
+def time_series_injections(grid, n_steps, seed=0, level=1.0):
+    """Gen / load injections for a time series on ``grid`` (AR(1) x daily sinusoid), around
+    ``level`` times the grid's base injections."""
+    m_gen = ar1_profiles(n_steps, grid.gen_bus.size, seed=seed) * level
+    m_load = ar1_profiles(n_steps, grid.load_bus.size, seed=seed + 1) * level
     gen_p = grid.gen_p_mw[None, :] * m_gen
     load_p = grid.load_p_mw[None, :] * m_load
     load_q = grid.load_q_mvar[None, :] * m_load
