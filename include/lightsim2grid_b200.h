@@ -171,6 +171,38 @@ int pf_multi_info(const pf_multi *multi, int *threads, int *grid, long long *sha
                   long long *scratch_bytes);
 void pf_multi_destroy(pf_multi *multi);
 
+/* Branches for flow computations (BaseBatchSolverSynch::compute_amps_flows /
+   compute_active_power_flows, src/batch_algorithm/BaseBatchSolverSynch.hpp:87-192): bus
+   indices of both sides, the AC admittances y_ff and y_ft (complex, interleaved), the nominal
+   voltage (kV) of the from bus, the in-service flag (NULL: every branch in service), sn_mva. */
+typedef struct pf_branch_set {
+    int nbr;
+    const int *from;
+    const int *to;
+    const double *yff_ri;
+    const double *yft_ri;
+    const double *vn_kv_from;
+    const unsigned char *status;
+    double sn_mva;
+} pf_branch_set;
+
+/* Flows of nrows result rows on the device: amps (kA) and / or active power (MW) at the from
+   side of every branch, nrows x nbr row-major (either output may be NULL).  Row r uses the
+   voltages V + map[r] * v_stride (map NULL: row r; map[r] < 0, or errs[map[r]] != 0 with errs
+   not NULL: all-zero voltages, giving NaN amps and 0 MW as the reference's arithmetic does).
+   out_ptr / out_ids (NULL: none) list each row's removed branches, set to 0 where finite
+   (ContingencyAnalysis::clean_flows, src/batch_algorithm/ContingencyAnalysis.cpp:237-250).
+   Every pointer, including those in `br`, is a device pointer; bus indices must be < n.
+   Asynchronous on `stream`. */
+int pf_flows_device(const pf_branch_set *br, int n, int nrows, const double *V_ri, long long v_stride,
+                    const int *map, const int *errs, const int *out_ptr, const int *out_ids, double *amps,
+                    double *p_mw, void *stream);
+
+/* The same from host arrays (V_ri: nrows x n complex, row-major; outputs nrows x nbr): checks
+   the bus indices, copies to the device, computes, copies back and synchronises. */
+int pf_flows_host(const pf_branch_set *br, int n, int nrows, const double *V_ri, const int *out_ptr,
+                  const int *out_ids, double *amps, double *p_mw);
+
 /* Scratch bytes pf_batch_device_scratch needs to run `ctas` CTAs at once (at most the plan's
    grid); < 0 on error. */
 long long pf_scratch_bytes(const pf_plan *plan, int ctas);

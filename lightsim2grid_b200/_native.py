@@ -45,12 +45,19 @@ class PfDeviceBatch(ctypes.Structure):
                 ("iters", ctypes.c_void_p), ("errs", ctypes.c_void_p)]
 
 
+class PfBranchSet(ctypes.Structure):
+    _fields_ = [("nbr", ctypes.c_int), ("from_", ctypes.c_void_p), ("to", ctypes.c_void_p),
+                ("yff_ri", ctypes.c_void_p), ("yft_ri", ctypes.c_void_p), ("vn_kv_from", ctypes.c_void_p),
+                ("status", ctypes.c_void_p), ("sn_mva", ctypes.c_double)]
+
+
 #: exported symbols, as declared in include/lightsim2grid_b200.h
 SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_get", "pf_set_ybus_values",
            "pf_solve", "pf_get_J", "pf_batch_n1", "pf_n1_prepare", "pf_batch_ts", "pf_batch_device", "pf_timers",
            "pf_host_jacobian_pattern", "pf_host_schedule_solve", "pf_batch_device_phase_cycles",
            "pf_batch_device_phase_trace", "pf_batch_device_noalloc", "pf_batch_device_scratch",
-           "pf_scratch_bytes", "pf_multi_create", "pf_multi_launch", "pf_multi_info", "pf_multi_destroy")
+           "pf_scratch_bytes", "pf_multi_create", "pf_multi_launch", "pf_multi_info", "pf_multi_destroy",
+           "pf_flows_device", "pf_flows_host")
 
 
 def load(path=None):
@@ -111,6 +118,13 @@ def load(path=None):
     lib.pf_multi_info.restype = ctypes.c_int
     lib.pf_multi_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+    lib.pf_flows_device.restype = ctypes.c_int
+    lib.pf_flows_device.argtypes = [ctypes.POINTER(PfBranchSet), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                    ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pf_flows_host.restype = ctypes.c_int
+    lib.pf_flows_host.argtypes = [ctypes.POINTER(PfBranchSet), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     lib.pf_multi_destroy.restype = None
     lib.pf_multi_destroy.argtypes = [ctypes.c_void_p]
     lib.pf_timers.restype = ctypes.c_int

@@ -119,22 +119,14 @@ class _BatchBase:
         Vstart = Vn if (self.init_from_n_powerflow and conv) else V0
         return Y, S, Vstart, conv
 
-    # flows (BaseBatchSolverSynch.hpp:87-192, computed on the host from the voltages)
-    def _branch_flows(self, amps):
-        g = self._grid
-        V = self._voltages
-        y_ff, y_ft, _, _ = g.branch_admittances()
-        f, t = g.line_from, g.line_to
-        Ef, Et = V[:, f], V[:, t]
-        S_ft = Ef * np.conj(y_ff[None, :] * Ef + y_ft[None, :] * Et)
-        if amps:
-            v_kv = np.abs(Ef) * g.bus_vn_kv[f][None, :]
-            with np.errstate(divide="ignore", invalid="ignore"):
-                res = np.abs(S_ft) * g.sn_mva / (np.sqrt(3.0) * v_kv)
-        else:
-            res = S_ft.real * g.sn_mva
-        res[:, ~g.line_status] = 0.0
-        return res
+    # flows (BaseBatchSolverSynch.hpp:87-192): the GPU kernel of lightsim2grid_b200.flows on the
+    # stored voltages (rows of failed or skipped cases are zero: NaN amps, 0 MW, as in the
+    # reference); `removed`: per row, branches zeroed where finite (clean_flows)
+    def _branch_flows(self, amps, removed=None):
+        from .flows import BranchSet, flows_host
+
+        a, p = flows_host(BranchSet(self._grid), self._voltages, removed=removed, amps=amps, power=not amps)
+        return a if amps else p
 
 
 class ContingencyAnalysisCPP(_BatchBase):
@@ -255,27 +247,19 @@ class ContingencyAnalysisCPP(_BatchBase):
         self._timer_total = time.perf_counter() - t0
 
     def compute_flows(self):
-        """Amps per branch; outaged branch 0, failed cases NaN (ContingencyAnalysis.cpp:237-250)."""
+        """Amps per branch and case (ContingencyAnalysis.hpp:110-114): removed branches 0,
+        failed or skipped cases NaN (their voltages are zero), ContingencyAnalysis.cpp:237-250."""
         t0 = time.perf_counter()
-        res = self._branch_flows(True)
-        self._clean(res)
-        self._amps_flows = res
+        self._amps_flows = self._branch_flows(True, removed=[list(c) for c in self._li_defaults])
         self._timer_compute_A = time.perf_counter() - t0
+        return self._amps_flows
 
     def compute_power_flows(self):
+        """Active power (MW) per branch and case (ContingencyAnalysis.hpp:116-120)."""
         t0 = time.perf_counter()
-        res = self._branch_flows(False)
-        self._clean(res)
-        self._active_power_flows = res
+        self._active_power_flows = self._branch_flows(False, removed=[list(c) for c in self._li_defaults])
         self._timer_compute_P = time.perf_counter() - t0
-
-    def _clean(self, res):
-        bad = ~self._conv
-        res[bad, :] = np.nan
-        for c, lst in enumerate(self._li_defaults):
-            for br in lst:
-                if np.isfinite(res[c, br]):
-                    res[c, br] = 0.0
+        return self._active_power_flows
 
     def modif_Ybus_time(self):
         return self._timer_pre_proc
@@ -324,14 +308,17 @@ class TimeSeriesCPP(_BatchBase):
         return self._status
 
     def compute_flows(self):
+        """Amps per branch and snapshot (TimeSeries.hpp:69-72)."""
         t0 = time.perf_counter()
         self._amps_flows = self._branch_flows(True)
         self._timer_compute_A = time.perf_counter() - t0
+        return self._amps_flows
 
     def compute_power_flows(self):
         t0 = time.perf_counter()
         self._active_power_flows = self._branch_flows(False)
         self._timer_compute_P = time.perf_counter() - t0
+        return self._active_power_flows
 
     def close(self):
         self.clear()

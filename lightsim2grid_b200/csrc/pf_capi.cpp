@@ -11,6 +11,7 @@
 
 #include "pf_capi_internal.hpp"
 #include "pf_engine.cuh"
+#include "pf_flows.cuh"
 #include "pf_plan.hpp"
 
 using l2g::cplx;
@@ -1238,6 +1239,112 @@ void pf_multi_destroy(pf_multi *mp) {
     if (!mp) return;
     for (DevBuf *b : {&mp->scratch, &mp->counter, &mp->segs}) b->release();
     delete mp;
+}
+
+
+int pf_flows_device(const pf_branch_set *br, int n, int nrows, const double *V_ri, long long v_stride,
+                    const int *map, const int *errs, const int *out_ptr, const int *out_ids, double *amps,
+                    double *p_mw, void *stream) {
+    if (!br || nrows < 0 || n <= 0 || br->nbr < 0 || (nrows > 0 && br->nbr > 0 && (!V_ri || !br->from || !br->to ||
+                                                                                     !br->yff_ri || !br->yft_ri ||
+                                                                                     !br->vn_kv_from)))
+        return fail(-1, "pf_flows_device: invalid argument");
+    if (out_ptr && !out_ids) return fail(-1, "pf_flows_device: out_ids missing");
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "pf_flows_device: device query");
+    l2g::FlowArgs a{};
+    a.V = reinterpret_cast<const double2 *>(V_ri);
+    a.v_stride = v_stride;
+    a.map = map;
+    a.errs = errs;
+    a.nrows = nrows;
+    a.n = n;
+    a.from = br->from;
+    a.to = br->to;
+    a.yff = reinterpret_cast<const double2 *>(br->yff_ri);
+    a.yft = reinterpret_cast<const double2 *>(br->yft_ri);
+    a.vn_kv_from = br->vn_kv_from;
+    a.status = br->status;
+    a.nbr = br->nbr;
+    a.sn_mva = br->sn_mva;
+    a.out_ptr = out_ptr;
+    a.out_ids = out_ids;
+    a.amps = amps;
+    a.p_mw = p_mw;
+    e = l2g::launch_branch_flows(a, sms, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "pf_flows_device: kernel");
+    return 0;
+}
+
+int pf_flows_host(const pf_branch_set *br, int n, int nrows, const double *V_ri, const int *out_ptr,
+                  const int *out_ids, double *amps, double *p_mw) {
+    if (!br || nrows < 0 || n <= 0 || br->nbr < 0) return fail(-1, "pf_flows_host: invalid argument");
+    const int nb = br->nbr;
+    if (nrows == 0 || nb == 0) return 0;
+    if (!V_ri || !br->from || !br->to || !br->yff_ri || !br->yft_ri || !br->vn_kv_from)
+        return fail(-1, "pf_flows_host: null argument");
+    for (int k = 0; k < nb; ++k)
+        if (br->from[k] < 0 || br->from[k] >= n || br->to[k] < 0 || br->to[k] >= n)
+            return fail(-1, "pf_flows_host: branch bus index out of range");
+    int nout = 0;
+    if (out_ptr) {
+        if (!out_ids) return fail(-1, "pf_flows_host: out_ids missing");
+        if (out_ptr[0] != 0) return fail(-1, "pf_flows_host: out_ptr must start at 0");
+        for (int r = 0; r < nrows; ++r)
+            if (out_ptr[r + 1] < out_ptr[r]) return fail(-1, "pf_flows_host: out_ptr not monotone");
+        nout = out_ptr[nrows];
+    }
+    std::vector<void *> bufs;
+    auto alloc = [&](size_t bytes, void **p) {
+        cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+        if (e == cudaSuccess) bufs.push_back(*p);
+        return e;
+    };
+    auto cleanup = [&]() {
+        for (void *p : bufs) cudaFree(p);
+    };
+    void *dV, *dF, *dT, *dYf, *dYt, *dVn, *dSt = nullptr, *dOp = nullptr, *dOi = nullptr, *dA = nullptr, *dP = nullptr;
+    const size_t vb = (size_t)nrows * n * 16, ob = (size_t)nrows * nb * 8;
+    cudaError_t e;
+    if ((e = alloc(vb, &dV)) != cudaSuccess || (e = alloc(nb * 4, &dF)) != cudaSuccess ||
+        (e = alloc(nb * 4, &dT)) != cudaSuccess || (e = alloc(nb * 16, &dYf)) != cudaSuccess ||
+        (e = alloc(nb * 16, &dYt)) != cudaSuccess || (e = alloc(nb * 8, &dVn)) != cudaSuccess ||
+        (br->status && (e = alloc(nb, &dSt)) != cudaSuccess) ||
+        (out_ptr && ((e = alloc((size_t)(nrows + 1) * 4, &dOp)) != cudaSuccess ||
+                     (e = alloc((size_t)std::max(nout, 1) * 4, &dOi)) != cudaSuccess)) ||
+        (amps && (e = alloc(ob, &dA)) != cudaSuccess) || (p_mw && (e = alloc(ob, &dP)) != cudaSuccess)) {
+        cleanup();
+        return cuda_fail(e, "pf_flows_host: allocation");
+    }
+    auto up = [&](void *d, const void *h, size_t b) { return cudaMemcpy(d, h, b, cudaMemcpyHostToDevice); };
+    if ((e = up(dV, V_ri, vb)) != cudaSuccess || (e = up(dF, br->from, nb * 4)) != cudaSuccess ||
+        (e = up(dT, br->to, nb * 4)) != cudaSuccess || (e = up(dYf, br->yff_ri, nb * 16)) != cudaSuccess ||
+        (e = up(dYt, br->yft_ri, nb * 16)) != cudaSuccess || (e = up(dVn, br->vn_kv_from, nb * 8)) != cudaSuccess ||
+        (dSt && (e = up(dSt, br->status, nb)) != cudaSuccess) ||
+        (dOp && ((e = up(dOp, out_ptr, (size_t)(nrows + 1) * 4)) != cudaSuccess ||
+                 (nout > 0 && (e = up(dOi, out_ids, (size_t)nout * 4)) != cudaSuccess)))) {
+        cleanup();
+        return cuda_fail(e, "pf_flows_host: upload");
+    }
+    pf_branch_set d{nb, static_cast<const int *>(dF), static_cast<const int *>(dT), static_cast<const double *>(dYf),
+                    static_cast<const double *>(dYt), static_cast<const double *>(dVn),
+                    static_cast<const unsigned char *>(dSt), br->sn_mva};
+    int rc = pf_flows_device(&d, n, nrows, static_cast<const double *>(dV), n, nullptr, nullptr,
+                             static_cast<const int *>(dOp), static_cast<const int *>(dOi), static_cast<double *>(dA),
+                             static_cast<double *>(dP), nullptr);
+    if (rc != 0) {
+        cleanup();
+        return rc;
+    }
+    if ((amps && (e = cudaMemcpy(amps, dA, ob, cudaMemcpyDeviceToHost)) != cudaSuccess) ||
+        (p_mw && (e = cudaMemcpy(p_mw, dP, ob, cudaMemcpyDeviceToHost)) != cudaSuccess)) {
+        cleanup();
+        return cuda_fail(e, "pf_flows_host: download");
+    }
+    cleanup();
+    return 0;
 }
 
 }  // extern "C"
