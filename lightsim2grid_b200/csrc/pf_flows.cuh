@@ -2,7 +2,6 @@
 #pragma once
 
 #include <cuda_runtime.h>
-#include <cstddef>
 
 namespace l2g {
 
@@ -26,10 +25,6 @@ struct FlowArgs {
     double *p_mw;            // nrows x nbr, row-major (may be null)
 };
 
-// Rows of up to this many bytes of voltages are staged in shared memory.
-constexpr size_t kFlowsSmemMax = 112 * 1024;
-
-size_t flows_smem_bytes(int n);
 cudaError_t launch_branch_flows(const FlowArgs &A, int num_sms, cudaStream_t st);
 
 }  // namespace l2g
