@@ -33,6 +33,11 @@ typedef struct pf_options {
     int refine;             /* mixed form: refine Newton steps once against the FP64
                                Jacobian.  0: default (on), 1: on, 2: off                       */
     double refine_threshold;/* ... the steps taken from ||F||_inf below this; 0: 1e-3          */
+    double lu_reuse_threshold;/* mixed form: refined steps taken from ||F||_inf below this reuse
+                               the previous iteration's LU instead of refactorising (capped at
+                               the refinement threshold); <= 0: never (default).  Measured at
+                               1e-5: 5-9 % faster, same iterations and flags, but results up
+                               to 5e-8 pu from the FP64 ones instead of 3e-10               */
 } pf_options;
 
 /* Sizes and schedule statistics of a plan. */

@@ -359,6 +359,13 @@ int upload(pf_plan *pl) {
     return 0;
 }
 
+// Mixed form: below which ||F||_inf a refined step reuses the previous iteration's LU
+// (never above the refinement threshold; option <= 0: never).
+double lu_reuse_below(const pf_plan *pl, double refine_below) {
+    const double want = pl->opt.lu_reuse_threshold;
+    return want <= 0 ? 0.0 : std::min(want, refine_below);
+}
+
 int configure(pf_plan *pl) {
     const l2g::Plan &P = pl->P;
     cudaError_t e = cudaGetDevice(&pl->device);
@@ -421,6 +428,7 @@ int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, u
     a.lu_in_smem = pl->lu_in_smem ? 1 : 0;
     a.refine = (precision == 1 && pl->refine) ? 1 : 0;
     a.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
+    a.reuse_below = lu_reuse_below(pl, a.refine_below);
     if (a.njobs <= 0) return 0;
     if (scratch_bytes < pl->slab) return fail(-1, "launch: the scratch memory holds no CTA slab");
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
@@ -1194,6 +1202,7 @@ int pf_multi_create(pf_plan *const *plans, const pf_device_batch *batches, int n
         sg.A.lu_in_smem = mp->lu_in_smem ? 1 : 0;
         sg.A.refine = mp->refine ? 1 : 0;
         sg.A.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
+        sg.A.reuse_below = lu_reuse_below(pl, sg.A.refine_below);
     }
     e = cudaMemcpy(mp->segs.p, host.data(), sizeof(l2g::Segment) * (size_t)nseg, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {

@@ -501,20 +501,31 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
         double *Jout = (A.Jout && inst == A.j_inst) ? A.Jout : nullptr;
         Trace tr{(A.trace != nullptr && blockIdx.x == 0 && pr.traced == 0) ? A.trace : nullptr, A.trace_cap, 0};
         pr.traced = 1;
+        bool have_lu = false;  // this instance's LU from an earlier iteration is in place
         while (!conv && it < A.max_iter) {
             ++it;
-            jacobian_fill<LT>(P, S, V, Ibus, lu, Jout);
-            __syncthreads();
-            pr.mark(1);
-            // refactorisation with the forward substitution of the right-hand side fused in
             const bool refine_now = REFINE && norm < A.refine_below;
+            // close to the solution the Jacobian barely moves between iterations: the step is
+            // solved with the previous iteration's LU and refined against the current FP64
+            // Jacobian (refine_now holds: reuse_below <= refine_below)
+            const bool reuse = REFINE && have_lu && Jout == nullptr && norm < A.reuse_below;
             tr.mark();
-            run_lu_program<LT, XT, LU_SMEM>(P.fac_cops, P.fac_ops, L.sb_fac, L.sw_fac, P.fac_nph, m, lu, x, tr);
-            check_pivots<LT>(P, S, lu);
-            pr.mark(2);
-            if (S.piv_err) {
-                err = 6;  // SolverReFactor
-                break;
+            if (!reuse) {
+                jacobian_fill<LT>(P, S, V, Ibus, lu, Jout);
+                __syncthreads();
+                pr.mark(1);
+                // refactorisation with the forward substitution of the right-hand side fused in
+                run_lu_program<LT, XT, LU_SMEM>(P.fac_cops, P.fac_ops, L.sb_fac, L.sw_fac, P.fac_nph, m, lu, x, tr);
+                check_pivots<LT>(P, S, lu);
+                pr.mark(2);
+                if (S.piv_err) {
+                    err = 6;  // SolverReFactor
+                    break;
+                }
+                have_lu = true;
+            } else {
+                run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr);
+                pr.mark(3);
             }
             run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr);
             scale_by_pivots<LT, XT>(P, lu, x);

@@ -63,6 +63,7 @@ struct BatchArgs {
     int lu_in_smem;
     int refine;               // FP32 LU only: one FP64-residual refinement of every Newton step
     double refine_below;      // ... taken when ||F||_inf before the step is below this
+    double reuse_below;       // refined steps from ||F||_inf below this reuse the previous LU (0: never)
     unsigned long long *phase_cycles;  // optional, kPhaseSlots per CTA: SM cycles per phase
     unsigned long long *trace;         // optional: CTA 0, first Newton iteration of its first
                                        // instance: clock after every phase of every program

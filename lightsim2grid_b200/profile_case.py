@@ -27,6 +27,7 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--refine", type=int, default=0, help="0 default (on), 1 on, 2 off")
     ap.add_argument("--refine-threshold", type=float, default=0.0)
+    ap.add_argument("--lu-reuse", type=float, default=0.0, help="LU reuse threshold (<= 0: never, the default)")
     ap.add_argument("--check", action="store_true", help="compare the voltages with an FP64 plan's")
     args = ap.parse_args()
 
@@ -44,7 +45,7 @@ def main():
     coeffs = [g.branch_coeffs([b]) for b in range(nb)]
     plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, threads=args.threads,
                 lu_placement=args.lu_placement, fuse_forward=args.fuse_forward, max_ctas_per_sm=args.ctas_per_sm,
-                refine=args.refine, refine_threshold=args.refine_threshold)
+                refine=args.refine, refine_threshold=args.refine_threshold, lu_reuse_threshold=args.lu_reuse)
     lib = plan._lib
     cp = np.zeros(nb + 1, np.int32)
     rows, cols, vals = [], [], []
