@@ -208,6 +208,38 @@ int pf_flows_device(const pf_branch_set *br, int n, int nrows, const double *V_r
 int pf_flows_host(const pf_branch_set *br, int n, int nrows, const double *V_ri, const int *out_ptr,
                   const int *out_ids, double *amps, double *p_mw);
 
+/* Ybus assembly on the device (GridModel::fillYbus, src/GridModel.cpp:676-699; branch pi-model
+   src/element_container/TwoSidesContainer_rxh_A.hpp:921-940, triplets pushed per branch as ff,
+   tt, ft, tf at :494-498 and summed in insertion order).  pf_ybus_positions maps (row, col)
+   pairs to the plan's Ybus storage positions (-1: not in the pattern; host only).
+   pf_assemble_ybus_device writes nnz values: entry p sums contributions cids[cptr[p] ..
+   cptr[p+1]), each 4 * branch + kind (0 ff, 1 tt, 2 ft, 3 tf), computed from the branch's r,
+   x, total shunt h (complex, split half / half) and in-service flag (NULL: all in service).
+   pf_set_ybus_values_device copies such values (the plan's storage order) into the plan's
+   device Ybus, asynchronously: later launches on the plan use them.  The plan's host-side
+   values (pf_n1_prepare's islanding check, pf_get_J) keep what pf_plan_create or
+   pf_set_ybus_values gave. */
+int pf_ybus_positions(const pf_plan *plan, int ncoef, const int *rows, const int *cols, int *pos);
+int pf_assemble_ybus_device(int nnz, const int *cptr, const int *cids, const double *r, const double *x,
+                            const double *h_ri, const unsigned char *status, double *ybus_ri, void *stream);
+int pf_set_ybus_values_device(pf_plan *plan, const double *ybus_ri, void *stream);
+
+/* Sbus rows assembled on the device (GridModel::fillSbus_me, src/GridModel.cpp:701-716; per
+   snapshot, TimeSeries::compute_Sbuses, src/batch_algorithm/TimeSeries.hpp:79-151): per bus,
+   generator and static-generator active powers minus load powers (element order), divided by
+   sn_mva when it differs from 1.  Bus -> element lists as CSR (n + 1 pointers each; the static
+   generator lists may be NULL); injections row-major, one row per snapshot.  Device pointers;
+   asynchronous. */
+typedef struct pf_sbus_layout {
+    int n, ngen, nsgen, nload;
+    const int *gen_ptr, *gen_ids;
+    const int *sgen_ptr, *sgen_ids;
+    const int *load_ptr, *load_ids;
+} pf_sbus_layout;
+int pf_assemble_sbus_device(const pf_sbus_layout *lay, int nsteps, const double *gen_p, const double *sgen_p,
+                            const double *load_p, const double *load_q, double sn_mva, double *sbus_ri,
+                            void *stream);
+
 /* Scratch bytes pf_batch_device_scratch needs to run `ctas` CTAs at once (at most the plan's
    grid); < 0 on error. */
 long long pf_scratch_bytes(const pf_plan *plan, int ctas);

@@ -51,13 +51,20 @@ class PfBranchSet(ctypes.Structure):
                 ("status", ctypes.c_void_p), ("sn_mva", ctypes.c_double)]
 
 
+class PfSbusLayout(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("ngen", ctypes.c_int), ("nsgen", ctypes.c_int), ("nload", ctypes.c_int),
+                ("gen_ptr", ctypes.c_void_p), ("gen_ids", ctypes.c_void_p), ("sgen_ptr", ctypes.c_void_p),
+                ("sgen_ids", ctypes.c_void_p), ("load_ptr", ctypes.c_void_p), ("load_ids", ctypes.c_void_p)]
+
+
 #: exported symbols, as declared in include/lightsim2grid_b200.h
 SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_get", "pf_set_ybus_values",
            "pf_solve", "pf_get_J", "pf_batch_n1", "pf_n1_prepare", "pf_batch_ts", "pf_batch_device", "pf_timers",
            "pf_host_jacobian_pattern", "pf_host_schedule_solve", "pf_batch_device_phase_cycles",
            "pf_batch_device_phase_trace", "pf_batch_device_noalloc", "pf_batch_device_scratch",
            "pf_scratch_bytes", "pf_multi_create", "pf_multi_launch", "pf_multi_info", "pf_multi_destroy",
-           "pf_flows_device", "pf_flows_host")
+           "pf_flows_device", "pf_flows_host", "pf_ybus_positions", "pf_assemble_ybus_device",
+           "pf_set_ybus_values_device", "pf_assemble_sbus_device")
 
 
 def load(path=None):
@@ -125,6 +132,17 @@ def load(path=None):
     lib.pf_flows_host.restype = ctypes.c_int
     lib.pf_flows_host.argtypes = [ctypes.POINTER(PfBranchSet), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pf_ybus_positions.restype = ctypes.c_int
+    lib.pf_ybus_positions.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p]
+    lib.pf_assemble_ybus_device.restype = ctypes.c_int
+    lib.pf_assemble_ybus_device.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 8
+    lib.pf_set_ybus_values_device.restype = ctypes.c_int
+    lib.pf_set_ybus_values_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pf_assemble_sbus_device.restype = ctypes.c_int
+    lib.pf_assemble_sbus_device.argtypes = [ctypes.POINTER(PfSbusLayout), ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                            ctypes.c_void_p, ctypes.c_void_p]
     lib.pf_multi_destroy.restype = None
     lib.pf_multi_destroy.argtypes = [ctypes.c_void_p]
     lib.pf_timers.restype = ctypes.c_int

@@ -12,6 +12,7 @@
 #include "pf_capi_internal.hpp"
 #include "pf_engine.cuh"
 #include "pf_flows.cuh"
+#include "pf_assembly.cuh"
 #include "pf_plan.hpp"
 
 using l2g::cplx;
@@ -1354,6 +1355,80 @@ int pf_flows_host(const pf_branch_set *br, int n, int nrows, const double *V_ri,
     }
     cleanup();
     return 0;
+}
+
+
+int pf_ybus_positions(const pf_plan *pl, int ncoef, const int *rows, const int *cols, int *pos) {
+    if (!pl || ncoef < 0 || (ncoef > 0 && (!rows || !cols || !pos))) return fail(-1, "pf_ybus_positions: invalid argument");
+    const l2g::Plan &P = pl->P;
+    for (int i = 0; i < ncoef; ++i) {
+        pos[i] = -1;
+        const int r = rows[i], c = cols[i];
+        if (r < 0 || r >= P.n || c < 0 || c >= P.n) continue;
+        for (int q = P.Rp[r]; q < P.Rp[r + 1]; ++q)
+            if (P.Rj[q] == c) {
+                pos[i] = q;
+                break;
+            }
+    }
+    return 0;
+}
+
+static int device_sms(int *sms) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "device query");
+}
+
+int pf_assemble_ybus_device(int nnz, const int *cptr, const int *cids, const double *r, const double *x,
+                            const double *h_ri, const unsigned char *status, double *ybus_ri, void *stream) {
+    if (nnz < 0 || (nnz > 0 && (!cptr || !cids || !r || !x || !h_ri || !ybus_ri)))
+        return fail(-1, "pf_assemble_ybus_device: invalid argument");
+    int sms = 0;
+    if (device_sms(&sms) != 0) return -1;
+    l2g::YbusArgs a{nnz, cptr, cids, r, x, reinterpret_cast<const double2 *>(h_ri), status,
+                    reinterpret_cast<double2 *>(ybus_ri)};
+    cudaError_t e = l2g::launch_assemble_ybus(a, sms, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? 0 : cuda_fail(e, "pf_assemble_ybus_device: kernel");
+}
+
+int pf_set_ybus_values_device(pf_plan *pl, const double *ybus_ri, void *stream) {
+    if (!pl || !ybus_ri) return fail(-1, "pf_set_ybus_values_device: null argument");
+    cudaError_t e = cudaMemcpyAsync(const_cast<double2 *>(pl->dp.Rx), ybus_ri, (size_t)pl->P.nnzY * 16,
+                                    cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? 0 : cuda_fail(e, "pf_set_ybus_values_device");
+}
+
+int pf_assemble_sbus_device(const pf_sbus_layout *lay, int nsteps, const double *gen_p, const double *sgen_p,
+                            const double *load_p, const double *load_q, double sn_mva, double *sbus_ri,
+                            void *stream) {
+    if (!lay || nsteps < 0 || lay->n <= 0 || !sbus_ri || !lay->gen_ptr || !lay->load_ptr ||
+        (lay->ngen > 0 && (!lay->gen_ids || !gen_p)) || (lay->nload > 0 && (!lay->load_ids || !load_p || !load_q)) ||
+        (lay->sgen_ptr && lay->nsgen > 0 && (!lay->sgen_ids || !sgen_p)))
+        return fail(-1, "pf_assemble_sbus_device: invalid argument");
+    int sms = 0;
+    if (device_sms(&sms) != 0) return -1;
+    l2g::SbusArgs a{};
+    a.nsteps = nsteps;
+    a.n = lay->n;
+    a.ngen = lay->ngen;
+    a.nsgen = lay->nsgen;
+    a.nload = lay->nload;
+    a.gen_ptr = lay->gen_ptr;
+    a.gen_ids = lay->gen_ids;
+    a.sgen_ptr = lay->sgen_ptr;
+    a.sgen_ids = lay->sgen_ids;
+    a.load_ptr = lay->load_ptr;
+    a.load_ids = lay->load_ids;
+    a.gen_p = gen_p;
+    a.sgen_p = sgen_p;
+    a.load_p = load_p;
+    a.load_q = load_q;
+    a.sn_mva = sn_mva;
+    a.out = reinterpret_cast<double2 *>(sbus_ri);
+    cudaError_t e = l2g::launch_assemble_sbus(a, sms, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? 0 : cuda_fail(e, "pf_assemble_sbus_device: kernel");
 }
 
 }  // extern "C"
