@@ -40,6 +40,19 @@ typedef struct pf_options {
                                to 5e-8 pu from the FP64 ones instead of 3e-10               */
 } pf_options;
 
+/* DC power flow plan (BaseDCAlgo::compute_pf, src/powerflow_algorithm/BaseDCAlgo.tpp:5-175;
+   the reference's DC solvers, SolverType DC / KLUDC): ybus_ri is the DC admittance matrix (CSC,
+   complex); the unknowns are the angles of every bus except the first slack (further slacks
+   count as PV), the matrix B = Re(Ybus) without that bus, analysed, ordered, pivoted and
+   scheduled as the Newton plans are, solved in FP64.  pf_solve, pf_batch_n1, pf_batch_device and
+   the scratch entry points run it: one linear solve per instance (iterations 1; max_iter and
+   tol unused); the angles are shifted by the start voltage's slack angle and the magnitudes are
+   the start magnitudes; a non-finite solution or one with |angle| >= 1e6 gives SolverSolve and a
+   zero voltage row.  pf_get_J and pf_multi_create reject DC plans. */
+int pf_dc_plan_create(int n, const int *colptr, const int *rowind, const double *ybus_ri, const int *slack_ids,
+                      int nslack, const int *pv, int npv, const int *pq, int npq, const pf_options *opts,
+                      pf_plan **plan);
+
 /* Sizes and schedule statistics of a plan. */
 typedef struct pf_plan_info {
     int n, m, nnz_ybus, nnz_j, nnz_lu;

@@ -6,7 +6,7 @@ Drop-in for lightsim2grid's Newton-Raphson solver and batch layers: ``SolverType
 ``TimeSeriesCPP``.  The compute path is the native library built from ``csrc/`` (C ABI in
 ``include/lightsim2grid_b200.h``); nothing falls back to the CPU.
 """
-from .solver import (SolverType, ErrorType, GPUNRSolver, GPUNRSolverSingleSlack, GPUNRMixedSolver,
+from .solver import (SolverType, ErrorType, GPUNRSolver, GPUNRSolverSingleSlack, GPUNRMixedSolver, GPUDCSolver,
                      GPUNRMixedSolverSingleSlack, Plan, SOLVER_CLASSES, GPU_SOLVERS)
 from .newtonpf import newtonpf, newtonpf_new, newtonpf_old
 from .gridmodel import GridModel, Coeff

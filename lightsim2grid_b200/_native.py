@@ -64,7 +64,7 @@ SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_g
            "pf_batch_device_phase_trace", "pf_batch_device_noalloc", "pf_batch_device_scratch",
            "pf_scratch_bytes", "pf_multi_create", "pf_multi_launch", "pf_multi_info", "pf_multi_destroy",
            "pf_flows_device", "pf_flows_host", "pf_ybus_positions", "pf_assemble_ybus_device",
-           "pf_set_ybus_values_device", "pf_assemble_sbus_device")
+           "pf_set_ybus_values_device", "pf_assemble_sbus_device", "pf_dc_plan_create")
 
 
 def load(path=None):
@@ -132,6 +132,9 @@ def load(path=None):
     lib.pf_flows_host.restype = ctypes.c_int
     lib.pf_flows_host.argtypes = [ctypes.POINTER(PfBranchSet), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pf_dc_plan_create.restype = ctypes.c_int
+    lib.pf_dc_plan_create.argtypes = [ctypes.c_int, i32p, i32p, f64p, i32p, ctypes.c_int, i32p, ctypes.c_int, i32p,
+                                      ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
     lib.pf_ybus_positions.restype = ctypes.c_int
     lib.pf_ybus_positions.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p]

@@ -357,6 +357,8 @@ int upload(pf_plan *pl) {
     d.fwd_base = I(owb);
     d.fwd_nph = P.forward.nphases();
     d.dpos = I(odpos);
+    d.dc = P.dc ? 1 : 0;
+    d.slack0 = P.slack0;
     return 0;
 }
 
@@ -642,6 +644,29 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 
 }  // namespace l2g
 
+// Shared tail of plan creation: islanding data, stream, device upload, launch configuration.
+int finish_plan(pf_plan *pl, pf_plan **out) {
+    compute_bridges(pl);
+    cudaError_t e = cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete pl;
+        return cuda_fail(e, "pf_plan_create: stream");
+    }
+    cudaEventCreate(&pl->ev0);
+    cudaEventCreate(&pl->ev1);
+    int rc = upload(pl);
+    if (!rc) rc = configure(pl);
+    if (rc) {
+        std::string keep = g_err;
+        release(pl);
+        delete pl;
+        g_err = keep;
+        return rc;
+    }
+    *out = pl;
+    return 0;
+}
+
 extern "C" {
 
 const char *pf_last_error(void) { return g_err.c_str(); }
@@ -681,25 +706,39 @@ int pf_plan_create(int n, const int *colptr, const int *rowind, const double *yb
         delete pl;
         return fail(rc, msg);
     }
-    compute_bridges(pl);
-    cudaError_t e = cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-        delete pl;
-        return cuda_fail(e, "pf_plan_create: stream");
+    return finish_plan(pl, out);
+}
+
+int pf_dc_plan_create(int n, const int *colptr, const int *rowind, const double *ybus_ri, const int *slack_ids,
+                      int nslack, const int *pv, int npv, const int *pq, int npq, const pf_options *opts,
+                      pf_plan **out) {
+    if (!out || !colptr || !rowind || !ybus_ri || !slack_ids || (npv && !pv) || (npq && !pq))
+        return fail(-1, "pf_dc_plan_create: null argument");
+    *out = nullptr;
+    pf_plan *pl = new pf_plan();
+    if (opts) pl->opt = *opts;
+    pl->opt.precision = 0;  // the reference's DC solve is FP64
+    l2g::PlanOptions po;
+    if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
+    int thr = pl->opt.threads;
+    if (thr <= 0) thr = n > 2000 ? 512 : (n > 300 ? 256 : 128);
+    thr = std::max(32, std::min(512, (thr / 32) * 32));
+    po.threads = pl->threads = thr;
+    po.fuse_forward = true;
+    std::string msg;
+    int rc;
+    try {
+        rc = l2g::build_dc_plan(pl->P, n, colptr, rowind, reinterpret_cast<const cplx *>(ybus_ri), slack_ids, nslack,
+                                pv, npv, pq, npq, po, msg);
+    } catch (const std::exception &ex) {
+        rc = -1;
+        msg = std::string("pf_dc_plan_create: ") + ex.what();
     }
-    cudaEventCreate(&pl->ev0);
-    cudaEventCreate(&pl->ev1);
-    rc = upload(pl);
-    if (!rc) rc = configure(pl);
-    if (rc) {
-        std::string keep = g_err;
-        release(pl);
+    if (rc != 0) {
         delete pl;
-        g_err = keep;
-        return rc;
+        return fail(rc, msg);
     }
-    *out = pl;
-    return 0;
+    return finish_plan(pl, out);
 }
 
 void pf_plan_destroy(pf_plan *plan) {
@@ -775,6 +814,7 @@ int pf_solve(pf_plan *pl, const double *V0_ri, const double *Sbus_ri, int max_it
 
 int pf_get_J(pf_plan *pl, int *m, int *Jp, int *Ji, double *Jx) {
     if (!pl) return fail(-1, "pf_get_J: null argument");
+    if (pl->P.dc) return fail(-1, "pf_get_J: a DC plan has no Jacobian");
     const l2g::Plan &P = pl->P;
     if (m) *m = P.m;
     if (Jp) std::memcpy(Jp, P.Jp.data(), P.Jp.size() * sizeof(int));
@@ -1171,6 +1211,10 @@ int pf_multi_create(pf_plan *const *plans, const pf_device_batch *batches, int n
                    pl->lu_in_smem != mp->lu_in_smem) {
             delete mp;
             return fail(-1, "pf_multi_create: plans differ in device, precision, refinement or LU placement");
+        }
+        if (pl->P.dc) {
+            delete mp;
+            return fail(-1, "pf_multi_create: DC plans run one plan per launch");
         }
         mp->plans.push_back(pl);
         mp->threads = std::max(mp->threads, pl->threads);

@@ -679,6 +679,104 @@ cudaError_t allow_max_smem(const void *fn) {
     return cudaSuccess;
 }
 
+// DC power flow of a batch (BaseDCAlgo::compute_pf, src/powerflow_algorithm/BaseDCAlgo.tpp:
+// 86-175), FP64, one CTA per instance: B from the real parts of the instance's Ybus (overrides
+// applied), right-hand side Re(Sbus) at the non-slack buses, refactorisation with the forward
+// substitution fused, backward substitution; the angles are shifted by the slack's start angle,
+// the magnitudes are the start magnitudes.  A non-finite solution or one with |theta| >= 1e6 is
+// SolverSolve (:115-123): zero voltages.  One linear solve: iters = 1.
+template <bool LU_SMEM>
+__global__ void __launch_bounds__(512, 1) dc_batch_kernel(const DevPlan P, const BatchArgs A) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ Shared S;
+    const int tid = threadIdx.x;
+    const int n = P.n, m = P.m;
+    const Layout<double, double> L = make_layout<double, double, LU_SMEM>(P, A, dyn);
+    stage_tables<double, double>(P, L);
+    __syncthreads();
+    double *x = L.x, *lu = L.lu;
+    Trace tr{nullptr, 0, 0};
+    for (;;) {
+        if (tid == 0) S.job = atomicAdd(A.job_counter, 1);
+        __syncthreads();
+        const int job = S.job;
+        __syncthreads();
+        if (job >= A.njobs) break;
+        const int first = A.job_first[job], count = A.job_count[job];
+        for (int inst = first; inst < first + count; ++inst) {
+            if (tid == 0) {
+                int k0 = 0, k1 = 0;
+                if (A.ovr_ptr) {
+                    k0 = A.ovr_ptr[inst];
+                    k1 = A.ovr_ptr[inst + 1];
+                }
+                S.novr = min(k1 - k0, kMaxOverrides);
+                S.piv_err = 0;
+            }
+            __syncthreads();
+            if (tid < S.novr) {
+                const int k0 = A.ovr_ptr[inst];
+                S.opos[tid] = A.ovr_pos[k0 + tid];
+                S.oval[tid] = A.ovr_val[k0 + tid];
+            }
+            __syncthreads();
+            for (int p = tid; p < P.nnzY; p += blockDim.x) {
+                const int t = P.ytarget[p].x;
+                if (t >= 0) lu[t] = ybus_value(P, S, p).x;
+            }
+            for (int i = tid; i < P.nfill; i += blockDim.x) lu[P.fillpos[i]] = 0.0;
+            const double2 *Sb = A.Sbus + (long long)inst * A.sbus_stride;
+            for (int b = tid; b < n; b += blockDim.x) {
+                const int ip = P.xP[b];
+                if (ip >= 0) x[ip] = Sb[b].x;
+            }
+            __syncthreads();
+            run_lu_program<double, double, LU_SMEM>(P.fac_cops, P.fac_ops, L.sb_fac, L.sw_fac, P.fac_nph, m, lu, x,
+                                                    tr);
+            check_pivots<double>(P, S, lu);
+            int err = 0;
+            if (S.piv_err) {
+                err = 6;  // SolverReFactor
+            } else {
+                run_lu_program<double, double, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu,
+                                                        x, tr);
+                scale_by_pivots<double, double>(P, lu, x);
+                double lmax = 0.0;
+                int lbad = 0;
+                for (int k = tid; k < m; k += blockDim.x) {
+                    lmax = fmax(lmax, fabs(x[k]));
+                    lbad |= !isfinite(x[k]);
+                }
+                double nrm;
+                int bad;
+                block_norm(S, lmax, lbad, nrm, bad);
+                if (bad || nrm >= 1e6) err = 7;  // SolverSolve
+            }
+            const double2 *v0 = A.V0 + (long long)inst * A.v0_stride;
+            double2 *vo = A.Vout + (long long)inst * n;
+            const double2 vs = v0[P.slack0];
+            const double a0 = atan2(vs.y, vs.x);
+            for (int b = tid; b < n; b += blockDim.x) {
+                double2 v = make_double2(0.0, 0.0);
+                if (err == 0) {
+                    const int ia = P.xVa[b];
+                    const double va = (ia >= 0 ? x[ia] : 0.0) + a0;
+                    const double vm = cabs2(v0[b]);
+                    double sn, cs;
+                    sincos(va, &sn, &cs);
+                    v = make_double2(vm * cs, vm * sn);
+                }
+                vo[b] = v;
+            }
+            if (tid == 0) {
+                A.iters[inst] = err == 0 ? 1 : 0;
+                A.errs[inst] = err;
+            }
+            __syncthreads();
+        }
+    }
+}
+
 template <typename LT, typename XT, bool SM, bool RF>
 cudaError_t launch_variant(const DevPlan &P, const BatchArgs &A, const MultiArgs &M, int threads, int grid,
                            size_t smem, cudaStream_t st) {
@@ -733,9 +831,23 @@ size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem) 
     return xb + lb + bb;
 }
 
+template <bool SM>
+cudaError_t launch_dc_variant(const DevPlan &P, const BatchArgs &A, int threads, int grid, size_t smem,
+                              cudaStream_t st) {
+    cudaError_t e = allow_max_smem(reinterpret_cast<const void *>(dc_batch_kernel<SM>));
+    if (e != cudaSuccess) return e;
+    dc_batch_kernel<SM><<<grid, threads, smem, st>>>(P, A);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_nr_batch(const DevPlan &P, const BatchArgs &A, int precision, int threads, int grid,
                             size_t smem, cudaStream_t stream, const MultiArgs &M) {
     const bool sm = A.lu_in_smem != 0;
+    if (P.dc) {
+        if (M.segs != nullptr) return cudaErrorInvalidValue;  // DC plans run one plan per launch
+        return sm ? launch_dc_variant<true>(P, A, threads, grid, smem, stream)
+                  : launch_dc_variant<false>(P, A, threads, grid, smem, stream);
+    }
     if (precision == 0) {
         return sm ? launch_variant<double, double, true, false>(P, A, M, threads, grid, smem, stream)
                   : launch_variant<double, double, false, false>(P, A, M, threads, grid, smem, stream);

@@ -34,6 +34,7 @@ struct DevPlan {
     int compact, lu_offset;
     const uint2 *fac_cops, *bwd_cops, *fwd_cops;
     const int *dpos;         // pivot position per column (m)
+    int dc, slack0;          // DC plan (B = Re(Ybus) without the slack) and its slack bus
 };
 
 // One batch launch.

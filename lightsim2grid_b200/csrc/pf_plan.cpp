@@ -212,16 +212,8 @@ void host_jacobian(const Plan &P, const cplx *Yx, const cplx *V, std::vector<dou
     }
 }
 
-int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, const cplx *V0, const cplx *Sbus,
-               const int *slack_ids, int nslack, const double *weights, const int *pv, int npv_in, const int *pq,
-               int npq, bool distributed, const PlanOptions &opt, std::string &msg) {
-    (void)Sbus;
-    P = Plan();
-    std::ostringstream err;
-    if (n <= 0 || nslack <= 0) {
-        msg = "build_plan: the grid needs at least one bus and one slack bus";
-        return NotInitError;
-    }
+// Ybus in canonical CSC form: valid pointers, sorted rows without duplicates.
+int check_ybus(int n, const int *Yp, const int *Yi, std::string &msg) {
     if (Yp[0] != 0 || Yp[n] < n) {
         msg = "build_plan: Ybus column pointer is invalid";
         return NotInitError;
@@ -236,50 +228,12 @@ int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, con
             }
         }
     }
-    std::vector<int> role(n, 0);  // 0 none, 1 slack, 2 pv, 3 pq
-    for (int t = 0; t < nslack; ++t) {
-        if (slack_ids[t] < 0 || slack_ids[t] >= n) { msg = "build_plan: slack id out of range"; return NotInitError; }
-        role[slack_ids[t]] = 1;
-    }
-    for (int t = 0; t < npv_in; ++t) {
-        if (pv[t] < 0 || pv[t] >= n || role[pv[t]] != 0) {
-            msg = "build_plan: a PV bus is out of range, repeated or also a slack";
-            return NotInitError;
-        }
-        role[pv[t]] = 2;
-    }
-    for (int t = 0; t < npq; ++t) {
-        if (pq[t] < 0 || pq[t] >= n || role[pq[t]] != 0) {
-            msg = "build_plan: a PQ bus is out of range, repeated or also PV / slack";
-            return NotInitError;
-        }
-        role[pq[t]] = 3;
-    }
-    P.n = n;
-    P.nnzY = Yp[n];
-    P.Yp.assign(Yp, Yp + n + 1);
-    P.Yi.assign(Yi, Yi + P.nnzY);
-    P.Yx.assign(Yx, Yx + P.nnzY);
-    P.distributed = distributed;
-    P.slack0 = slack_ids[0];
-    P.slack_ids.assign(slack_ids, slack_ids + nslack);
-    P.weights.assign(weights, weights + n);
-    // retrieve_pv_with_slack (src/powerflow_algorithm/BaseAlgo.hpp:201-216)
-    if (distributed)
-        for (int t = 1; t < nslack; ++t) P.mypv.push_back(slack_ids[t]);
-    P.mypv.insert(P.mypv.end(), pv, pv + npv_in);
-    P.pq.assign(pq, pq + npq);
-    P.npv = (int)P.mypv.size();
-    P.npq = npq;
-    P.pvpq = P.mypv;
-    P.pvpq.insert(P.pvpq.end(), pq, pq + npq);
-    P.npvpq = P.npv + npq;
-    P.off = distributed ? 1 : 0;
-    P.m = P.npvpq + npq + P.off;
-    const int m = P.m;
-    if (m == 0) { msg = "build_plan: no PV or PQ bus"; return NotInitError; }
+    return NoError;
+}
 
-    // CSR copy
+// CSR copy of P's Ybus (pattern, values, CSC -> CSR position map).
+void make_csr(Plan &P) {
+    const int n = P.n;
     P.Rp.assign(n + 1, 0);
     for (int p = 0; p < P.nnzY; ++p) P.Rp[P.Yi[p] + 1]++;
     for (int r = 0; r < n; ++r) P.Rp[r + 1] += P.Rp[r];
@@ -287,90 +241,31 @@ int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, con
     P.Rrow.assign(P.nnzY, 0);
     P.csr_of_csc.assign(P.nnzY, 0);
     P.Rx.assign(P.nnzY, 0.0);
-    {
-        std::vector<int> fp(P.Rp.begin(), P.Rp.end() - 1);
-        for (int c = 0; c < n; ++c)
-            for (int p = P.Yp[c]; p < P.Yp[c + 1]; ++p) {
-                int r = P.Yi[p];
-                int d = fp[r]++;
-                P.Rj[d] = c;
-                P.Rrow[d] = r;
-                P.csr_of_csc[p] = d;
-                P.Rx[d] = P.Yx[p];
-            }
-    }
+    std::vector<int> fp(P.Rp.begin(), P.Rp.end() - 1);
+    for (int c = 0; c < n; ++c)
+        for (int p = P.Yp[c]; p < P.Yp[c + 1]; ++p) {
+            int r = P.Yi[p];
+            int d = fp[r]++;
+            P.Rj[d] = c;
+            P.Rrow[d] = r;
+            P.csr_of_csc[p] = d;
+            P.Rx[d] = P.Yx[p];
+        }
+}
 
-    // ---------------------------------------------------------------- Jacobian pattern
-    std::vector<int> pvpq_inv(n, -1), pq_inv(n, -1);
-    for (int t = 0; t < P.npvpq; ++t) pvpq_inv[P.pvpq[t]] = t;
-    for (int t = 0; t < npq; ++t) pq_inv[P.pq[t]] = t;
-    const int off = P.off, npvpq = P.npvpq;
-    struct Trip { int row, col, src; uint8_t kind; double val; };
-    std::vector<Trip> T;
-    T.reserve(4 * (size_t)P.nnzY + n + 4);
-    for (int c = 0; c < npvpq; ++c) {
-        int bus = P.pvpq[c];
-        for (int p = Yp[bus]; p < Yp[bus + 1]; ++p)
-            if (pvpq_inv[Yi[p]] >= 0) T.push_back({pvpq_inv[Yi[p]] + off, c + off, p, 0, 0.0});
-        for (int p = Yp[bus]; p < Yp[bus + 1]; ++p)
-            if (pq_inv[Yi[p]] >= 0) T.push_back({npvpq + pq_inv[Yi[p]] + off, c + off, p, 1, 0.0});
-    }
-    for (int c = 0; c < npq; ++c) {
-        int bus = P.pq[c];
-        for (int p = Yp[bus]; p < Yp[bus + 1]; ++p)
-            if (pvpq_inv[Yi[p]] >= 0) T.push_back({pvpq_inv[Yi[p]] + off, npvpq + c + off, p, 2, 0.0});
-        for (int p = Yp[bus]; p < Yp[bus + 1]; ++p)
-            if (pq_inv[Yi[p]] >= 0) T.push_back({npvpq + pq_inv[Yi[p]] + off, npvpq + c + off, p, 3, 0.0});
-    }
-    if (distributed) {
-        const int s0 = P.slack0;
-        for (int c = 0; c < n; ++c) {
-            if (pvpq_inv[c] < 0) continue;
-            for (int p = Yp[c]; p < Yp[c + 1]; ++p)
-                if (Yi[p] == s0) T.push_back({0, pvpq_inv[c] + 1, p, 0, 0.0});
-        }
-        for (int c = 0; c < n; ++c) {
-            if (pq_inv[c] < 0) continue;
-            for (int p = Yp[c]; p < Yp[c + 1]; ++p)
-                if (Yi[p] == s0) T.push_back({0, npvpq + pq_inv[c] + 1, p, 2, 0.0});
-        }
-        T.push_back({0, 0, -1, 0, weights[s0]});
-        for (int t = 0; t < npvpq; ++t) {
-            double sw = weights[P.pvpq[t]];
-            if (std::fabs(sw) > 1e-7) T.push_back({t + 1, 0, -1, 0, sw});
-        }
-    }
-    std::stable_sort(T.begin(), T.end(), [](const Trip &a, const Trip &b) {
-        return a.col != b.col ? a.col < b.col : a.row < b.row;
-    });
-    const int nnzJ = (int)T.size();
-    P.Jp.assign(m + 1, 0);
-    P.Ji.resize(nnzJ);
-    P.jsrc.resize(nnzJ);
-    P.jkind.resize(nnzJ);
-    P.jconst.assign(nnzJ, 0.0);
-    for (int t = 0; t < nnzJ; ++t) {
-        if (t > 0 && T[t].col == T[t - 1].col && T[t].row == T[t - 1].row) {
-            msg = "build_plan: duplicate Jacobian entry (is a bus both slack and PV/PQ?)";
-            return NotInitError;
-        }
-        P.Jp[T[t].col + 1]++;
-        P.Ji[t] = T[t].row;
-        P.jsrc[t] = T[t].src;
-        P.jkind[t] = T[t].kind;
-        P.jconst[t] = T[t].val;
-    }
-    for (int c = 0; c < m; ++c) P.Jp[c + 1] += P.Jp[c];
-
+// Ordering, first factorisation with threshold partial pivoting, LU layout, phase programs and
+// fill maps for the matrix whose pattern is P.Jp / P.Ji (m = P.m columns), whose entry t takes
+// its values from Ybus position jsrc[t] (part jkind[t]) or the constant jconst[t] (jsrc < 0),
+// and whose values for the first factorisation are Jx.
+int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, std::string &msg) {
+    const int m = P.m;
+    std::ostringstream err;
     // ---------------------------------------------------------------- ordering
     P.q = minimum_degree(m, P.Jp, P.Ji);
     P.qinv.assign(m, 0);
     for (int k = 0; k < m; ++k) P.qinv[P.q[k]] = k;
 
     // ---------------------------------------------------------------- first factorisation
-    std::vector<cplx> Vinit(V0, V0 + n);
-    std::vector<double> Jx;
-    host_jacobian(P, P.Yx.data(), Vinit.data(), Jx);
     P.pinv.assign(m, -1);
     P.prow.assign(m, -1);
     std::vector<std::vector<int>> Lrows(m), Ucols(m);  // Lrows: J rows (later steps), Ucols: steps
@@ -432,7 +327,7 @@ int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, con
                 if (a > amax) { amax = a; piv = r; }
             }
             if (piv < 0 || !(amax > 0.0) || !std::isfinite(amax)) {
-                err << "build_plan: the first Jacobian is singular (step " << k << ")";
+                err << "build_plan: the first matrix is singular (step " << k << ")";
                 msg = err.str();
                 return SolverFactor;
             }
@@ -622,6 +517,136 @@ int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, con
     for (int p = 0; p < P.nnzLU; ++p)
         if (!covered[p]) P.fillpos.push_back(p);
 
+    return NoError;
+}
+
+int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, const cplx *V0, const cplx *Sbus,
+               const int *slack_ids, int nslack, const double *weights, const int *pv, int npv_in, const int *pq,
+               int npq, bool distributed, const PlanOptions &opt, std::string &msg) {
+    (void)Sbus;
+    P = Plan();
+    std::ostringstream err;
+    if (n <= 0 || nslack <= 0) {
+        msg = "build_plan: the grid needs at least one bus and one slack bus";
+        return NotInitError;
+    }
+    if (check_ybus(n, Yp, Yi, msg) != NoError) return NotInitError;
+    std::vector<int> role(n, 0);  // 0 none, 1 slack, 2 pv, 3 pq
+    for (int t = 0; t < nslack; ++t) {
+        if (slack_ids[t] < 0 || slack_ids[t] >= n) { msg = "build_plan: slack id out of range"; return NotInitError; }
+        role[slack_ids[t]] = 1;
+    }
+    for (int t = 0; t < npv_in; ++t) {
+        if (pv[t] < 0 || pv[t] >= n || role[pv[t]] != 0) {
+            msg = "build_plan: a PV bus is out of range, repeated or also a slack";
+            return NotInitError;
+        }
+        role[pv[t]] = 2;
+    }
+    for (int t = 0; t < npq; ++t) {
+        if (pq[t] < 0 || pq[t] >= n || role[pq[t]] != 0) {
+            msg = "build_plan: a PQ bus is out of range, repeated or also PV / slack";
+            return NotInitError;
+        }
+        role[pq[t]] = 3;
+    }
+    P.n = n;
+    P.nnzY = Yp[n];
+    P.Yp.assign(Yp, Yp + n + 1);
+    P.Yi.assign(Yi, Yi + P.nnzY);
+    P.Yx.assign(Yx, Yx + P.nnzY);
+    P.distributed = distributed;
+    P.slack0 = slack_ids[0];
+    P.slack_ids.assign(slack_ids, slack_ids + nslack);
+    P.weights.assign(weights, weights + n);
+    // retrieve_pv_with_slack (src/powerflow_algorithm/BaseAlgo.hpp:201-216)
+    if (distributed)
+        for (int t = 1; t < nslack; ++t) P.mypv.push_back(slack_ids[t]);
+    P.mypv.insert(P.mypv.end(), pv, pv + npv_in);
+    P.pq.assign(pq, pq + npq);
+    P.npv = (int)P.mypv.size();
+    P.npq = npq;
+    P.pvpq = P.mypv;
+    P.pvpq.insert(P.pvpq.end(), pq, pq + npq);
+    P.npvpq = P.npv + npq;
+    P.off = distributed ? 1 : 0;
+    P.m = P.npvpq + npq + P.off;
+    const int m = P.m;
+    if (m == 0) { msg = "build_plan: no PV or PQ bus"; return NotInitError; }
+
+    make_csr(P);
+
+    // ---------------------------------------------------------------- Jacobian pattern
+    std::vector<int> pvpq_inv(n, -1), pq_inv(n, -1);
+    for (int t = 0; t < P.npvpq; ++t) pvpq_inv[P.pvpq[t]] = t;
+    for (int t = 0; t < npq; ++t) pq_inv[P.pq[t]] = t;
+    const int off = P.off, npvpq = P.npvpq;
+    struct Trip { int row, col, src; uint8_t kind; double val; };
+    std::vector<Trip> T;
+    T.reserve(4 * (size_t)P.nnzY + n + 4);
+    for (int c = 0; c < npvpq; ++c) {
+        int bus = P.pvpq[c];
+        for (int p = Yp[bus]; p < Yp[bus + 1]; ++p)
+            if (pvpq_inv[Yi[p]] >= 0) T.push_back({pvpq_inv[Yi[p]] + off, c + off, p, 0, 0.0});
+        for (int p = Yp[bus]; p < Yp[bus + 1]; ++p)
+            if (pq_inv[Yi[p]] >= 0) T.push_back({npvpq + pq_inv[Yi[p]] + off, c + off, p, 1, 0.0});
+    }
+    for (int c = 0; c < npq; ++c) {
+        int bus = P.pq[c];
+        for (int p = Yp[bus]; p < Yp[bus + 1]; ++p)
+            if (pvpq_inv[Yi[p]] >= 0) T.push_back({pvpq_inv[Yi[p]] + off, npvpq + c + off, p, 2, 0.0});
+        for (int p = Yp[bus]; p < Yp[bus + 1]; ++p)
+            if (pq_inv[Yi[p]] >= 0) T.push_back({npvpq + pq_inv[Yi[p]] + off, npvpq + c + off, p, 3, 0.0});
+    }
+    if (distributed) {
+        const int s0 = P.slack0;
+        for (int c = 0; c < n; ++c) {
+            if (pvpq_inv[c] < 0) continue;
+            for (int p = Yp[c]; p < Yp[c + 1]; ++p)
+                if (Yi[p] == s0) T.push_back({0, pvpq_inv[c] + 1, p, 0, 0.0});
+        }
+        for (int c = 0; c < n; ++c) {
+            if (pq_inv[c] < 0) continue;
+            for (int p = Yp[c]; p < Yp[c + 1]; ++p)
+                if (Yi[p] == s0) T.push_back({0, npvpq + pq_inv[c] + 1, p, 2, 0.0});
+        }
+        T.push_back({0, 0, -1, 0, weights[s0]});
+        for (int t = 0; t < npvpq; ++t) {
+            double sw = weights[P.pvpq[t]];
+            if (std::fabs(sw) > 1e-7) T.push_back({t + 1, 0, -1, 0, sw});
+        }
+    }
+    std::stable_sort(T.begin(), T.end(), [](const Trip &a, const Trip &b) {
+        return a.col != b.col ? a.col < b.col : a.row < b.row;
+    });
+    const int nnzJ = (int)T.size();
+    P.Jp.assign(m + 1, 0);
+    P.Ji.resize(nnzJ);
+    P.jsrc.resize(nnzJ);
+    P.jkind.resize(nnzJ);
+    P.jconst.assign(nnzJ, 0.0);
+    for (int t = 0; t < nnzJ; ++t) {
+        if (t > 0 && T[t].col == T[t - 1].col && T[t].row == T[t - 1].row) {
+            msg = "build_plan: duplicate Jacobian entry (is a bus both slack and PV/PQ?)";
+            return NotInitError;
+        }
+        P.Jp[T[t].col + 1]++;
+        P.Ji[t] = T[t].row;
+        P.jsrc[t] = T[t].src;
+        P.jkind[t] = T[t].kind;
+        P.jconst[t] = T[t].val;
+    }
+    for (int c = 0; c < m; ++c) P.Jp[c + 1] += P.Jp[c];
+
+    // ---------------------------------------------------------------- LU analysis
+    {
+        std::vector<cplx> Vinit(V0, V0 + n);
+        std::vector<double> Jx;
+        host_jacobian(P, P.Yx.data(), Vinit.data(), Jx);
+        const int rc = analyze_lu(P, Jx, opt, msg);
+        if (rc != NoError) return rc;
+    }
+
     // ---------------------------------------------------------------- bus maps
     P.xP.assign(n, -1);
     P.xQ.assign(n, -1);
@@ -638,6 +663,77 @@ int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, con
         if (pq_inv[b] >= 0) P.xVm[b] = P.qinv[npvpq + pq_inv[b] + off];
     }
     if (distributed) P.xSlack = P.qinv[0];
+    return NoError;
+}
+
+int build_dc_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, const int *slack_ids, int nslack,
+                  const int *pv, int npv, const int *pq, int npq, const PlanOptions &opt, std::string &msg) {
+    P = Plan();
+    if (n <= 0 || nslack <= 0) {
+        msg = "build_dc_plan: the grid needs at least one bus and one slack bus";
+        return NotInitError;
+    }
+    if (check_ybus(n, Yp, Yi, msg) != NoError) return NotInitError;
+    for (int t = 0; t < nslack; ++t)
+        if (slack_ids[t] < 0 || slack_ids[t] >= n) { msg = "build_dc_plan: slack id out of range"; return NotInitError; }
+    for (int t = 0; t < npv; ++t)
+        if (pv[t] < 0 || pv[t] >= n) { msg = "build_dc_plan: PV bus out of range"; return NotInitError; }
+    for (int t = 0; t < npq; ++t)
+        if (pq[t] < 0 || pq[t] >= n) { msg = "build_dc_plan: PQ bus out of range"; return NotInitError; }
+    P.dc = true;
+    P.n = n;
+    P.nnzY = Yp[n];
+    P.Yp.assign(Yp, Yp + n + 1);
+    P.Yi.assign(Yi, Yi + P.nnzY);
+    P.Yx.assign(Yx, Yx + P.nnzY);
+    P.slack0 = slack_ids[0];
+    P.slack_ids.assign(slack_ids, slack_ids + nslack);
+    P.weights.assign(n, 0.0);
+    // BaseDCAlgo::compute_pf (src/powerflow_algorithm/BaseDCAlgo.tpp:55-66): the slacks after
+    // the first count as PV (retrieve_pv_with_slack, BaseAlgo.hpp:201-216); the slack buses are
+    // the buses neither PV nor PQ (extract_slack_bus_id, BaseAlgo.cpp:143-181); every other bus
+    // is an unknown angle, numbered in bus order (fill_mat_bus_id, BaseDCAlgo.tpp:192-201)
+    std::vector<char> tagged(n, 0);
+    for (int t = 1; t < nslack; ++t) tagged[slack_ids[t]] = 1;
+    for (int t = 0; t < npv; ++t) tagged[pv[t]] = 1;
+    for (int t = 0; t < npq; ++t) tagged[pq[t]] = 1;
+    std::vector<int> id(n, -1);
+    int m = 0;
+    for (int b = 0; b < n; ++b)
+        if (tagged[b]) id[b] = m++;
+    if (m == n) { msg = "build_dc_plan: every bus is PV or PQ, there is no slack"; return NotInitError; }
+    if (m == 0) { msg = "build_dc_plan: no PV or PQ bus"; return NotInitError; }
+    P.m = m;
+    make_csr(P);
+    // B = Re(Ybus) without the slack rows and columns, Ybus's pattern kept
+    // (remove_slack_buses, BaseDCAlgo.tpp:208-232)
+    P.Jp.assign(m + 1, 0);
+    for (int c = 0; c < n; ++c) {
+        if (id[c] < 0) continue;
+        for (int p = Yp[c]; p < Yp[c + 1]; ++p)
+            if (id[Yi[p]] >= 0) {
+                P.Ji.push_back(id[Yi[p]]);
+                P.jsrc.push_back(p);
+                P.jkind.push_back(0);
+                P.jconst.push_back(0.0);
+            }
+        P.Jp[id[c] + 1] = (int)P.Ji.size();
+    }
+    for (int c = 0; c < m; ++c) P.Jp[c + 1] = std::max(P.Jp[c + 1], P.Jp[c]);
+    std::vector<double> Bx(P.Ji.size());
+    for (size_t t = 0; t < Bx.size(); ++t) Bx[t] = Yx[P.jsrc[t]].real();
+    const int rc = analyze_lu(P, Bx, opt, msg);
+    if (rc != NoError) return rc;
+    // bus maps: right-hand side Re(Sbus(b)) at xP[b], angle at xVa[b]
+    P.xP.assign(n, -1);
+    P.xQ.assign(n, -1);
+    P.xVa.assign(n, -1);
+    P.xVm.assign(n, -1);
+    for (int b = 0; b < n; ++b)
+        if (id[b] >= 0) {
+            P.xP[b] = P.pinv[id[b]];
+            P.xVa[b] = P.qinv[id[b]];
+        }
     return NoError;
 }
 

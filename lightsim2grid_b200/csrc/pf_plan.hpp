@@ -46,6 +46,7 @@ struct Plan {
     std::vector<int> csr_of_csc;      // CSC position -> CSR position
     std::vector<cplx> Rx;             // base values, CSR order
     bool distributed = false;
+    bool dc = false;                  // DC plan: B = Re(Ybus) without the slack, no Newton loop
     int slack0 = 0;
     std::vector<int> slack_ids;
     std::vector<double> weights;      // n
@@ -129,6 +130,12 @@ int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, con
 int compact_lu_offset(int m);
 bool compact_fits(const Plan &P);
 void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out);  // 2 words per op
+
+// Builds a DC plan (BaseDCAlgo, src/powerflow_algorithm/BaseDCAlgo.tpp): the matrix is
+// B = Re(Ybus) over every bus except the first slack (the other slacks count as PV), factorised
+// and scheduled like a Jacobian.  Ybus is the DC admittance matrix.  Returns an Err code.
+int build_dc_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, const int *slack_ids, int nslack,
+                  const int *pv, int npv, const int *pq, int npq, const PlanOptions &opt, std::string &msg);
 
 // Host evaluation of the Jacobian values (J CSC order) at V for Ybus values Yx (CSC order).
 void host_jacobian(const Plan &P, const cplx *Yx, const cplx *V, std::vector<double> &Jx);

@@ -145,6 +145,31 @@ class GridModel:
         Y.sort_indices()
         return Y
 
+    def get_dcYbus(self):
+        """DC Ybus (fillYbus with ac = false, GridModel.cpp:676-699): per branch in service
+        y_ff = y_tt = 1/x, y_ft = y_tf = -1/x (TwoSidesContainer_rxh_A.hpp:933-939)."""
+        on = self.line_status
+        f, t = self.line_from[on], self.line_to[on]
+        yd = (1.0 / (self.line_x[on] + 0j))
+        rows = np.concatenate([f, t, f, t])
+        cols = np.concatenate([f, t, t, f])
+        vals = np.concatenate([yd, yd, -yd, -yd])
+        Y = sparse.csc_matrix((vals, (rows, cols)), shape=(self.n_bus, self.n_bus), dtype=np.complex128)
+        Y.sum_duplicates()
+        Y.sort_indices()
+        return Y
+
+    def dc_branch_coeffs(self, branch_ids):
+        """DC Ybus coefficients of the given branches, in the reference's order."""
+        out = []
+        for br in branch_ids:
+            if not self.line_status[br]:
+                continue
+            b1, b2 = int(self.line_from[br]), int(self.line_to[br])
+            yd = 1.0 / (self.line_x[br] + 0j)
+            out.extend([Coeff(b1, b1, yd), Coeff(b2, b2, yd), Coeff(b1, b2, -yd), Coeff(b2, b1, -yd)])
+        return out
+
     def _sbus_from(self, gen_p, sgen_p, load_p, load_q):
         S = np.zeros(self.n_bus, dtype=np.complex128)
         np.add.at(S, self.gen_bus, gen_p)

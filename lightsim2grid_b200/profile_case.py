@@ -29,6 +29,7 @@ def main():
     ap.add_argument("--refine-threshold", type=float, default=0.0)
     ap.add_argument("--lu-reuse", type=float, default=0.0, help="LU reuse threshold (<= 0: never, the default)")
     ap.add_argument("--check", action="store_true", help="compare the voltages with an FP64 plan's")
+    ap.add_argument("--dc", action="store_true", help="DC power flows (DC Ybus, DC outage coefficients)")
     args = ap.parse_args()
 
     import torch
@@ -43,7 +44,10 @@ def main():
     Vn = base.get_V()
     nb = g.nb_powerline() if args.cases <= 0 else min(args.cases, g.nb_powerline())
     coeffs = [g.branch_coeffs([b]) for b in range(nb)]
-    plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, threads=args.threads,
+    if args.dc:
+        Y = g.get_dcYbus()
+        coeffs = [g.dc_branch_coeffs([b]) for b in range(nb)]
+    plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, dc=args.dc, threads=args.threads,
                 lu_placement=args.lu_placement, fuse_forward=args.fuse_forward, max_ctas_per_sm=args.ctas_per_sm,
                 refine=args.refine, refine_threshold=args.refine_threshold, lu_reuse_threshold=args.lu_reuse)
     lib = plan._lib

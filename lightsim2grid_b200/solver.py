@@ -15,7 +15,7 @@ from . import _native as nat
 
 
 class SolverType(enum.IntEnum):
-    """Members 0-21 are the reference's (src/ChooseSolver.hpp:17-25); 22-25 are this engine's."""
+    """Members 0-21 are the reference's (src/ChooseSolver.hpp:17-25); 22-26 are this engine's."""
 
     SparseLU = 0
     KLU = 1
@@ -47,6 +47,8 @@ class SolverType(enum.IntEnum):
     GPUNRMixed = 24
     #: single slack, FP32 LU and solves, FP64 mismatch / update / convergence test
     GPUNRMixedSingleSlack = 25
+    #: DC power flow on the GPU, FP64 (drop-in for KLUDC)
+    GPUDC = 26
 
 
 class ErrorType(enum.IntEnum):
@@ -95,7 +97,7 @@ class Plan:
 
     def __init__(self, Ybus, V0, Sbus, slack_ids, slack_weights, pv, pq, distributed=False, precision=0,
                  threads=0, lu_placement=0, fuse_forward=0, fp64_fallback=0, max_ctas_per_sm=0, refine=0,
-                 refine_threshold=0.0, lu_reuse_threshold=0.0):
+                 refine_threshold=0.0, lu_reuse_threshold=0.0, dc=False):
         self._lib = nat.load()
         Y = canonical_csc(Ybus)
         n = Y.shape[0]
@@ -122,12 +124,22 @@ class Plan:
                             refine=int(refine), refine_threshold=float(refine_threshold),
                             lu_reuse_threshold=float(lu_reuse_threshold))
         h = nat.ctypes.c_void_p()
-        rc = self._lib.pf_plan_create(
-            n, nat.ptr(self.Yp, nat.i32p), nat.ptr(self.Yi, nat.i32p), nat.cptr(self.Yx), nat.cptr(V0),
-            nat.cptr(Sbus), nat.ptr(self.slack_ids, nat.i32p), self.slack_ids.size, nat.ptr(w, nat.f64p),
-            nat.ptr(self.pv, nat.i32p), self.pv.size, nat.ptr(self.pq, nat.i32p), self.pq.size,
-            1 if distributed else 0, nat.ctypes.byref(opt), nat.ctypes.byref(h))
-        nat.check(rc, "pf_plan_create", self._lib)
+        self.dc = bool(dc)
+        if self.dc:
+            # DC power flow (BaseDCAlgo): Ybus is the DC admittance matrix, FP64
+            self.precision = 0
+            rc = self._lib.pf_dc_plan_create(
+                n, nat.ptr(self.Yp, nat.i32p), nat.ptr(self.Yi, nat.i32p), nat.cptr(self.Yx),
+                nat.ptr(self.slack_ids, nat.i32p), self.slack_ids.size, nat.ptr(self.pv, nat.i32p), self.pv.size,
+                nat.ptr(self.pq, nat.i32p), self.pq.size, nat.ctypes.byref(opt), nat.ctypes.byref(h))
+            nat.check(rc, "pf_dc_plan_create", self._lib)
+        else:
+            rc = self._lib.pf_plan_create(
+                n, nat.ptr(self.Yp, nat.i32p), nat.ptr(self.Yi, nat.i32p), nat.cptr(self.Yx), nat.cptr(V0),
+                nat.cptr(Sbus), nat.ptr(self.slack_ids, nat.i32p), self.slack_ids.size, nat.ptr(w, nat.f64p),
+                nat.ptr(self.pv, nat.i32p), self.pv.size, nat.ptr(self.pq, nat.i32p), self.pq.size,
+                1 if distributed else 0, nat.ctypes.byref(opt), nat.ctypes.byref(h))
+            nat.check(rc, "pf_plan_create", self._lib)
         self._h = h
 
     def __del__(self):
@@ -254,6 +266,7 @@ class _GPUNRSolverBase:
 
     _distributed = False
     _precision = 0
+    _dc = False
 
     def __init__(self, **plan_options):
         self._plan = None
@@ -287,7 +300,7 @@ class _GPUNRSolverBase:
             w[sl] = 1.0 / max(sl.size, 1)
         if self._plan is None or not self._plan.same_structure(Y, slack_ids, pv, pq):
             self._plan = Plan(Y, V, Sbus, slack_ids, w, pv, pq, distributed=self._distributed,
-                              precision=self._precision, **self._plan_options)
+                              precision=self._precision, dc=self._dc, **self._plan_options)
         else:
             self._plan.set_ybus_values(Y.data)
         Vout, conv, it, err = self._plan.solve(V, Sbus, max_iter, tol)
@@ -356,6 +369,16 @@ class GPUNRMixedSolverSingleSlack(_GPUNRSolverBase):
     _precision = 1
 
 
+class GPUDCSolver(_GPUNRSolverBase):
+    """Drop-in for KLUDCSolver (BaseDCAlgo, src/powerflow_algorithm/BaseDCAlgo.tpp): one FP64
+    linear solve of B theta = Re(Sbus) with B = Re(Ybus) of the DC Ybus, without the slack."""
+
+    _dc = True
+
+    def get_J(self):
+        raise RuntimeError("get_J: a DC solver has no Jacobian")
+
+
 class GPUNRMixedSolver(_GPUNRSolverBase):
     """Distributed slack, FP32 LU and solves, FP64 mismatch, update and convergence test."""
 
@@ -368,4 +391,5 @@ SOLVER_CLASSES = {
     SolverType.GPUNRSingleSlack: GPUNRSolverSingleSlack,
     SolverType.GPUNRMixed: GPUNRMixedSolver,
     SolverType.GPUNRMixedSingleSlack: GPUNRMixedSolverSingleSlack,
+    SolverType.GPUDC: GPUDCSolver,
 }
