@@ -253,6 +253,40 @@ int pf_assemble_sbus_device(const pf_sbus_layout *lay, int nsteps, const double 
                             const double *load_p, const double *load_q, double sn_mva, double *sbus_ri,
                             void *stream);
 
+/* Native serving core (no counterpart in the reference, which has no request loop): power-flow
+   and N-1 requests over several grids, continuously batched on one GPU.  Each grid: its plan,
+   base-case voltages and injections (host arrays, copied to the device once), its branch-removal
+   coefficients as CSR over branches (as for pf_batch_n1) and its Newton settings.  Device memory
+   is one arena of hbm_budget bytes allocated at creation; each admitted request gets one region
+   of it (inputs, outputs, kernel working memory) and one of `slots` streams with pinned staging.
+   pf_server_submit queues a request: kind 0 = one power flow with the base injections scaled
+   bus by bus by scale[n]; kind 1 = the outages of `nbranches` branches from the base-case state.
+   V_out (rows x n complex, rows = 1 or nbranches), iters_out and errs_out (rows) receive the
+   results in case order (islanded outages: zero row, SingularMatrix; failures: zero row).
+   pf_server_poll admits queued requests oldest first while a slot is free and the arena has room,
+   launches them, and writes the ids of finished requests (their outputs filled) to done_ids;
+   it returns how many.  Not thread-safe: one caller thread per server. */
+typedef struct pf_server pf_server;
+typedef struct pf_server_grid {
+    pf_plan *plan;
+    const double *V0_ri;     /* base-case voltages (n complex)                     */
+    const double *Sbus_ri;   /* base-case injections (n complex)                   */
+    int nbr;                 /* branches                                           */
+    const int *case_ptr;     /* nbr + 1: coefficients of branch b: [case_ptr[b], case_ptr[b+1]) */
+    const int *rows;
+    const int *cols;
+    const double *vals_ri;
+    int max_iter;            /* 0: 10     */
+    double tol;              /* 0: 1e-8   */
+} pf_server_grid;
+int pf_server_create(const pf_server_grid *grids, int ngrids, long long hbm_budget, int slots, int max_instances,
+                     pf_server **server);
+int pf_server_submit(pf_server *server, long long id, int grid, int kind, const double *scale, int nbranches,
+                     const int *branches, double *V_out, int *iters_out, int *errs_out);
+int pf_server_poll(pf_server *server, long long *done_ids, int cap);
+int pf_server_state(const pf_server *server, int *pending, int *inflight, long long *bytes_in_use);
+void pf_server_destroy(pf_server *server);
+
 /* Scratch bytes pf_batch_device_scratch needs to run `ctas` CTAs at once (at most the plan's
    grid); < 0 on error. */
 long long pf_scratch_bytes(const pf_plan *plan, int ctas);

@@ -57,6 +57,13 @@ class PfSbusLayout(ctypes.Structure):
                 ("sgen_ids", ctypes.c_void_p), ("load_ptr", ctypes.c_void_p), ("load_ids", ctypes.c_void_p)]
 
 
+class PfServerGrid(ctypes.Structure):
+    _fields_ = [("plan", ctypes.c_void_p), ("V0_ri", ctypes.c_void_p), ("Sbus_ri", ctypes.c_void_p),
+                ("nbr", ctypes.c_int), ("case_ptr", ctypes.c_void_p), ("rows", ctypes.c_void_p),
+                ("cols", ctypes.c_void_p), ("vals_ri", ctypes.c_void_p), ("max_iter", ctypes.c_int),
+                ("tol", ctypes.c_double)]
+
+
 #: exported symbols, as declared in include/lightsim2grid_b200.h
 SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_get", "pf_set_ybus_values",
            "pf_solve", "pf_get_J", "pf_batch_n1", "pf_n1_prepare", "pf_batch_ts", "pf_batch_device", "pf_timers",
@@ -64,7 +71,8 @@ SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_g
            "pf_batch_device_phase_trace", "pf_batch_device_noalloc", "pf_batch_device_scratch",
            "pf_scratch_bytes", "pf_multi_create", "pf_multi_launch", "pf_multi_info", "pf_multi_destroy",
            "pf_flows_device", "pf_flows_host", "pf_ybus_positions", "pf_assemble_ybus_device",
-           "pf_set_ybus_values_device", "pf_assemble_sbus_device", "pf_dc_plan_create")
+           "pf_set_ybus_values_device", "pf_assemble_sbus_device", "pf_dc_plan_create", "pf_server_create",
+           "pf_server_submit", "pf_server_poll", "pf_server_state", "pf_server_destroy")
 
 
 def load(path=None):
@@ -132,6 +140,18 @@ def load(path=None):
     lib.pf_flows_host.restype = ctypes.c_int
     lib.pf_flows_host.argtypes = [ctypes.POINTER(PfBranchSet), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pf_server_create.restype = ctypes.c_int
+    lib.pf_server_create.argtypes = [ctypes.POINTER(PfServerGrid), ctypes.c_int, ctypes.c_longlong, ctypes.c_int,
+                                     ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    lib.pf_server_submit.restype = ctypes.c_int
+    lib.pf_server_submit.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pf_server_poll.restype = ctypes.c_int
+    lib.pf_server_poll.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    lib.pf_server_state.restype = ctypes.c_int
+    lib.pf_server_state.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pf_server_destroy.restype = None
+    lib.pf_server_destroy.argtypes = [ctypes.c_void_p]
     lib.pf_dc_plan_create.restype = ctypes.c_int
     lib.pf_dc_plan_create.argtypes = [ctypes.c_int, i32p, i32p, f64p, i32p, ctypes.c_int, i32p, ctypes.c_int, i32p,
                                       ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]

@@ -1,0 +1,443 @@
+// Native serving core: power-flow and N-1 requests over several plans, continuously batched
+// on one GPU.  Built on the public C ABI (pf_n1_prepare, pf_batch_device_scratch).
+//
+// Every grid keeps its plan, base-case voltages and injections and its branch-removal
+// coefficients; device memory is one arena of the HBM budget, carved first-fit into one region
+// per admitted request (inputs, outputs and the kernel's working memory), so serving allocates
+// no device memory after creation.  Requests are admitted oldest first when a stream slot is
+// free and their region fits; each runs as its own launch on its slot's stream with pinned
+// staging, so requests that arrive while others run overlap with them on the device.  Results
+// are copied into the caller's buffers when the slot's event has completed.
+#include "../../include/lightsim2grid_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <complex>
+#include <cstring>
+#include <deque>
+#include <list>
+#include <string>
+#include <vector>
+
+#include "pf_capi_internal.hpp"
+
+namespace {
+
+using cplx = std::complex<double>;
+
+int fail(const std::string &msg) {
+    l2g::set_last_error(msg);
+    return -1;
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// First-fit allocator over [0, size): holes sorted by offset, coalesced on release.
+struct Arena {
+    size_t size = 0;
+    std::list<std::pair<size_t, size_t>> holes;
+    void init(size_t s) {
+        size = s;
+        holes.assign(1, {0, s});
+    }
+    bool alloc(size_t n, size_t &off) {
+        n = align256(n);
+        for (auto it = holes.begin(); it != holes.end(); ++it)
+            if (it->second >= n) {
+                off = it->first;
+                if (it->second == n) holes.erase(it);
+                else {
+                    it->first += n;
+                    it->second -= n;
+                }
+                return true;
+            }
+        return false;
+    }
+    void release(size_t off, size_t n) {
+        n = align256(n);
+        auto it = holes.begin();
+        while (it != holes.end() && it->first < off) ++it;
+        it = holes.insert(it, {off, n});
+        auto nx = std::next(it);
+        if (nx != holes.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            holes.erase(nx);
+        }
+        if (it != holes.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                holes.erase(it);
+            }
+        }
+    }
+};
+
+struct Grid {
+    pf_plan *plan = nullptr;
+    int n = 0, nbr = 0, ctas = 0;
+    std::vector<cplx> S;            // base injections (host)
+    void *dV0 = nullptr, *dS = nullptr;
+    std::vector<int> cptr, rows, cols;
+    std::vector<cplx> vals;
+    double tol = 1e-8;
+    int max_iter = 10;
+};
+
+struct Slot {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    unsigned char *pin_in = nullptr, *pin_out = nullptr;
+    bool high = false;  // on a high-priority stream
+};
+
+// Requests with at most this many instance-buses run on high-priority streams: the block
+// scheduler then dispatches their CTAs before the pending CTAs of large batches launched
+// earlier, so a small request does not wait behind them.
+constexpr long long kSmallWork = 20000;
+
+struct Req {
+    long long id = 0;
+    int grid = 0, kind = 0, ncases = 0, ninst = 0;
+    std::vector<double> scale;
+    std::vector<int> solv;                 // N-1: per case, solvable
+    std::vector<int> optr, opos;
+    std::vector<cplx> oval;
+    double *V = nullptr;                   // caller buffers, case order
+    int *iters = nullptr, *errs = nullptr;
+    size_t scratch = 0, outs = 0, ins = 0, bytes = 0, off = 0;
+    int slot = -1;
+};
+
+}  // namespace
+
+struct pf_server {
+    std::vector<Grid> grids;
+    int max_k = 64, nslots = 0;
+    size_t budget = 0, in_use = 0, in_cap = 0, out_cap = 0;
+    unsigned char *arena_ptr = nullptr;
+    Arena arena;
+    std::vector<Slot> slots;
+    std::vector<int> free_high, free_low;
+    int *djf = nullptr, *djc = nullptr;
+    std::deque<Req *> pending;
+    std::vector<Req *> inflight;
+};
+
+namespace {
+
+void destroy(pf_server *s) {
+    for (Grid &g : s->grids) {
+        if (g.dV0) cudaFree(g.dV0);
+        if (g.dS) cudaFree(g.dS);
+    }
+    for (Slot &sl : s->slots) {
+        if (sl.ev) cudaEventDestroy(sl.ev);
+        if (sl.st) cudaStreamDestroy(sl.st);
+        if (sl.pin_in) cudaFreeHost(sl.pin_in);
+        if (sl.pin_out) cudaFreeHost(sl.pin_out);
+    }
+    if (s->arena_ptr) cudaFree(s->arena_ptr);
+    if (s->djf) cudaFree(s->djf);
+    if (s->djc) cudaFree(s->djc);
+    for (Req *r : s->pending) delete r;
+    for (Req *r : s->inflight) delete r;
+    delete s;
+}
+
+// Inputs of a request: the scaled injections (PF) or its overrides; sizes of its region.
+int prepare(pf_server *s, Req *r) {
+    Grid &g = s->grids[r->grid];
+    if (r->kind == 0) {
+        r->ninst = 1;
+        r->ins = align256((size_t)g.n * 16);
+    } else {
+        std::vector<int> cp(r->ncases + 1, 0), rows, cols;
+        std::vector<cplx> vals;
+        for (int c = 0; c < r->ncases; ++c) {
+            const int b = r->solv[c];  // branch id, replaced by the solvable flag below
+            if (b < 0 || b >= g.nbr) return fail("pf_server_submit: branch id out of range");
+            for (int q = g.cptr[b]; q < g.cptr[b + 1]; ++q) {
+                rows.push_back(g.rows[q]);
+                cols.push_back(g.cols[q]);
+                vals.push_back(g.vals[q]);
+            }
+            cp[c + 1] = (int)rows.size();
+        }
+        if (rows.empty()) {
+            rows.push_back(0);
+            cols.push_back(0);
+            vals.push_back(0.0);
+        }
+        const int cap = std::max(cp[r->ncases], 1);
+        r->optr.assign(r->ncases + 1, 0);
+        r->opos.assign(cap, 0);
+        r->oval.assign(cap, 0.0);
+        std::vector<int> solv(r->ncases, 0);
+        const int w = pf_n1_prepare(g.plan, r->ncases, cp.data(), rows.data(), cols.data(),
+                                    reinterpret_cast<const double *>(vals.data()), solv.data(), r->optr.data(),
+                                    r->opos.data(), reinterpret_cast<double *>(r->oval.data()), cap);
+        if (w < 0) return w;
+        r->solv = solv;
+        r->ninst = 0;
+        for (int c = 0; c < r->ncases; ++c) r->ninst += solv[c];
+        r->optr.resize(r->ninst + 1);
+        r->opos.resize(std::max(w, 1));
+        r->oval.resize(std::max(w, 1));
+        r->ins = align256((size_t)(r->ninst + 1) * 4) + align256(r->opos.size() * 4) + align256(r->oval.size() * 16);
+    }
+    if (r->ninst > s->max_k) return fail("pf_server_submit: request has more instances than the server's maximum");
+    if (r->ins > s->in_cap) return fail("pf_server_submit: request inputs exceed the staging buffers");
+    const int ctas = std::max(1, std::min(r->ninst, g.ctas));
+    r->scratch = r->ninst ? align256((size_t)pf_scratch_bytes(g.plan, ctas)) : 0;
+    r->outs = align256((size_t)r->ninst * g.n * 16 + 8 * (size_t)r->ninst);
+    r->bytes = r->scratch + r->outs + r->ins;
+    return 0;
+}
+
+int launch(pf_server *s, Req *r) {
+    Grid &g = s->grids[r->grid];
+    Slot &sl = s->slots[r->slot];
+    unsigned char *base = s->arena_ptr + r->off;
+    unsigned char *scr = base, *out = base + r->scratch, *in = out + r->outs;
+    cudaError_t e = cudaSuccess;
+    if (r->ninst > 0) {
+        pf_device_batch b{};
+        b.n_inst = r->ninst;
+        b.V0 = g.dV0;
+        b.max_iter = g.max_iter;
+        b.tol = g.tol;
+        b.job_first = s->djf;
+        b.job_count = s->djc;
+        b.njobs = r->ninst;
+        b.Vout = out;
+        b.iters = reinterpret_cast<int *>(out + (size_t)r->ninst * g.n * 16);
+        b.errs = b.iters + r->ninst;
+        if (r->kind == 0) {
+            cplx *S = reinterpret_cast<cplx *>(sl.pin_in);
+            for (int i = 0; i < g.n; ++i) S[i] = g.S[i] * r->scale[i];
+            e = cudaMemcpyAsync(in, sl.pin_in, (size_t)g.n * 16, cudaMemcpyHostToDevice, sl.st);
+            b.Sbus = in;
+        } else {
+            const size_t a1 = align256((size_t)(r->ninst + 1) * 4), a2 = align256(r->opos.size() * 4);
+            std::memcpy(sl.pin_in, r->optr.data(), (size_t)(r->ninst + 1) * 4);
+            std::memcpy(sl.pin_in + a1, r->opos.data(), r->opos.size() * 4);
+            std::memcpy(sl.pin_in + a1 + a2, r->oval.data(), r->oval.size() * 16);
+            e = cudaMemcpyAsync(in, sl.pin_in, a1 + a2 + r->oval.size() * 16, cudaMemcpyHostToDevice, sl.st);
+            b.Sbus = g.dS;
+            b.ovr_ptr = reinterpret_cast<const int *>(in);
+            b.ovr_pos = reinterpret_cast<const int *>(in + a1);
+            b.ovr_val = in + a1 + a2;
+        }
+        if (e != cudaSuccess) return fail(std::string("pf_server: upload: ") + cudaGetErrorString(e));
+        const int rc = pf_batch_device_scratch(g.plan, &b, scr, (long long)r->scratch, sl.st);
+        if (rc != 0) return rc;
+        e = cudaMemcpyAsync(sl.pin_out, out, (size_t)r->ninst * g.n * 16 + 8 * (size_t)r->ninst,
+                            cudaMemcpyDeviceToHost, sl.st);
+        if (e != cudaSuccess) return fail(std::string("pf_server: download: ") + cudaGetErrorString(e));
+    }
+    e = cudaEventRecord(sl.ev, sl.st);
+    if (e != cudaSuccess) return fail(std::string("pf_server: event: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+// Results of a finished request into the caller's buffers, in case order.
+void deliver(pf_server *s, Req *r) {
+    Grid &g = s->grids[r->grid];
+    const unsigned char *po = s->slots[r->slot].pin_out;
+    const cplx *V = reinterpret_cast<const cplx *>(po);
+    const int *it = reinterpret_cast<const int *>(po + (size_t)r->ninst * g.n * 16);
+    const int *er = it + r->ninst;
+    cplx *Vo = reinterpret_cast<cplx *>(r->V);
+    const int rows = r->kind == 0 ? 1 : r->ncases;
+    int k = 0;
+    for (int c = 0; c < rows; ++c) {
+        const bool solved = r->kind == 0 || r->solv[c];
+        if (!solved) {
+            std::fill(Vo + (size_t)c * g.n, Vo + (size_t)(c + 1) * g.n, cplx(0.0, 0.0));
+            r->iters[c] = 0;
+            r->errs[c] = 1;  // SingularMatrix: the outage islands the grid (skipped)
+            continue;
+        }
+        if (er[k] == 0) std::memcpy(Vo + (size_t)c * g.n, V + (size_t)k * g.n, (size_t)g.n * 16);
+        else std::fill(Vo + (size_t)c * g.n, Vo + (size_t)(c + 1) * g.n, cplx(0.0, 0.0));
+        r->iters[c] = it[k];
+        r->errs[c] = er[k];
+        ++k;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int pf_server_create(const pf_server_grid *grids, int ngrids, long long hbm_budget, int slots, int max_instances,
+                     pf_server **out) {
+    if (!out || !grids || ngrids <= 0 || hbm_budget <= 0 || slots <= 0 || max_instances <= 0)
+        return fail("pf_server_create: invalid argument");
+    *out = nullptr;
+    pf_server *s = new pf_server();
+    s->max_k = max_instances;
+    s->budget = (size_t)hbm_budget;
+    int nmax = 0;
+    cudaError_t e;
+    for (int i = 0; i < ngrids; ++i) {
+        const pf_server_grid &gi = grids[i];
+        pf_plan_info info;
+        if (!gi.plan || pf_plan_info_get(gi.plan, &info) != 0 || !gi.V0_ri || !gi.Sbus_ri || gi.nbr < 0 ||
+            (gi.nbr > 0 && (!gi.case_ptr || !gi.rows || !gi.cols || !gi.vals_ri))) {
+            destroy(s);
+            return fail("pf_server_create: invalid grid " + std::to_string(i));
+        }
+        Grid g;
+        g.plan = gi.plan;
+        g.n = info.n;
+        g.ctas = info.grid;
+        g.nbr = gi.nbr;
+        g.max_iter = gi.max_iter > 0 ? gi.max_iter : 10;
+        g.tol = gi.tol > 0 ? gi.tol : 1e-8;
+        const cplx *S = reinterpret_cast<const cplx *>(gi.Sbus_ri);
+        g.S.assign(S, S + g.n);
+        g.cptr.assign(gi.case_ptr, gi.case_ptr + gi.nbr + 1);
+        const int nc = gi.nbr > 0 ? gi.case_ptr[gi.nbr] : 0;
+        g.rows.assign(gi.rows, gi.rows + nc);
+        g.cols.assign(gi.cols, gi.cols + nc);
+        const cplx *cv = reinterpret_cast<const cplx *>(gi.vals_ri);
+        g.vals.assign(cv, cv + nc);
+        if ((e = cudaMalloc(&g.dV0, (size_t)g.n * 16)) != cudaSuccess ||
+            (e = cudaMalloc(&g.dS, (size_t)g.n * 16)) != cudaSuccess ||
+            (e = cudaMemcpy(g.dV0, gi.V0_ri, (size_t)g.n * 16, cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(g.dS, gi.Sbus_ri, (size_t)g.n * 16, cudaMemcpyHostToDevice)) != cudaSuccess) {
+            s->grids.push_back(g);
+            destroy(s);
+            return fail(std::string("pf_server_create: grid upload: ") + cudaGetErrorString(e));
+        }
+        nmax = std::max(nmax, g.n);
+        s->grids.push_back(g);
+    }
+    s->in_cap = std::max(align256((size_t)nmax * 16), (size_t)s->max_k * 40 * 24 + 1024);
+    s->out_cap = (size_t)s->max_k * nmax * 16 + 8 * (size_t)s->max_k + 256;
+    std::vector<int> jf(s->max_k), jc(s->max_k, 1);
+    for (int i = 0; i < s->max_k; ++i) jf[i] = i;
+    if ((e = cudaMalloc(&s->arena_ptr, s->budget)) != cudaSuccess ||
+        (e = cudaMalloc(&s->djf, (size_t)s->max_k * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&s->djc, (size_t)s->max_k * 4)) != cudaSuccess ||
+        (e = cudaMemcpy(s->djf, jf.data(), jf.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(s->djc, jc.data(), jc.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        destroy(s);
+        return fail(std::string("pf_server_create: device memory: ") + cudaGetErrorString(e));
+    }
+    s->arena.init(s->budget);
+    s->slots.resize(slots);
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    for (int i = 0; i < slots; ++i) {
+        Slot &sl = s->slots[i];
+        sl.high = i < (slots + 1) / 2;
+        if ((e = cudaStreamCreateWithPriority(&sl.st, cudaStreamNonBlocking, sl.high ? prio_high : prio_low)) !=
+                cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaHostAlloc(reinterpret_cast<void **>(&sl.pin_in), s->in_cap, cudaHostAllocDefault)) != cudaSuccess ||
+            (e = cudaHostAlloc(reinterpret_cast<void **>(&sl.pin_out), s->out_cap, cudaHostAllocDefault)) !=
+                cudaSuccess) {
+            destroy(s);
+            return fail(std::string("pf_server_create: slots: ") + cudaGetErrorString(e));
+        }
+    }
+    for (int i = slots - 1; i >= 0; --i) (s->slots[i].high ? s->free_high : s->free_low).push_back(i);
+    s->nslots = slots;
+    *out = s;
+    return 0;
+}
+
+int pf_server_submit(pf_server *s, long long id, int grid, int kind, const double *scale, int nbranches,
+                     const int *branches, double *V_out, int *iters_out, int *errs_out) {
+    if (!s || grid < 0 || grid >= (int)s->grids.size() || (kind != 0 && kind != 1) || !V_out || !iters_out ||
+        !errs_out || (kind == 0 && !scale) || (kind == 1 && (nbranches <= 0 || !branches)))
+        return fail("pf_server_submit: invalid argument");
+    Req *r = new Req();
+    r->id = id;
+    r->grid = grid;
+    r->kind = kind;
+    r->V = V_out;
+    r->iters = iters_out;
+    r->errs = errs_out;
+    if (kind == 0) {
+        r->scale.assign(scale, scale + s->grids[grid].n);
+    } else {
+        r->ncases = nbranches;
+        r->solv.assign(branches, branches + nbranches);
+    }
+    const int rc = prepare(s, r);
+    if (rc != 0) {
+        delete r;
+        return rc;
+    }
+    if (r->bytes > s->budget) {
+        delete r;
+        return fail("pf_server_submit: the request needs more device memory than the whole budget");
+    }
+    s->pending.push_back(r);
+    return 0;
+}
+
+int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
+    if (!s || (cap > 0 && !done_ids)) return fail("pf_server_poll: invalid argument");
+    int nd = 0;
+    // completions
+    for (size_t i = 0; i < s->inflight.size() && nd < cap;) {
+        Req *r = s->inflight[i];
+        const cudaError_t q = cudaEventQuery(s->slots[r->slot].ev);
+        if (q == cudaErrorNotReady) {
+            ++i;
+            continue;
+        }
+        if (q != cudaSuccess) return fail(std::string("pf_server_poll: ") + cudaGetErrorString(q));
+        deliver(s, r);
+        s->arena.release(r->off, r->bytes);
+        s->in_use -= align256(r->bytes);
+        (s->slots[r->slot].high ? s->free_high : s->free_low).push_back(r->slot);
+        done_ids[nd++] = r->id;
+        delete r;
+        s->inflight[i] = s->inflight.back();
+        s->inflight.pop_back();
+    }
+    // admissions, oldest first
+    while (!s->pending.empty() && (!s->free_high.empty() || !s->free_low.empty())) {
+        Req *r = s->pending.front();
+        size_t off = 0;
+        if (!s->arena.alloc(r->bytes, off)) break;
+        s->pending.pop_front();
+        r->off = off;
+        s->in_use += align256(r->bytes);
+        // small requests prefer high-priority streams, large ones low-priority ones
+        const bool small = (long long)r->ninst * s->grids[r->grid].n <= kSmallWork;
+        std::vector<int> &pref = small ? s->free_high : s->free_low;
+        std::vector<int> &other = small ? s->free_low : s->free_high;
+        std::vector<int> &pool = pref.empty() ? other : pref;
+        r->slot = pool.back();
+        pool.pop_back();
+        const int rc = launch(s, r);
+        s->inflight.push_back(r);
+        if (rc != 0) return rc;
+    }
+    return nd;
+}
+
+int pf_server_state(const pf_server *s, int *pending, int *inflight, long long *bytes_in_use) {
+    if (!s) return fail("pf_server_state: null argument");
+    if (pending) *pending = (int)s->pending.size();
+    if (inflight) *inflight = (int)s->inflight.size();
+    if (bytes_in_use) *bytes_in_use = (long long)s->in_use;
+    return 0;
+}
+
+void pf_server_destroy(pf_server *s) {
+    if (!s) return;
+    for (Req *r : s->inflight) cudaEventSynchronize(s->slots[r->slot].ev);
+    destroy(s);
+}
+
+}  // extern "C"
