@@ -83,12 +83,18 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a while to start: wait for its first sample, keep only later ones
+        t_end = time.time() + 5.0
+        while not self.lines and time.time() < t_end and self.proc.poll() is None:
+            time.sleep(0.005)
+        self.first = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -104,7 +110,8 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        first = getattr(self, "first", 0)
+        for ln in (self.lines[first:] if len(self.lines) > first else self.lines):
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
                 continue
