@@ -53,6 +53,23 @@ int pf_dc_plan_create(int n, const int *colptr, const int *rowind, const double 
                       int nslack, const int *pv, int npv, const int *pq, int npq, const pf_options *opts,
                       pf_plan **plan);
 
+/* Fast decoupled power flow plan (BaseFDPFAlgo::compute_pf, src/powerflow_algorithm/
+   BaseFDPFAlgo.tpp:11-173; the reference's FDPF_XB_* / FDPF_BX_* solvers, src/ChooseSolver.hpp:
+   21-24).  bp_* and bpp_* are the grid-level B' and B'' (n x n, real CSC) that
+   GridModel::fillBp_Bpp builds for the XB or BX method (src/GridModel.cpp:1037-1064); the plan
+   keeps B'[pvpq, pvpq] and B''[pq, pq] (pvpq = slacks after the first, pv, pq), factorises
+   both once and uses those factors for every later call and instance, as the reference's batch
+   computers do (the solver is told nothing changed after the base power flow).  Each iteration
+   is a B' half-step on the angles and a B'' half-step on the magnitudes, each followed by the
+   mismatch (V conj(Ybus V) - Sbus + Re(sum Sbus) w) / Vm; converged when its P (pvpq) and Q (pq)
+   parts are below tol.  FP64.  pf_solve, pf_batch_n1, pf_batch_ts, pf_batch_device and the
+   scratch entry points run it; pf_get_J and pf_multi_create reject it.  A singular B' or B''
+   fails here with SolverFactor. */
+int pf_fdpf_plan_create(int n, const int *colptr, const int *rowind, const double *ybus_ri, const int *bp_colptr,
+                        const int *bp_rowind, const double *bp_x, const int *bpp_colptr, const int *bpp_rowind,
+                        const double *bpp_x, const int *slack_ids, int nslack, const double *slack_weights,
+                        const int *pv, int npv, const int *pq, int npq, const pf_options *opts, pf_plan **plan);
+
 /* Sizes and schedule statistics of a plan. */
 typedef struct pf_plan_info {
     int n, m, nnz_ybus, nnz_j, nnz_lu;

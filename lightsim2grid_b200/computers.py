@@ -17,7 +17,7 @@ import time
 
 import numpy as np
 
-from .solver import SolverType, GPU_SOLVERS, Plan, solver_flags
+from .solver import SolverType, GPU_SOLVERS, FDPF_SOLVERS, Plan, solver_flags
 
 
 class _BatchBase:
@@ -113,7 +113,11 @@ class _BatchBase:
         distributed, precision = solver_flags(self._solver_type)
         V0 = Vinit.copy()
         V0[g.gen_bus] = np.abs(g.gen_vm_pu) * np.exp(1j * np.angle(V0[g.gen_bus]))
-        self._plan = Plan(Y, V0, S, sl, w, pv, pq, distributed=distributed, precision=precision,
+        fdpf = None
+        if self._solver_type in FDPF_SOLVERS:
+            # fast decoupled: B' and B'' of the base grid, kept for every case and step
+            fdpf = g.get_Bp_Bpp(FDPF_SOLVERS[self._solver_type])
+        self._plan = Plan(Y, V0, S, sl, w, pv, pq, distributed=distributed, precision=precision, fdpf=fdpf,
                           **self._plan_options)
         Vn, conv, it, err = self._plan.solve(V0, S, max_iter, tol)
         Vstart = Vn if (self.init_from_n_powerflow and conv) else V0

@@ -73,6 +73,9 @@ struct pf_plan {
     void *d_int = nullptr;
     void *d_dbl = nullptr;
     l2g::DevPlan dp{};
+    // fast-decoupled plans: the B' and B'' systems
+    l2g::DevPlan dsub[2]{};
+    void *d_sub_int[2] = {nullptr, nullptr}, *d_sub_dbl[2] = {nullptr, nullptr};
     // device work buffers
     DevBuf scratch, counter, V0, Sbus, optr, opos, oval, jfirst, jcount, Vout, iters, errs, Jout, cycles, Vcase,
         casemap;
@@ -264,8 +267,10 @@ std::vector<int> pack_pairs(const std::vector<int> &a, const std::vector<int> &b
     return out;
 }
 
-int upload(pf_plan *pl) {
-    const l2g::Plan &P = pl->P;
+// Uploads the structure arrays of one plan (and, for a fast-decoupled system, its factor
+// values) into two device blobs and points the fields of `d` into them.
+int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl, const std::vector<double> *luval,
+                int lu_offset = -1, bool compact_ok = true) {
     std::vector<unsigned char> bi, bd;
     size_t oRp = push(bi, P.Rp), oRj = push(bi, P.Rj), oRrow = push(bi, P.Rrow);
     size_t oyt = push(bi, P.ytarget), oyj = push(bi, P.yjpos);
@@ -275,12 +280,12 @@ int upload(pf_plan *pl) {
     size_t obo = push(bi, P.backward.ops), obb = push(bi, P.backward.base), obw = push(bi, P.backward.width);
     size_t owo = push(bi, P.forward.ops), owb = push(bi, P.forward.base), oww = push(bi, P.forward.width);
     // packed operations for the shared-memory LU layout (always fit when the LU does)
-    const bool compact = l2g::compact_fits(P);
+    const bool compact = lu_offset >= 0 ? compact_ok : l2g::compact_fits(P);
     std::vector<unsigned> cf, cb, cw;
     if (compact) {
-        l2g::compact_ops(P.factor, P.m, cf);
-        l2g::compact_ops(P.backward, P.m, cb);
-        l2g::compact_ops(P.forward, P.m, cw);
+        l2g::compact_ops(P.factor, P.m, cf, lu_offset);
+        l2g::compact_ops(P.backward, P.m, cb, lu_offset);
+        l2g::compact_ops(P.forward, P.m, cw, lu_offset);
     }
     size_t ocf = push(bi, cf), ocb = push(bi, cb), ocw = push(bi, cw);
     size_t odpos = push(bi, P.dpos);
@@ -298,22 +303,23 @@ int upload(pf_plan *pl) {
             else if (std::fabs(P.weights[r]) > 1e-7) wJ[r] = P.weights[r];
         }
     size_t oRx = push(bd, rx), ow = push(bd, P.weights), ocv = push(bd, P.cval), owJ = push(bd, wJ);
-    if (pl->d_int) cudaFree(pl->d_int);
-    if (pl->d_dbl) cudaFree(pl->d_dbl);
-    pl->d_int = pl->d_dbl = nullptr;
-    cudaError_t e = cudaMalloc(&pl->d_int, std::max<size_t>(bi.size(), 16));
+    size_t olu = push(bd, luval ? *luval : std::vector<double>());
+    if (d_int) cudaFree(d_int);
+    if (d_dbl) cudaFree(d_dbl);
+    d_int = d_dbl = nullptr;
+    cudaError_t e = cudaMalloc(&d_int, std::max<size_t>(bi.size(), 16));
     if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: cudaMalloc");
-    e = cudaMalloc(&pl->d_dbl, std::max<size_t>(bd.size(), 16));
+    e = cudaMalloc(&d_dbl, std::max<size_t>(bd.size(), 16));
     if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: cudaMalloc");
-    e = cudaMemcpy(pl->d_int, bi.data(), bi.size(), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: upload");
-    e = cudaMemcpy(pl->d_dbl, bd.data(), bd.size(), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: upload");
-    unsigned char *bI = static_cast<unsigned char *>(pl->d_int), *bD = static_cast<unsigned char *>(pl->d_dbl);
+    if (!bi.empty() && (e = cudaMemcpy(d_int, bi.data(), bi.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_fail(e, "pf_plan_create: upload");
+    if (!bd.empty() && (e = cudaMemcpy(d_dbl, bd.data(), bd.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_fail(e, "pf_plan_create: upload");
+    unsigned char *bI = static_cast<unsigned char *>(d_int), *bD = static_cast<unsigned char *>(d_dbl);
     auto I = [&](size_t o) { return reinterpret_cast<const int *>(bI + o); };
     auto I4 = [&](size_t o) { return reinterpret_cast<const int4 *>(bI + o); };
     auto D = [&](size_t o) { return reinterpret_cast<const double *>(bD + o); };
-    l2g::DevPlan &d = pl->dp;
+    d = l2g::DevPlan{};
     d.n = P.n;
     d.m = P.m;
     d.nnzY = P.nnzY;
@@ -345,7 +351,7 @@ int upload(pf_plan *pl) {
     d.fwd_width = I(oww);
     auto U2 = [&](size_t o) { return reinterpret_cast<const uint2 *>(bI + o); };
     d.compact = compact ? 1 : 0;
-    d.lu_offset = l2g::compact_lu_offset(P.m);
+    d.lu_offset = lu_offset >= 0 ? lu_offset : l2g::compact_lu_offset(P.m);
     d.fac_cops = compact ? U2(ocf) : nullptr;
     d.bwd_cops = compact ? U2(ocb) : nullptr;
     d.fwd_cops = compact ? U2(ocw) : nullptr;
@@ -359,6 +365,21 @@ int upload(pf_plan *pl) {
     d.dpos = I(odpos);
     d.dc = P.dc ? 1 : 0;
     d.slack0 = P.slack0;
+    d.luval = luval ? D(olu) : nullptr;
+    return 0;
+}
+
+int upload(pf_plan *pl) {
+    int rc = upload_plan(pl->P, pl->dp, pl->d_int, pl->d_dbl, nullptr);
+    if (rc || !pl->P.fdpf) return rc;
+    int off[2];
+    bool fits = false;
+    l2g::fdpf_lu_offsets(pl->P, off[0], off[1], fits);
+    for (int k = 0; k < 2; ++k) {
+        rc = upload_plan(pl->P.sub[k], pl->dsub[k], pl->d_sub_int[k], pl->d_sub_dbl[k], &pl->P.sublu[k], off[k],
+                         fits);
+        if (rc) return rc;
+    }
     return 0;
 }
 
@@ -381,6 +402,32 @@ int configure(pf_plan *pl) {
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, pl->device);
     pl->precision = pl->opt.precision ? 1 : 0;
     const int thr = pl->threads;
+    if (P.fdpf) {
+        // FP64; both factors in every CTA's shared memory when they fit
+        pl->precision = 0;
+        pl->refine = false;
+        const size_t static_smem = 4096;  // Shared struct and the three staged plans
+        const size_t sm_in = l2g::fdpf_smem_bytes(pl->dsub[0], pl->dsub[1], true);
+        const size_t sm_out = l2g::fdpf_smem_bytes(pl->dsub[0], pl->dsub[1], false);
+        const bool fits = pl->dsub[0].compact && pl->dsub[1].compact && sm_in + static_smem <= (size_t)optin;
+        if (pl->opt.lu_placement == 1 && !fits) return fail(-1, "pf_plan_create: the factors do not fit in shared memory");
+        if (sm_out + static_smem > (size_t)optin)
+            return fail(-1, "pf_plan_create: the solve vectors do not fit in shared memory");
+        pl->lu_in_smem = pl->opt.lu_placement == 2 ? false : fits;
+        pl->smem = pl->lu_in_smem ? sm_in : sm_out;
+        pl->slab = l2g::fdpf_slab_bytes(pl->dp);
+        const int want = pl->opt.max_ctas_per_sm;
+        int occ = l2g::fdpf_occupancy(pl->lu_in_smem, thr, want > 0 ? want : 8, pl->smem);
+        if (occ <= 0) return fail(-1, "pf_plan_create: the kernel cannot be launched with this configuration");
+        if (want > 0) occ = std::min(occ, want);
+        pl->ctas_per_sm = occ;
+        pl->grid = pl->num_sms * occ;
+        e = pl->scratch.ensure(pl->slab * (size_t)pl->grid);
+        if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: scratch allocation");
+        e = pl->counter.ensure(256);
+        if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: counter allocation");
+        return 0;
+    }
     const int lub = pl->precision ? 4 : 8, xb = pl->precision ? 4 : 8;
     const size_t static_smem = 2048;  // Shared struct of the kernel, rounded up
     size_t sm_in = l2g::smem_bytes(pl->dp, lub, xb, true);
@@ -413,6 +460,11 @@ void release(pf_plan *pl) {
     if (pl->d_int) cudaFree(pl->d_int);
     if (pl->d_dbl) cudaFree(pl->d_dbl);
     pl->d_int = pl->d_dbl = nullptr;
+    for (int k = 0; k < 2; ++k) {
+        if (pl->d_sub_int[k]) cudaFree(pl->d_sub_int[k]);
+        if (pl->d_sub_dbl[k]) cudaFree(pl->d_sub_dbl[k]);
+        pl->d_sub_int[k] = pl->d_sub_dbl[k] = nullptr;
+    }
     if (pl->ev0) cudaEventDestroy(pl->ev0);
     if (pl->ev1) cudaEventDestroy(pl->ev1);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -438,6 +490,12 @@ int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, u
     if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
     int grid = std::min(pl->grid, a.njobs);
     grid = std::min<long long>(grid, (long long)(scratch_bytes / pl->slab));
+    if (pl->P.fdpf) {
+        e = l2g::launch_fdpf_batch(pl->dp, pl->dsub[0], pl->dsub[1], a, pl->threads, pl->ctas_per_sm, grid,
+                                   pl->smem, st);
+        if (e != cudaSuccess) return cuda_fail(e, "launch: kernel");
+        return 0;
+    }
     // the FP64 re-run of a mixed plan uses the FP64 kernel with this plan's layout:
     // LU bytes differ, so recompute shared memory and slab use for that precision
     size_t smem = pl->smem;
@@ -741,6 +799,60 @@ int pf_dc_plan_create(int n, const int *colptr, const int *rowind, const double 
     return finish_plan(pl, out);
 }
 
+int pf_fdpf_plan_create(int n, const int *colptr, const int *rowind, const double *ybus_ri, const int *bp_colptr,
+                        const int *bp_rowind, const double *bp_x, const int *bpp_colptr, const int *bpp_rowind,
+                        const double *bpp_x, const int *slack_ids, int nslack, const double *slack_weights,
+                        const int *pv, int npv, const int *pq, int npq, const pf_options *opts, pf_plan **out) {
+    if (!out || !colptr || !rowind || !ybus_ri || !bp_colptr || !bp_rowind || !bp_x || !bpp_colptr || !bpp_rowind ||
+        !bpp_x || !slack_ids || !slack_weights || (npv && !pv) || (npq && !pq))
+        return fail(-1, "pf_fdpf_plan_create: null argument");
+    *out = nullptr;
+    pf_plan *pl = new pf_plan();
+    if (opts) pl->opt = *opts;
+    pl->opt.precision = 0;  // the reference's fast-decoupled solves are FP64
+    l2g::PlanOptions po;
+    if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
+    int thr = pl->opt.threads;
+    if (thr <= 0) {
+        // factors in global memory, read through L1 by every CTA of an SM, and several small
+        // CTAs per SM to overlap the latency of the substitution phases: up to 8 while the solve
+        // vectors stay within about 100 KB of shared memory per SM, else 4 CTAs of 128 threads,
+        // or 2 of 256 for systems above 4000 unknowns (measured on 118- to 6515-bus grids)
+        if (pl->opt.lu_placement == 1) {
+            thr = 512;
+        } else {
+            const long long m_max = std::max<long long>(npv + nslack - 1 + npq, npq);
+            const long long per = (m_max + 1) * 8 + 4096;
+            int ctas = (int)std::min<long long>(8, (100 << 10) / per);
+            thr = 128;
+            if (ctas < 4) {
+                ctas = m_max <= 4000 ? 4 : 2;
+                thr = m_max <= 4000 ? 128 : 256;
+            }
+            if (pl->opt.max_ctas_per_sm <= 0) pl->opt.max_ctas_per_sm = ctas;
+            if (pl->opt.lu_placement == 0) pl->opt.lu_placement = 2;
+        }
+    }
+    thr = std::max(32, std::min(512, (thr / 32) * 32));
+    po.threads = pl->threads = thr;
+    po.fuse_forward = true;
+    std::string msg;
+    int rc;
+    try {
+        rc = l2g::build_fdpf_plan(pl->P, n, colptr, rowind, reinterpret_cast<const cplx *>(ybus_ri),
+                                  l2g::RealCsc{bp_colptr, bp_rowind, bp_x}, l2g::RealCsc{bpp_colptr, bpp_rowind, bpp_x},
+                                  slack_ids, nslack, slack_weights, pv, npv, pq, npq, po, msg);
+    } catch (const std::exception &ex) {
+        rc = -1;
+        msg = std::string("pf_fdpf_plan_create: ") + ex.what();
+    }
+    if (rc != 0) {
+        delete pl;
+        return fail(rc, msg);
+    }
+    return finish_plan(pl, out);
+}
+
 void pf_plan_destroy(pf_plan *plan) {
     if (!plan) return;
     release(plan);
@@ -762,6 +874,17 @@ int pf_plan_info_get(const pf_plan *pl, pf_plan_info *info) {
     info->groups_forward = P.forward.nphases();
     info->groups_backward = P.backward.nphases();
     info->flops_refactor = P.flops_refactor;
+    if (P.fdpf) {
+        // the two decoupled systems together (nothing is refactorised)
+        info->nnz_j = (int)(P.sub[0].Ji.size() + P.sub[1].Ji.size());
+        info->nnz_lu = P.sub[0].nnzLU + P.sub[1].nnzLU;
+        info->levels_refactor = info->groups_refactor = 0;
+        info->levels_forward = P.sub[0].levels_fwd + P.sub[1].levels_fwd;
+        info->levels_backward = P.sub[0].levels_bwd + P.sub[1].levels_bwd;
+        info->groups_forward = P.sub[0].forward.nphases() + P.sub[1].forward.nphases();
+        info->groups_backward = P.sub[0].backward.nphases() + P.sub[1].backward.nphases();
+        info->flops_refactor = 0;
+    }
     info->precision = pl->precision;
     info->threads = pl->threads;
     info->lu_in_shared = pl->lu_in_smem ? 1 : 0;
@@ -815,6 +938,7 @@ int pf_solve(pf_plan *pl, const double *V0_ri, const double *Sbus_ri, int max_it
 int pf_get_J(pf_plan *pl, int *m, int *Jp, int *Ji, double *Jx) {
     if (!pl) return fail(-1, "pf_get_J: null argument");
     if (pl->P.dc) return fail(-1, "pf_get_J: a DC plan has no Jacobian");
+    if (pl->P.fdpf) return fail(-1, "pf_get_J: a fast-decoupled plan has no Jacobian");
     const l2g::Plan &P = pl->P;
     if (m) *m = P.m;
     if (Jp) std::memcpy(Jp, P.Jp.data(), P.Jp.size() * sizeof(int));
@@ -1212,9 +1336,9 @@ int pf_multi_create(pf_plan *const *plans, const pf_device_batch *batches, int n
             delete mp;
             return fail(-1, "pf_multi_create: plans differ in device, precision, refinement or LU placement");
         }
-        if (pl->P.dc) {
+        if (pl->P.dc || pl->P.fdpf) {
             delete mp;
-            return fail(-1, "pf_multi_create: DC plans run one plan per launch");
+            return fail(-1, "pf_multi_create: DC and fast-decoupled plans run one plan per launch");
         }
         mp->plans.push_back(pl);
         mp->threads = std::max(mp->threads, pl->threads);

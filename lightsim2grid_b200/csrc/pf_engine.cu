@@ -115,6 +115,31 @@ __device__ __forceinline__ void dsbus(double2 y, double2 vr, double2 vc, bool di
     dvm = a;
 }
 
+// (Ybus V)[r], over the row's entries in column order
+__device__ __forceinline__ double2 ybus_row_product(const DevPlan &P, const Shared &S, const double2 *__restrict__ V,
+                                                    int r) {
+    double2 s = make_double2(0.0, 0.0);
+    const int p0 = P.Rp[r], p1 = P.Rp[r + 1];
+    for (int p = p0; p < p1; p += 4) {
+        // indices first, then values: the loads of four entries are in flight together
+        int c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) c[u] = p + u < p1 ? P.Rj[p + u] : -1;
+        double2 y[4], vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            y[u] = c[u] >= 0 ? ybus_value(P, S, p + u) : make_double2(0.0, 0.0);
+            vv[u] = c[u] >= 0 ? V[c[u]] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            s.x += y[u].x * vv[u].x - y[u].y * vv[u].y;
+            s.y += y[u].x * vv[u].y + y[u].y * vv[u].x;
+        }
+    }
+    return s;
+}
+
 // F at V: writes Ibus, the FP64 mismatch per bus and the permuted right-hand side x;
 // returns ||F||_inf and a non-finite flag to every thread.
 template <typename XT>
@@ -125,25 +150,7 @@ __device__ void mismatch(const DevPlan &P, Shared &S, const double2 *__restrict_
     int lbad = 0;
     const double sa = S.slack_absorbed;
     for (int r = threadIdx.x; r < P.n; r += blockDim.x) {
-        double2 s = make_double2(0.0, 0.0);
-        const int p0 = P.Rp[r], p1 = P.Rp[r + 1];
-        for (int p = p0; p < p1; p += 4) {
-            // indices first, then values: the loads of four entries are in flight together
-            int c[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) c[u] = p + u < p1 ? P.Rj[p + u] : -1;
-            double2 y[4], vv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                y[u] = c[u] >= 0 ? ybus_value(P, S, p + u) : make_double2(0.0, 0.0);
-                vv[u] = c[u] >= 0 ? V[c[u]] : make_double2(0.0, 0.0);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                s.x += y[u].x * vv[u].x - y[u].y * vv[u].y;
-                s.y += y[u].x * vv[u].y + y[u].y * vv[u].x;
-            }
-        }
+        const double2 s = ybus_row_product(P, S, V, r);
         Ibus[r] = s;
         const double2 vr = V[r];
         const double2 sb = Sbus[r];
@@ -777,6 +784,258 @@ __global__ void __launch_bounds__(512, 1) dc_batch_kernel(const DevPlan P, const
     }
 }
 
+// Fast decoupled power flow of a batch (BaseFDPFAlgo::compute_pf, src/powerflow_algorithm/
+// BaseFDPFAlgo.tpp:11-173, with has_converged, BaseFDPFAlgo.hpp:118-170), FP64, one CTA per
+// instance.  B' (over pvpq) and B'' (over pq) were factorised when the plan was built and do
+// not change between instances (the reference's batch computers keep the base factors for
+// every contingency and step); each CTA copies both factors into its shared memory once when
+// they fit, else reads them from global memory (one copy, L2 resident).  An iteration:
+//   P half-step  dVa = B'^-1 P, Va[pvpq] -= dVa, t = exp(j Va), V = Vm t, (Vm, Va) = (|V|, arg V)
+//   Q half-step  dVm = B''^-1 Q, Vm[pq] -= dVm, V = Vm t, (Vm, Va) = (|V|, arg V)
+// each followed by the mismatch  mis = (V conj(Ybus V) - Sbus + slack_absorbed w) / Vm,
+// P = Re(mis)[pvpq], Q = Im(mis)[pq], converged when max(|P|, |Q|) < tol, InifiniteValue when
+// any bus's mis is not finite; slack_absorbed = Re(sum Sbus), the reference's start value,
+// which its FDPF never updates.
+// Only one of P and Q is needed at a time (P before a B' solve, Q before a B'' solve), so the
+// two systems share one solve vector; with the factors in shared memory the index space is
+// x | LU(B') | LU(B''), each system's packed operations addressing its LU at its lu_offset.
+struct FdpfLayout {
+    double *x[2];         // the shared solve vector (both entries equal)
+    const double *lu[2];  // factor values (shared or global)
+    int *sbf[2], *swf[2], *sbb[2], *swb[2];
+    double2 *V, *T;       // voltages, exp(j Va) of the last P half-step
+    double *Vm, *Va;
+};
+
+__host__ __device__ __forceinline__ size_t fdpf_region_bytes(const DevPlan &B0, const DevPlan &B1, bool lu_in_smem) {
+    const size_t e0 = lu_in_smem ? (size_t)B0.lu_offset + (size_t)B0.nnzLU : (size_t)B0.m + 1;
+    const size_t e1 = lu_in_smem ? (size_t)B1.lu_offset + (size_t)B1.nnzLU : (size_t)B1.m + 1;
+    const size_t e = e0 > e1 ? e0 : e1;
+    return (e * sizeof(double) + 15) & ~(size_t)15;
+}
+
+// B: the two systems' plans (in shared memory)
+template <bool LU_SMEM>
+__device__ __forceinline__ FdpfLayout fdpf_layout(const DevPlan &P, const DevPlan *B, const BatchArgs &A,
+                                                  unsigned char *dyn) {
+    FdpfLayout L;
+    double *x = reinterpret_cast<double *>(dyn);
+    for (int k = 0; k < 2; ++k) {
+        L.x[k] = x;
+        L.lu[k] = LU_SMEM ? x + B[k].lu_offset : B[k].luval;
+    }
+    int *t = reinterpret_cast<int *>(dyn + fdpf_region_bytes(B[0], B[1], LU_SMEM));
+    for (int k = 0; k < 2; ++k) {
+        L.sbf[k] = t;
+        t += B[k].fwd_nph + 1;
+        L.sbb[k] = t;
+        t += B[k].bwd_nph + 1;
+        L.swf[k] = t;
+        t += B[k].fwd_nph;
+        L.swb[k] = t;
+        t += B[k].bwd_nph;
+    }
+    unsigned char *slab = A.scratch + (size_t)blockIdx.x * (size_t)A.slab_bytes;
+    L.V = reinterpret_cast<double2 *>(slab);
+    L.T = L.V + P.n;
+    L.Vm = reinterpret_cast<double *>(L.T + P.n);
+    L.Va = L.Vm + P.n;
+    return L;
+}
+
+// B x = b for one decoupled system: forward and backward programs over the constant factors,
+// then the division by the pivots (the backward program keeps z undivided).
+template <bool LU_SMEM>
+__device__ __forceinline__ void fdpf_solve(const DevPlan &B, const FdpfLayout &L, int k, Trace &tr) {
+    double *x = L.x[k];
+    double *lu = const_cast<double *>(L.lu[k]);  // read only: substitutions do not write the LU
+    run_lu_program<double, double, LU_SMEM>(B.fwd_cops, B.fwd_ops, L.sbf[k], L.swf[k], B.fwd_nph, B.m, lu, x, tr);
+    run_lu_program<double, double, LU_SMEM>(B.bwd_cops, B.bwd_ops, L.sbb[k], L.swb[k], B.bwd_nph, B.m, lu, x, tr);
+    for (int i = threadIdx.x; i < B.m; i += blockDim.x) x[i] = x[i] / lu[B.dpos[i]];
+    __syncthreads();
+}
+
+// mis = (V conj(Ybus V) - Sbus + slack_absorbed w) / Vm: P into x at xP (which 0, for the next
+// B' solve) or Q into x at xQ (which 1, for the next B'' solve); returns max(|P|, |Q|) and "some
+// bus's mis is not finite" to every thread.
+__device__ void fdpf_mismatch(const DevPlan &P, Shared &S, const double2 *__restrict__ V,
+                              const double *__restrict__ Vm, const double2 *__restrict__ Sbus, double *x, int which,
+                              double &norm, int &bad) {
+    double lmax = 0.0;
+    int lbad = 0;
+    const double sa = S.slack_absorbed;
+    for (int r = threadIdx.x; r < P.n; r += blockDim.x) {
+        const double2 s = ybus_row_product(P, S, V, r);
+        const double2 vr = V[r];
+        const double2 sb = Sbus[r];
+        double mr = vr.x * s.x + vr.y * s.y - sb.x;  // V * conj(I) - S + slack_absorbed * w
+        double mi = vr.y * s.x - vr.x * s.y - sb.y;
+        mr += sa * P.w[r];
+        const double vm = Vm[r];
+        mr /= vm;
+        mi /= vm;
+        lbad |= !isfinite(mr) || !isfinite(mi);
+        const int ip = P.xP[r], iq = P.xQ[r];
+        if (ip >= 0) {
+            if (which == 0) x[ip] = mr;
+            lmax = fmax(lmax, fabs(mr));
+        }
+        if (iq >= 0) {
+            if (which == 1) x[iq] = mi;
+            lmax = fmax(lmax, fabs(mi));
+        }
+    }
+    block_norm(S, lmax, lbad, norm, bad);
+}
+
+// MAXT / MINB: launch bounds.  With the factors in global memory (read by every CTA of an SM
+// through L1) small CTAs, many per SM, hide the latency of the substitution phases.
+template <bool LU_SMEM, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) fdpf_batch_kernel(const DevPlan P0, const DevPlan B0, const DevPlan B1,
+                                                                const BatchArgs A) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ Shared S;
+    // the three plans in shared memory: indexed by system without copies of kernel parameters
+    __shared__ __align__(16) DevPlan sp[3];
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        sp[0] = P0;
+        sp[1] = B0;
+        sp[2] = B1;
+    }
+    __syncthreads();
+    const DevPlan &P = sp[0];
+    const DevPlan *B = sp + 1;
+    const int n = P.n;
+    const FdpfLayout L = fdpf_layout<LU_SMEM>(P, B, A, dyn);
+    {
+        for (int k = 0; k < 2; ++k) {
+            const DevPlan &b = B[k];
+            for (int i = tid; i <= b.fwd_nph; i += blockDim.x) L.sbf[k][i] = b.fwd_base[i];
+            for (int i = tid; i <= b.bwd_nph; i += blockDim.x) L.sbb[k][i] = b.bwd_base[i];
+            for (int i = tid; i < b.fwd_nph; i += blockDim.x) L.swf[k][i] = b.fwd_width[i];
+            for (int i = tid; i < b.bwd_nph; i += blockDim.x) L.swb[k][i] = b.bwd_width[i];
+            if (LU_SMEM)
+                for (int i = tid; i < b.nnzLU; i += blockDim.x) L.x[k][b.lu_offset + i] = b.luval[i];
+        }
+    }
+    __syncthreads();
+    double2 *V = L.V, *T = L.T;
+    double *Vm = L.Vm, *Va = L.Va;
+    Trace tr{nullptr, 0, 0};
+    for (;;) {
+        if (tid == 0) S.job = atomicAdd(A.job_counter, 1);
+        __syncthreads();
+        const int job = S.job;
+        __syncthreads();
+        if (job >= A.njobs) break;
+        const int first = A.job_first[job], count = A.job_count[job];
+        for (int step = 0; step < count; ++step) {
+            const int inst = first + step;
+            const double2 *Sb = A.Sbus + (long long)inst * A.sbus_stride;
+            if (step == 0 || !A.chain) {
+                const double2 *v0 = A.V0 + (long long)inst * A.v0_stride;
+                for (int b = tid; b < n; b += blockDim.x) V[b] = v0[b];
+            }
+            for (int b = tid; b < n; b += blockDim.x) {
+                const double2 v = V[b];
+                Vm[b] = cabs2(v);
+                Va[b] = atan2(v.y, v.x);
+            }
+            if (tid == 0) {
+                int k0 = 0, k1 = 0;
+                if (A.ovr_ptr) {
+                    k0 = A.ovr_ptr[inst];
+                    k1 = A.ovr_ptr[inst + 1];
+                }
+                S.novr = min(k1 - k0, kMaxOverrides);
+            }
+            __syncthreads();
+            if (tid < S.novr) {
+                const int k0 = A.ovr_ptr[inst];
+                S.opos[tid] = A.ovr_pos[k0 + tid];
+                S.oval[tid] = A.ovr_val[k0 + tid];
+            }
+            double ls = 0.0;
+            for (int b = tid; b < n; b += blockDim.x) ls += Sb[b].x;
+            const double tot = block_sum(S, ls);  // contains barriers
+            if (tid == 0) S.slack_absorbed = tot;
+            __syncthreads();
+            double norm;
+            int bad;
+            fdpf_mismatch(P, S, V, Vm, Sb, L.x[0], 0, norm, bad);
+            bool conv = !bad && norm < A.tol;
+            int it = 0, err = 0;
+            while (!conv && it < A.max_iter) {
+                ++it;
+                // P half-step
+                fdpf_solve<LU_SMEM>(B[0], L, 0, tr);
+                for (int b = tid; b < n; b += blockDim.x) {
+                    double va = Va[b];
+                    const int ia = P.xVa[b];
+                    if (ia >= 0) va -= L.x[0][ia];
+                    double sn, cs;
+                    sincos(va, &sn, &cs);
+                    T[b] = make_double2(cs, sn);
+                    const double vm = Vm[b];
+                    const double2 v = make_double2(vm * cs, vm * sn);
+                    V[b] = v;
+                    Vm[b] = cabs2(v);
+                    Va[b] = atan2(v.y, v.x);
+                }
+                __syncthreads();
+                fdpf_mismatch(P, S, V, Vm, Sb, L.x[0], 1, norm, bad);
+                if (bad) {
+                    err = 3;  // InifiniteValue
+                    break;
+                }
+                if (norm < A.tol) {
+                    conv = true;
+                    break;
+                }
+                // Q half-step
+                fdpf_solve<LU_SMEM>(B[1], L, 1, tr);
+                for (int b = tid; b < n; b += blockDim.x) {
+                    double vm = Vm[b];
+                    const int im = P.xVm[b];
+                    if (im >= 0) vm -= L.x[1][im];
+                    const double2 t = T[b];
+                    const double2 v = make_double2(vm * t.x, vm * t.y);
+                    V[b] = v;
+                    Vm[b] = cabs2(v);
+                    Va[b] = atan2(v.y, v.x);
+                }
+                __syncthreads();
+                fdpf_mismatch(P, S, V, Vm, Sb, L.x[0], 0, norm, bad);
+                if (bad) {
+                    // the reference notices the error after the next iteration's B' solve
+                    err = 3;
+                    if (it < A.max_iter) ++it;
+                    break;
+                }
+                conv = norm < A.tol;
+            }
+            if (!conv && err == 0) err = 2;  // TooManyIterations
+            double2 *vo = A.Vout + (long long)inst * n;
+            for (int b = tid; b < n; b += blockDim.x) vo[b] = V[b];
+            if (tid == 0) {
+                A.iters[inst] = it;
+                A.errs[inst] = err;
+            }
+            __syncthreads();
+            if (A.chain && err != 0) {
+                // the reference stops a time series at its first divergence
+                for (int s2 = step + 1 + tid; s2 < count; s2 += blockDim.x) {
+                    A.iters[first + s2] = 0;
+                    A.errs[first + s2] = 8;  // NotInitError: not computed
+                }
+                break;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 template <typename LT, typename XT, bool SM, bool RF>
 cudaError_t launch_variant(const DevPlan &P, const BatchArgs &A, const MultiArgs &M, int threads, int grid,
                            size_t smem, cudaStream_t st) {
@@ -838,6 +1097,50 @@ cudaError_t launch_dc_variant(const DevPlan &P, const BatchArgs &A, int threads,
     if (e != cudaSuccess) return e;
     dc_batch_kernel<SM><<<grid, threads, smem, st>>>(P, A);
     return cudaGetLastError();
+}
+
+template <bool SM, int MAXT, int MINB>
+cudaError_t launch_fdpf_variant(const DevPlan &P, const DevPlan &B0, const DevPlan &B1, const BatchArgs &A,
+                                int threads, int grid, size_t smem, cudaStream_t st) {
+    cudaError_t e = allow_max_smem(reinterpret_cast<const void *>(fdpf_batch_kernel<SM, MAXT, MINB>));
+    if (e != cudaSuccess) return e;
+    fdpf_batch_kernel<SM, MAXT, MINB><<<grid, threads, smem, st>>>(P, B0, B1, A);
+    return cudaGetLastError();
+}
+
+// the kernel variant of a configuration: factors in shared memory (512 threads, 1 CTA per SM),
+// or in global memory with 128-thread CTAs, 4 (registers unconstrained) or 8 (64 registers) per
+// SM, or wider CTAs
+const void *fdpf_kernel(bool lu_in_smem, int threads, int ctas_per_sm) {
+    if (lu_in_smem) return reinterpret_cast<const void *>(fdpf_batch_kernel<true, 512, 1>);
+    if (threads <= 128 && ctas_per_sm > 4) return reinterpret_cast<const void *>(fdpf_batch_kernel<false, 128, 8>);
+    if (threads <= 128) return reinterpret_cast<const void *>(fdpf_batch_kernel<false, 128, 4>);
+    return reinterpret_cast<const void *>(fdpf_batch_kernel<false, 512, 1>);
+}
+
+cudaError_t launch_fdpf_batch(const DevPlan &P, const DevPlan &B0, const DevPlan &B1, const BatchArgs &A,
+                              int threads, int ctas_per_sm, int grid, size_t smem, cudaStream_t stream) {
+    if (A.lu_in_smem) return launch_fdpf_variant<true, 512, 1>(P, B0, B1, A, threads, grid, smem, stream);
+    if (threads <= 128 && ctas_per_sm > 4)
+        return launch_fdpf_variant<false, 128, 8>(P, B0, B1, A, threads, grid, smem, stream);
+    if (threads <= 128) return launch_fdpf_variant<false, 128, 4>(P, B0, B1, A, threads, grid, smem, stream);
+    return launch_fdpf_variant<false, 512, 1>(P, B0, B1, A, threads, grid, smem, stream);
+}
+
+size_t fdpf_smem_bytes(const DevPlan &B0, const DevPlan &B1, bool lu_in_smem) {
+    size_t b = fdpf_region_bytes(B0, B1, lu_in_smem);
+    for (const DevPlan *B : {&B0, &B1}) b += (size_t)(2 * (B->fwd_nph + B->bwd_nph) + 2) * sizeof(int);
+    return (b + 15) & ~(size_t)15;
+}
+
+size_t fdpf_slab_bytes(const DevPlan &P) { return ((size_t)P.n * 48 + 255) & ~(size_t)255; }
+
+int fdpf_occupancy(bool lu_in_smem, int threads, int ctas_per_sm, size_t smem) {
+    const void *fn = fdpf_kernel(lu_in_smem, threads, ctas_per_sm);
+    int nb = 0;
+    if (allow_max_smem(fn) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess) return 0;
+    return nb;
 }
 
 cudaError_t launch_nr_batch(const DevPlan &P, const BatchArgs &A, int precision, int threads, int grid,

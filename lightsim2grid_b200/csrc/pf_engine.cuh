@@ -35,6 +35,7 @@ struct DevPlan {
     const uint2 *fac_cops, *bwd_cops, *fwd_cops;
     const int *dpos;         // pivot position per column (m)
     int dc, slack0;          // DC plan (B = Re(Ybus) without the slack) and its slack bus
+    const double *luval;     // constant factor values (LU layout) of a fast-decoupled system
 };
 
 // One batch launch.
@@ -108,5 +109,17 @@ cudaError_t launch_scatter_case_rows(const double2 *src, const int *errs, const 
                                      double2 *dst, int num_sms, cudaStream_t st);
 // Resident CTAs per SM for a configuration (0 if it cannot launch).
 int nr_occupancy(int precision, bool lu_in_smem, bool refine, int threads, size_t smem);
+
+// Fast decoupled power flow of a batch: P carries the Ybus rows, slack weights and bus maps,
+// B0 / B1 the substitution programs and constant factors of B' and B''.  lu_in_smem: both
+// factors are copied into every CTA's shared memory (else read from global memory).
+// ctas_per_sm: the residency the launch was configured for (selects the register budget of
+// the 128-thread variants: up to 4 per SM unconstrained, more with 64 registers).
+cudaError_t launch_fdpf_batch(const DevPlan &P, const DevPlan &B0, const DevPlan &B1, const BatchArgs &A,
+                              int threads, int ctas_per_sm, int grid, size_t smem, cudaStream_t stream);
+size_t fdpf_smem_bytes(const DevPlan &B0, const DevPlan &B1, bool lu_in_smem);
+size_t fdpf_slab_bytes(const DevPlan &P);
+// resident CTAs per SM of the variant chosen for (lu_in_smem, threads, wanted ctas_per_sm; 0: most)
+int fdpf_occupancy(bool lu_in_smem, int threads, int ctas_per_sm, size_t smem);
 
 }  // namespace l2g

@@ -161,8 +161,8 @@ int compact_lu_offset(int m) { return (m + 1 + 3) & ~3; }
 
 bool compact_fits(const Plan &P) { return (long long)compact_lu_offset(P.m) + P.nnzLU <= 65536; }
 
-void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out) {
-    const unsigned L = (unsigned)compact_lu_offset(m), dummy = (unsigned)m;
+void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out, int lu_offset) {
+    const unsigned L = (unsigned)(lu_offset >= 0 ? lu_offset : compact_lu_offset(m)), dummy = (unsigned)m;
     const int n = pr.nops();
     out.resize(2 * (size_t)n);
     for (int o = 0; o < n; ++o) {
@@ -177,6 +177,13 @@ void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out) {
         out[2 * (size_t)o] = X | (Y << 16);
         out[2 * (size_t)o + 1] = Z | (W << 16);
     }
+}
+
+void fdpf_lu_offsets(const Plan &P, int &off0, int &off1, bool &fits) {
+    const int x = std::max(compact_lu_offset(P.sub[0].m), compact_lu_offset(P.sub[1].m));
+    off0 = x;
+    off1 = x + ((P.sub[0].nnzLU + 3) & ~3);
+    fits = (long long)off1 + P.sub[1].nnzLU <= 65536;
 }
 
 void host_jacobian(const Plan &P, const cplx *Yx, const cplx *V, std::vector<double> &Jx) {
@@ -734,6 +741,150 @@ int build_dc_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, 
             P.xP[b] = P.pinv[id[b]];
             P.xVa[b] = P.qinv[id[b]];
         }
+    return NoError;
+}
+
+namespace {
+
+// The system of one decoupled half-step: the rows / columns `ids` (grid buses) of a grid-level
+// matrix, with their values as the constants of the plan; analysed like a Jacobian and
+// factorised on the host by running the refactorisation program's updates in order (the
+// operations of a phase are independent, so program order is a valid serial order).
+int fdpf_system(Plan &S, int n, const RealCsc &B, const std::vector<int> &ids, const PlanOptions &opt,
+                const char *what, std::string &msg, std::vector<double> &lu) {
+    S = Plan();
+    const int m = (int)ids.size();
+    S.m = m;
+    std::vector<int> inv(n, -1);
+    for (int k = 0; k < m; ++k) inv[ids[k]] = k;
+    S.Jp.assign(m + 1, 0);
+    std::vector<std::pair<int, double>> col;
+    std::vector<double> Bx;
+    for (int k = 0; k < m; ++k) {
+        const int c = ids[k];
+        col.clear();
+        for (int p = B.p[c]; p < B.p[c + 1]; ++p)
+            if (B.i[p] >= 0 && B.i[p] < n && inv[B.i[p]] >= 0) col.push_back({inv[B.i[p]], B.x[p]});
+        std::sort(col.begin(), col.end());
+        for (auto &e : col) {
+            S.Ji.push_back(e.first);
+            S.jsrc.push_back(-1);
+            S.jkind.push_back(0);
+            S.jconst.push_back(e.second);
+            Bx.push_back(e.second);
+        }
+        S.Jp[k + 1] = (int)S.Ji.size();
+    }
+    if (m == 0) {
+        S.factor.base.assign(1, 0);
+        S.backward.base.assign(1, 0);
+        S.forward.base.assign(1, 0);
+        lu.clear();
+        return NoError;
+    }
+    std::string sub;
+    const int rc = analyze_lu(S, Bx, opt, sub);
+    if (rc != NoError) {
+        msg = std::string("build_fdpf_plan: ") + what + ": " + sub;
+        return rc;
+    }
+    lu.assign(S.nnzLU, 0.0);
+    for (size_t t = 0; t < S.cpos.size(); ++t) lu[S.cpos[t]] = S.cval[t];
+    const int nops = S.factor.nops();
+    for (int o = 0; o < nops; ++o) {
+        const int *op = &S.factor.ops[4 * (size_t)o];
+        if (((unsigned)op[3] >> 28) != 0u) continue;  // substitution pushes and padding
+        const int w = op[3] & 0x0fffffff;
+        lu[op[0]] -= lu[op[1]] * (lu[op[2]] / lu[w]);
+    }
+    for (int k = 0; k < m; ++k) {
+        const double d = lu[S.dpos[k]];
+        if (d == 0.0 || !std::isfinite(d)) {
+            msg = std::string("build_fdpf_plan: ") + what + " is singular";
+            return SolverFactor;
+        }
+    }
+    return NoError;
+}
+
+}  // namespace
+
+int build_fdpf_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, const RealCsc &Bp,
+                    const RealCsc &Bpp, const int *slack_ids, int nslack, const double *weights, const int *pv,
+                    int npv, const int *pq, int npq, const PlanOptions &opt, std::string &msg) {
+    P = Plan();
+    if (n <= 0 || nslack <= 0) {
+        msg = "build_fdpf_plan: the grid needs at least one bus and one slack bus";
+        return NotInitError;
+    }
+    if (check_ybus(n, Yp, Yi, msg) != NoError) return NotInitError;
+    for (const RealCsc *B : {&Bp, &Bpp})
+        if (!B->p || !B->i || !B->x || B->p[0] != 0 || B->p[n] < 0) {
+            msg = "build_fdpf_plan: B' and B'' must be n x n CSC matrices";
+            return NotInitError;
+        }
+    std::vector<int> role(n, 0);  // 0 none, 1 slack, 2 pv, 3 pq
+    for (int t = 0; t < nslack; ++t) {
+        if (slack_ids[t] < 0 || slack_ids[t] >= n) { msg = "build_fdpf_plan: slack id out of range"; return NotInitError; }
+        role[slack_ids[t]] = 1;
+    }
+    for (int t = 0; t < npv; ++t) {
+        if (pv[t] < 0 || pv[t] >= n || role[pv[t]] != 0) {
+            msg = "build_fdpf_plan: a PV bus is out of range, repeated or also a slack";
+            return NotInitError;
+        }
+        role[pv[t]] = 2;
+    }
+    for (int t = 0; t < npq; ++t) {
+        if (pq[t] < 0 || pq[t] >= n || role[pq[t]] != 0) {
+            msg = "build_fdpf_plan: a PQ bus is out of range, repeated or also PV / slack";
+            return NotInitError;
+        }
+        role[pq[t]] = 3;
+    }
+    P.fdpf = true;
+    P.factor.base.assign(1, 0);  // no programs of its own: the systems in `sub` carry them
+    P.backward.base.assign(1, 0);
+    P.forward.base.assign(1, 0);
+    P.n = n;
+    P.nnzY = Yp[n];
+    P.Yp.assign(Yp, Yp + n + 1);
+    P.Yi.assign(Yi, Yi + P.nnzY);
+    P.Yx.assign(Yx, Yx + P.nnzY);
+    P.slack0 = slack_ids[0];
+    P.slack_ids.assign(slack_ids, slack_ids + nslack);
+    P.weights.assign(weights, weights + n);
+    make_csr(P);
+    // pvpq = [slacks after the first, pv, pq] (BaseFDPFAlgo.tpp:61-70)
+    for (int t = 1; t < nslack; ++t) P.mypv.push_back(slack_ids[t]);
+    P.mypv.insert(P.mypv.end(), pv, pv + npv);
+    P.pq.assign(pq, pq + npq);
+    P.pvpq = P.mypv;
+    P.pvpq.insert(P.pvpq.end(), pq, pq + npq);
+    P.npv = (int)P.mypv.size();
+    P.npq = npq;
+    P.npvpq = (int)P.pvpq.size();
+    P.sub.resize(2);
+    P.sublu.resize(2);
+    int rc = fdpf_system(P.sub[0], n, Bp, P.pvpq, opt, "B'", msg, P.sublu[0]);
+    if (rc != NoError) return rc;
+    rc = fdpf_system(P.sub[1], n, Bpp, P.pq, opt, "B''", msg, P.sublu[1]);
+    if (rc != NoError) return rc;
+    P.m = P.npvpq + npq;
+    // bus maps: P of bus b at xP[b] of the B' right-hand side, its angle step at xVa[b];
+    // Q at xQ[b] of the B'' right-hand side, its magnitude step at xVm[b]
+    P.xP.assign(n, -1);
+    P.xQ.assign(n, -1);
+    P.xVa.assign(n, -1);
+    P.xVm.assign(n, -1);
+    for (int k = 0; k < P.npvpq; ++k) {
+        P.xP[P.pvpq[k]] = P.sub[0].pinv[k];
+        P.xVa[P.pvpq[k]] = P.sub[0].qinv[k];
+    }
+    for (int k = 0; k < npq; ++k) {
+        P.xQ[pq[k]] = P.sub[1].pinv[k];
+        P.xVm[pq[k]] = P.sub[1].qinv[k];
+    }
     return NoError;
 }
 

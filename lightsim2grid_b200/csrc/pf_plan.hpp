@@ -110,6 +110,15 @@ struct Plan {
     // statistics
     long long flops_refactor = 0;     // multiply-adds of one refactorisation
     int levels_refactor = 0, levels_fwd = 0, levels_bwd = 0;
+
+    // ------------------------------------------------------------ fast decoupled
+    // FDPF plan: the Ybus data above drive the mismatch; sub[0] is B' over pvpq, sub[1] B''
+    // over pq (each with its own ordering, pivots, LU layout and substitution programs) and
+    // sublu[k] their factor values, computed once (the matrices do not change between calls).
+    // Bus maps: xP / xVa index the B' system, xQ / xVm the B'' system.
+    bool fdpf = false;
+    std::vector<Plan> sub;
+    std::vector<std::vector<double>> sublu;
 };
 
 struct PlanOptions {
@@ -129,13 +138,32 @@ int build_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, con
 // 16 bits per index, so every operation is  s[x] -= s[y] * s[z] / s[w]  (8 bytes).
 int compact_lu_offset(int m);
 bool compact_fits(const Plan &P);
-void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out);  // 2 words per op
+// 2 words per op; lu_offset >= 0 places the LU elsewhere in the index space (the two systems of
+// a fast-decoupled plan share one solve vector, their LUs follow it one after the other)
+void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out, int lu_offset = -1);
+// Index-space offsets of the B' and B'' LUs of a fast-decoupled plan behind their shared solve
+// vector, and whether both fit the 16-bit packed indices.
+void fdpf_lu_offsets(const Plan &P, int &off0, int &off1, bool &fits);
 
 // Builds a DC plan (BaseDCAlgo, src/powerflow_algorithm/BaseDCAlgo.tpp): the matrix is
 // B = Re(Ybus) over every bus except the first slack (the other slacks count as PV), factorised
 // and scheduled like a Jacobian.  Ybus is the DC admittance matrix.  Returns an Err code.
 int build_dc_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, const int *slack_ids, int nslack,
                   const int *pv, int npv, const int *pq, int npq, const PlanOptions &opt, std::string &msg);
+
+// A real sparse matrix, CSC (n x n, canonical).
+struct RealCsc {
+    const int *p, *i;
+    const double *x;
+};
+
+// Builds a fast-decoupled plan (BaseFDPFAlgo, src/powerflow_algorithm/BaseFDPFAlgo.tpp:11-214):
+// pvpq = [slacks after the first, pv, pq] (retrieve_pv_with_slack, BaseAlgo.hpp:201-216),
+// B'_ = Bp[pvpq, pvpq] and B''_ = Bpp[pq, pq] (fill_sparse_matrices, BaseFDPFAlgo.tpp:175-214)
+// from the grid-level B' and B'' (n x n), both factorised here.  Returns an Err code.
+int build_fdpf_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, const RealCsc &Bp,
+                    const RealCsc &Bpp, const int *slack_ids, int nslack, const double *weights, const int *pv,
+                    int npv, const int *pq, int npq, const PlanOptions &opt, std::string &msg);
 
 // Host evaluation of the Jacobian values (J CSC order) at V for Ybus values Yx (CSC order).
 void host_jacobian(const Plan &P, const cplx *Yx, const cplx *V, std::vector<double> &Jx);

@@ -159,6 +159,40 @@ class GridModel:
         Y.sort_indices()
         return Y
 
+    def get_Bp_Bpp(self, method=0):
+        """Grid-level B' and B'' of the fast decoupled power flow, ``method`` 0 = XB, 1 = BX
+        (GridModel::fillBp_Bpp, GridModel.cpp:1037-1064; line terms TwoSidesContainer_rxh_A.hpp:
+        503-580 with get_fdpf_coeffs :810-837).  Per line in service, with ys' = 1/(j x) and
+        ys'' = 1/(r + j x) for XB (swapped for BX): B' gets -Im(ys') at (f,f) and (t,t) and
+        +Im(ys') at (f,t) and (t,f); B'' gets -(Im(ys'') + Im(h)/2) at (f,f) and (t,t) and
+        +Im(ys'') off the diagonal.  Canonical CSC, duplicates summed."""
+        on = self.line_status
+        f, t = self.line_from[on], self.line_to[on]
+        r, x, h = self.line_r[on], self.line_x[on], self.line_h[on]
+        ys_x = 1.0 / (1j * x)
+        ys_rx = 1.0 / (r + 1j * x)
+        ys_p, ys_pp = (ys_x, ys_rx) if int(method) == 0 else (ys_rx, ys_x)
+        bp, bpp = np.imag(ys_p), np.imag(ys_pp)
+        hh = np.imag(0.5 * h)
+        rows = np.concatenate([f, t, f, t])
+        cols = np.concatenate([f, t, t, f])
+        out = []
+        for vals in (np.concatenate([-bp, -bp, bp, bp]),
+                     np.concatenate([-(bpp + hh), -(bpp + hh), bpp, bpp])):
+            B = sparse.csc_matrix((vals, (rows, cols)), shape=(self.n_bus, self.n_bus), dtype=np.float64)
+            B.sum_duplicates()
+            B.sort_indices()
+            out.append(B)
+        return out[0], out[1]
+
+    def debug_get_Bp_python(self, method=0):
+        """Grid-level B' (the reference binds GridModel.debug_get_Bp_python(FDPFMethod))."""
+        return self.get_Bp_Bpp(method)[0]
+
+    def debug_get_Bpp_python(self, method=0):
+        """Grid-level B''."""
+        return self.get_Bp_Bpp(method)[1]
+
     def dc_branch_coeffs(self, branch_ids):
         """DC Ybus coefficients of the given branches, in the reference's order."""
         out = []

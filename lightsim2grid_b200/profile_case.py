@@ -30,6 +30,8 @@ def main():
     ap.add_argument("--lu-reuse", type=float, default=0.0, help="LU reuse threshold (<= 0: never, the default)")
     ap.add_argument("--check", action="store_true", help="compare the voltages with an FP64 plan's")
     ap.add_argument("--dc", action="store_true", help="DC power flows (DC Ybus, DC outage coefficients)")
+    ap.add_argument("--fdpf", type=int, default=-1, help="fast decoupled power flows: 0 XB, 1 BX (-1: Newton)")
+    ap.add_argument("--max-iter", type=int, default=10)
     args = ap.parse_args()
 
     import torch
@@ -47,7 +49,8 @@ def main():
     if args.dc:
         Y = g.get_dcYbus()
         coeffs = [g.dc_branch_coeffs([b]) for b in range(nb)]
-    plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, dc=args.dc, threads=args.threads,
+    fdpf = g.get_Bp_Bpp(args.fdpf) if args.fdpf >= 0 else None
+    plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, dc=args.dc, fdpf=fdpf, threads=args.threads,
                 lu_placement=args.lu_placement, fuse_forward=args.fuse_forward, max_ctas_per_sm=args.ctas_per_sm,
                 refine=args.refine, refine_threshold=args.refine_threshold, lu_reuse_threshold=args.lu_reuse)
     lib = plan._lib
@@ -78,8 +81,9 @@ def main():
             torch.zeros(ns, dtype=torch.int32, device=dev), torch.zeros(ns, dtype=torch.int32, device=dev)]
     b = nat.PfDeviceBatch(n_inst=ns, V0=bufs[0].data_ptr(), v0_stride=0, Sbus=bufs[1].data_ptr(), sbus_stride=0,
                           ovr_ptr=bufs[2].data_ptr(), ovr_pos=bufs[3].data_ptr(), ovr_val=bufs[4].data_ptr(),
-                          max_iter=10, tol=1e-8, chain=0, job_first=bufs[5].data_ptr(), job_count=bufs[6].data_ptr(),
-                          njobs=ns, Vout=bufs[7].data_ptr(), iters=bufs[8].data_ptr(), errs=bufs[9].data_ptr())
+                          max_iter=args.max_iter, tol=1e-8, chain=0, job_first=bufs[5].data_ptr(),
+                          job_count=bufs[6].data_ptr(), njobs=ns, Vout=bufs[7].data_ptr(), iters=bufs[8].data_ptr(),
+                          errs=bufs[9].data_ptr())
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
         assert lib.pf_batch_device(plan.handle, nat.ctypes.byref(b), stream.cuda_stream) == 0, nat.last_error(lib)
@@ -97,7 +101,8 @@ def main():
                                             nat.ptr(cyc, nat.f64p)) == 0, nat.last_error(lib)
     names = ["mismatch", "jfill", "refactor", "forward", "backward", "refine", "update", "instances"]
     tot = cyc[:7].sum()
-    phase_share = {k: round(float(v / tot), 4) for k, v in zip(names[:7], cyc[:7])}
+    # the DC and fast-decoupled kernels do not record phase cycles
+    phase_share = {k: round(float(v / tot), 4) for k, v in zip(names[:7], cyc[:7])} if tot > 0 else None
     tr = np.zeros(2048)
     ntr = lib.pf_batch_device_phase_trace(plan.handle, nat.ctypes.byref(b), stream.cuda_stream,
                                           nat.ptr(tr, nat.f64p), 2048)
@@ -128,7 +133,8 @@ def main():
     out = {"grid": args.grid, "cases": ns, "precision": args.precision, "ms": times, "check": check,
            "converged": int((er == 0).sum()), "iterations": int(it.sum()),
            "pf_per_s": float((er == 0).sum() / (np.mean(times) * 1e-3)),
-           "cycles_per_iteration_per_cta": float(tot / max(1, int(it.sum()))), "phase_share": phase_share,
+           "cycles_per_iteration_per_cta": float(tot / max(1, int(it.sum()))) if tot > 0 else None,
+           "phase_share": phase_share,
            "plan": plan.info(), "phase_trace_cycles": trace}
     print(json.dumps(out))
 

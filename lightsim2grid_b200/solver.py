@@ -15,7 +15,7 @@ from . import _native as nat
 
 
 class SolverType(enum.IntEnum):
-    """Members 0-21 are the reference's (src/ChooseSolver.hpp:17-25); 22-26 are this engine's."""
+    """Members 0-21 are the reference's (src/ChooseSolver.hpp:17-25); 22-28 are this engine's."""
 
     SparseLU = 0
     KLU = 1
@@ -49,6 +49,17 @@ class SolverType(enum.IntEnum):
     GPUNRMixedSingleSlack = 25
     #: DC power flow on the GPU, FP64 (drop-in for KLUDC)
     GPUDC = 26
+    #: fast decoupled power flow on the GPU, XB method, FP64 (drop-in for FDPF_XB_KLU)
+    GPUFDPF_XB = 27
+    #: fast decoupled power flow on the GPU, BX method, FP64 (drop-in for FDPF_BX_KLU)
+    GPUFDPF_BX = 28
+
+
+class FDPFMethod(enum.IntEnum):
+    """src/BaseConstants.hpp:35."""
+
+    XB = 0
+    BX = 1
 
 
 class ErrorType(enum.IntEnum):
@@ -67,11 +78,15 @@ class ErrorType(enum.IntEnum):
 
 
 GPU_SOLVERS = (SolverType.GPUNR, SolverType.GPUNRSingleSlack, SolverType.GPUNRMixed,
-               SolverType.GPUNRMixedSingleSlack)
+               SolverType.GPUNRMixedSingleSlack, SolverType.GPUFDPF_XB, SolverType.GPUFDPF_BX)
+
+#: fast decoupled solver types and their method
+FDPF_SOLVERS = {SolverType.GPUFDPF_XB: FDPFMethod.XB, SolverType.GPUFDPF_BX: FDPFMethod.BX}
 
 
 def solver_flags(solver_type):
-    """``(distributed, precision)`` of a GPU solver type."""
+    """``(distributed, precision)`` of a GPU solver type (fast decoupled: ``(False, 0)``, the
+    slack weights enter through pvpq and the mismatch)."""
     st = SolverType(solver_type)
     if st not in GPU_SOLVERS:
         raise RuntimeError("Solver type {} is not available in lightsim2grid_b200 (available: {})".format(
@@ -97,7 +112,7 @@ class Plan:
 
     def __init__(self, Ybus, V0, Sbus, slack_ids, slack_weights, pv, pq, distributed=False, precision=0,
                  threads=0, lu_placement=0, fuse_forward=0, fp64_fallback=0, max_ctas_per_sm=0, refine=0,
-                 refine_threshold=0.0, lu_reuse_threshold=0.0, dc=False):
+                 refine_threshold=0.0, lu_reuse_threshold=0.0, dc=False, fdpf=None):
         self._lib = nat.load()
         Y = canonical_csc(Ybus)
         n = Y.shape[0]
@@ -125,7 +140,29 @@ class Plan:
                             lu_reuse_threshold=float(lu_reuse_threshold))
         h = nat.ctypes.c_void_p()
         self.dc = bool(dc)
-        if self.dc:
+        self.fdpf = fdpf is not None
+        if self.fdpf:
+            # fast decoupled (BaseFDPFAlgo): fdpf = (B', B''), grid-level n x n real matrices
+            self.precision = 0
+            Bs = []
+            for B in fdpf:
+                B = sparse.csc_matrix(B, dtype=np.float64)
+                if B.shape != (n, n):
+                    raise RuntimeError("B' and B'' must be {} x {}".format(n, n))
+                B = B.copy()
+                B.sum_duplicates()
+                B.sort_indices()
+                Bs.append((nat.as_i32(B.indptr), nat.as_i32(B.indices), nat.as_f64(B.data)))
+            self._fdpf_arrays = Bs
+            (bpp_, bpi, bpx), (bppp, bppi, bppx) = Bs
+            rc = self._lib.pf_fdpf_plan_create(
+                n, nat.ptr(self.Yp, nat.i32p), nat.ptr(self.Yi, nat.i32p), nat.cptr(self.Yx),
+                nat.ptr(bpp_, nat.i32p), nat.ptr(bpi, nat.i32p), nat.ptr(bpx, nat.f64p), nat.ptr(bppp, nat.i32p),
+                nat.ptr(bppi, nat.i32p), nat.ptr(bppx, nat.f64p), nat.ptr(self.slack_ids, nat.i32p),
+                self.slack_ids.size, nat.ptr(w, nat.f64p), nat.ptr(self.pv, nat.i32p), self.pv.size,
+                nat.ptr(self.pq, nat.i32p), self.pq.size, nat.ctypes.byref(opt), nat.ctypes.byref(h))
+            nat.check(rc, "pf_fdpf_plan_create", self._lib)
+        elif self.dc:
             # DC power flow (BaseDCAlgo): Ybus is the DC admittance matrix, FP64
             self.precision = 0
             rc = self._lib.pf_dc_plan_create(
@@ -379,6 +416,117 @@ class GPUDCSolver(_GPUNRSolverBase):
         raise RuntimeError("get_J: a DC solver has no Jacobian")
 
 
+def _fingerprint(B):
+    B = sparse.csc_matrix(B, dtype=np.float64).copy()
+    B.sum_duplicates()
+    B.sort_indices()
+    return B.shape, B.indptr.copy(), B.indices.copy(), B.data.copy()
+
+
+def _same_fingerprint(a, b):
+    return a[0] == b[0] and all(np.array_equal(x, y) for x, y in zip(a[1:], b[1:]))
+
+
+class _GPUFDPFSolverBase(_GPUNRSolverBase):
+    """Drop-in for the reference's FDPF solvers (BaseFDPFAlgo, src/powerflow_algorithm/
+    BaseFDPFAlgo.tpp:11-214; bound as FDPF_XB_* / FDPF_BX_*).  The reference's solver takes B'
+    and B'' from the grid model it is attached to (GridModel::fillBp_Bpp); here
+    ``set_gridmodel(grid)`` (a ``lightsim2grid_b200.GridModel``) or ``set_Bp_Bpp(Bp, Bpp)``
+    gives them.  The factors are kept while B', B'', the pattern, slacks, PV and PQ stay the same."""
+
+    _method = FDPFMethod.XB
+
+    def __init__(self, **plan_options):
+        self._Bp = self._Bpp = None
+        self._grid = None
+        self._bfp = []
+        super().__init__(**plan_options)
+
+    def set_gridmodel(self, grid):
+        self._grid = grid
+        self._plan = None
+
+    def set_Bp_Bpp(self, Bp, Bpp):
+        self._Bp, self._Bpp = sparse.csc_matrix(Bp), sparse.csc_matrix(Bpp)
+        self._grid = None
+        self._plan = None
+
+    def _matrices(self):
+        if self._grid is not None:
+            return self._grid.get_Bp_Bpp(self._method)
+        if self._Bp is None:
+            raise RuntimeError("compute_pf: no B' / B'' (call set_gridmodel or set_Bp_Bpp first)")
+        return self._Bp, self._Bpp
+
+    def compute_pf(self, Ybus, V, Sbus, slack_ids, slack_weights, pv, pq, max_iter, tol):
+        t0 = time.perf_counter()
+        Y = canonical_csc(Ybus)
+        n = Y.shape[0]
+        V = nat.as_c128(V).ravel()
+        Sbus = nat.as_c128(Sbus).ravel()
+        if Sbus.size != n or Y.shape[1] != n:
+            raise RuntimeError("BaseFDPFAlgo::compute_pf: Size of the Sbus should be the same as the size of Ybus. "
+                               "Currently: Sbus  ({}) and Ybus ({}, {}).".format(Sbus.size, Y.shape[0], Y.shape[1]))
+        if V.size != n:
+            raise RuntimeError("BaseFDPFAlgo::compute_pf: Size of V (init voltages) should be the same as the size "
+                               "of Ybus. Currently: V  ({}) and Ybus ({}, {}).".format(V.size, Y.shape[0], Y.shape[1]))
+        w = nat.as_f64(slack_weights)
+        if w.size != n:
+            w = np.zeros(n)
+            sl = nat.as_i32(slack_ids)
+            w[sl] = 1.0 / max(sl.size, 1)
+        Bp, Bpp = self._matrices()
+        fp = [_fingerprint(B) for B in (Bp, Bpp)]
+        same = (self._plan is not None and self._plan.same_structure(Y, slack_ids, pv, pq)
+                and all(_same_fingerprint(a, b) for a, b in zip(fp, self._bfp)))
+        if not same:
+            self._plan = Plan(Y, V, Sbus, slack_ids, w, pv, pq, fdpf=(Bp, Bpp), **self._plan_options)
+            self._bfp = fp
+        else:
+            self._plan.set_ybus_values(Y.data)
+        Vout, conv, it, err = self._plan.solve(V, Sbus, max_iter, tol)
+        self._V = Vout
+        self._nb_iter = it
+        self._err = ErrorType(err)
+        self._timer_total = time.perf_counter() - t0
+        return conv
+
+    solve = compute_pf
+
+    def get_J(self):
+        raise RuntimeError("get_J: a fast decoupled solver has no Jacobian")
+
+    def _sub(self, which):
+        if self._plan is None:
+            raise RuntimeError("no power flow has been computed")
+        p = self._plan
+        Bp, Bpp = self._matrices()
+        pvpq = np.r_[p.slack_ids[1:], p.pv, p.pq].astype(np.int64)
+        ids = pvpq if which == 0 else p.pq.astype(np.int64)
+        B = sparse.csc_matrix(Bp if which == 0 else Bpp)
+        return B[ids][:, ids].tocsc()
+
+    def debug_get_Bp_python(self):
+        """B'[pvpq, pvpq] as the solver uses it (BaseFDPFAlgo.hpp:47)."""
+        return self._sub(0)
+
+    def debug_get_Bpp_python(self):
+        """B''[pq, pq] as the solver uses it (BaseFDPFAlgo.hpp:48)."""
+        return self._sub(1)
+
+
+class GPUFDPFSolverXB(_GPUFDPFSolverBase):
+    """Drop-in for FDPF_XB_KLUSolver: B' without resistances, B'' with them."""
+
+    _method = FDPFMethod.XB
+
+
+class GPUFDPFSolverBX(_GPUFDPFSolverBase):
+    """Drop-in for FDPF_BX_KLUSolver: B' with resistances, B'' without them."""
+
+    _method = FDPFMethod.BX
+
+
 class GPUNRMixedSolver(_GPUNRSolverBase):
     """Distributed slack, FP32 LU and solves, FP64 mismatch, update and convergence test."""
 
@@ -392,4 +540,6 @@ SOLVER_CLASSES = {
     SolverType.GPUNRMixed: GPUNRMixedSolver,
     SolverType.GPUNRMixedSingleSlack: GPUNRMixedSolverSingleSlack,
     SolverType.GPUDC: GPUDCSolver,
+    SolverType.GPUFDPF_XB: GPUFDPFSolverXB,
+    SolverType.GPUFDPF_BX: GPUFDPFSolverBX,
 }
