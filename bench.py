@@ -404,7 +404,7 @@ def run_ours(args):
         e2e_t = float(tt.item())
     ns = mixed["ns"]
     h2d = 2 * n * 16 + (ns + 1) * 4 + int(cp[-1]) * (4 + 16) + 2 * ns * 4
-    d2h = ns * n * 16 + 2 * ns * 4
+    d2h = nc * n * 16 + 2 * ns * 4  # every case's voltage row (zero rows included), iterations, errors
 
     serve = None
     if ws == 1 and args.serve_seconds > 0:

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -80,6 +81,7 @@ struct pf_plan {
     DevBuf scratch, counter, V0, Sbus, optr, opos, oval, jfirst, jcount, Vout, iters, errs, Jout, cycles, Vcase,
         casemap;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // result downloads that overlap the FP64 re-run
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // host state
     std::vector<double> lastJ;
@@ -468,6 +470,8 @@ void release(pf_plan *pl) {
     if (pl->ev0) cudaEventDestroy(pl->ev0);
     if (pl->ev1) cudaEventDestroy(pl->ev1);
     if (pl->stream) cudaStreamDestroy(pl->stream);
+    if (pl->copy_stream) cudaStreamDestroy(pl->copy_stream);
+    pl->copy_stream = nullptr;
     pl->ev0 = pl->ev1 = nullptr;
     pl->stream = nullptr;
 }
@@ -542,7 +546,8 @@ cudaError_t h2d(DevBuf &b, const T *src, size_t count, cudaStream_t st) {
 int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, const cplx *Sbus, long long sbus_stride,
               const std::vector<int> &optr, const std::vector<int> &opos, const std::vector<cplx> &oval,
               const std::vector<int> &jfirst, const std::vector<int> &jcount, int chain, int max_iter, double tol,
-              cplx *Vout, int *iters, int *errs, bool want_J) {
+              cplx *Vout, int *iters, int *errs, bool want_J,
+              const std::function<int(const std::vector<char> &)> *settled = nullptr) {
     const int n = pl->P.n;
     cudaStream_t st = pl->stream;
     double t0 = now();
@@ -599,8 +604,12 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
     float kms = 0.f;
     cudaEventElapsedTime(&kms, pl->ev0, pl->ev1);
     double kernel_s = kms * 1e-3;
-    // mixed form: re-run in FP64 the jobs that contain a failure
+    // mixed form: re-run in FP64 the jobs that contain a failure.  `settled` (if given) is called
+    // once the re-run is queued, with the instances it recomputes: every other instance's row is
+    // final, so the caller can copy those rows out while the re-run runs.
     int rerun = 0;
+    std::vector<char> again;
+    if (settled) again.assign((size_t)n_inst, 0);
     if (pl->precision == 1 && pl->opt.fp64_fallback != 2) {
         std::vector<int> rf, rc2;
         for (size_t j = 0; j < jfirst.size(); ++j) {
@@ -611,6 +620,8 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
                 rf.push_back(jfirst[j]);
                 rc2.push_back(jcount[j]);
                 rerun += jcount[j];
+                if (settled)
+                    for (int s = 0; s < jcount[j]; ++s) again[(size_t)jfirst[j] + s] = 1;
             }
         }
         if (!rf.empty()) {
@@ -623,6 +634,8 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
             rc = launch(pl, a, 0, st);
             if (rc) return rc;
             cudaEventRecord(pl->ev1, st);
+            if (settled && (rc = (*settled)(again)) != 0) return rc;
+            settled = nullptr;
             if ((e = cudaMemcpyAsync(iters, pl->iters.p, (size_t)n_inst * sizeof(int), cudaMemcpyDeviceToHost,
                                      st)) != cudaSuccess)
                 return cuda_fail(e, "rerun: download");
@@ -634,6 +647,7 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
             kernel_s += kms * 1e-3;
         }
     }
+    if (settled && (rc = (*settled)(again)) != 0) return rc;
     double t2 = now();
     if (Vout &&
         (e = cudaMemcpyAsync(Vout, pl->Vout.p, (size_t)n_inst * n * sizeof(cplx), cudaMemcpyDeviceToHost, st)) !=
@@ -706,7 +720,9 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 int finish_plan(pf_plan *pl, pf_plan **out) {
     compute_bridges(pl);
     cudaError_t e = cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&pl->copy_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
+        if (pl->stream) cudaStreamDestroy(pl->stream);
         delete pl;
         return cuda_fail(e, "pf_plan_create: stream");
     }
@@ -1007,16 +1023,55 @@ int pf_batch_n1(pf_plan *pl, int ncases, const int *case_ptr, const int *coef_ro
     std::vector<int> it(std::max(ns, 1)), er(std::max(ns, 1));
     double t1 = now();
     cplx *Vo = reinterpret_cast<cplx *>(V_out_ri);
+    // result rows in case order on the device, then one copy into the caller's array, on the copy
+    // stream: issued as soon as the rows are final, so the copy overlaps the FP64 re-run of the
+    // instances that failed in the mixed form; their rows follow once the re-run is done
+    cudaStream_t cs = pl->copy_stream;
+    std::vector<int> map(ncases, -1);
+    for (int i = 0; i < ns; ++i) map[idx[i]] = i;
+    std::vector<char> rerun_rows;
+    const std::function<int(const std::vector<char> &)> settled = [&](const std::vector<char> &again) -> int {
+        std::vector<int> m1 = map;
+        for (int c = 0; c < ncases; ++c)
+            if (m1[c] >= 0 && again[m1[c]]) m1[c] = -1;  // zero for now, copied after the re-run
+        rerun_rows = again;
+        cudaError_t e;
+        if ((e = pl->casemap.ensure((size_t)std::max(ncases, 1) * sizeof(int))) != cudaSuccess)
+            return cuda_fail(e, "pf_batch_n1: alloc");
+        if ((e = pl->Vcase.ensure((size_t)std::max(ncases, 1) * n * sizeof(cplx))) != cudaSuccess)
+            return cuda_fail(e, "pf_batch_n1: alloc");
+        if ((e = cudaMemcpyAsync(pl->casemap.p, m1.data(), (size_t)ncases * sizeof(int), cudaMemcpyHostToDevice,
+                                 cs)) != cudaSuccess)
+            return cuda_fail(e, "pf_batch_n1: upload");
+        if ((e = cudaStreamSynchronize(cs)) != cudaSuccess) return cuda_fail(e, "pf_batch_n1: upload");
+        if ((e = l2g::launch_scatter_case_rows(static_cast<const double2 *>(pl->Vout.p),
+                                               static_cast<const int *>(pl->errs.p),
+                                               static_cast<const int *>(pl->casemap.p), ncases, n,
+                                               static_cast<double2 *>(pl->Vcase.p), pl->num_sms, cs)) != cudaSuccess)
+            return cuda_fail(e, "pf_batch_n1: scatter");
+        if ((e = cudaMemcpyAsync(Vo, pl->Vcase.p, (size_t)ncases * n * sizeof(cplx), cudaMemcpyDeviceToHost, cs)) !=
+            cudaSuccess)
+            return cuda_fail(e, "pf_batch_n1: download");
+        return 0;
+    };
     if (ns > 0) {
         int rc = run_batch(pl, ns, reinterpret_cast<const cplx *>(V0_ri), 0, reinterpret_cast<const cplx *>(Sbus_ri),
-                           0, optr, opos, oval, jf, jc, 0, max_iter, tol, nullptr, it.data(), er.data(), false);
-        if (rc) return rc;
-    }
-    // result rows in case order, on the device, then one copy into the caller's array
-    {
+                           0, optr, opos, oval, jf, jc, 0, max_iter, tol, nullptr, it.data(), er.data(), false,
+                           &settled);
+        if (rc) {
+            cudaStreamSynchronize(cs);
+            return rc;
+        }
+        // rows of re-run instances that converged in FP64 (the others stay zero)
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < ns && e == cudaSuccess; ++i)
+            if (rerun_rows[i] && er[i] == 0)
+                e = cudaMemcpyAsync(Vo + (size_t)idx[i] * n, static_cast<const cplx *>(pl->Vout.p) + (size_t)i * n,
+                                    (size_t)n * sizeof(cplx), cudaMemcpyDeviceToHost, cs);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+        if (e != cudaSuccess) return cuda_fail(e, "pf_batch_n1: download");
+    } else {
         cudaStream_t st = pl->stream;
-        std::vector<int> map(ncases, -1);
-        for (int i = 0; i < ns; ++i) map[idx[i]] = i;
         cudaError_t e;
         if ((e = pl->casemap.ensure((size_t)std::max(ncases, 1) * sizeof(int))) != cudaSuccess)
             return cuda_fail(e, "pf_batch_n1: alloc");
