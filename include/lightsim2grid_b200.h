@@ -88,7 +88,10 @@ typedef struct pf_device_batch {
     long long v0_stride;     /* in complex elements                                          */
     const void *Sbus;        /* complex, n per instance (or one vector if sbus_stride == 0)  */
     long long sbus_stride;
-    const int *ovr_ptr;      /* n_inst + 1; Ybus overrides per instance (may be NULL)        */
+    const int *ovr_ptr;      /* n_inst + 1; Ybus overrides per instance (may be NULL); at most
+                                32 per instance: an instance with more is not computed
+                                (errs NotInitError, iterations 0, start voltages out; a
+                                time-series chain stops there)                                */
     const int *ovr_pos;      /* CSR positions of the overridden Ybus entries                  */
     const void *ovr_val;     /* complex, new value of each overridden entry                   */
     int max_iter;

@@ -481,7 +481,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 k0 = A.ovr_ptr[inst];
                 k1 = A.ovr_ptr[inst + 1];
             }
-            S.novr = min(k1 - k0, kMaxOverrides);
+            S.novr = k1 - k0 > kMaxOverrides ? -1 : k1 - k0;  // -1: too many to stage
             S.piv_err = 0;
             S.slack_absorbed = 0.0;
         }
@@ -498,6 +498,24 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
             if (tid == 0) S.slack_absorbed = tot;
         }
         __syncthreads();
+        if (S.novr < 0) {
+            // more Ybus overrides than the kernel stages: not computed (start voltages out)
+            double2 *vo = A.Vout + (long long)inst * n;
+            for (int b = tid; b < n; b += blockDim.x) vo[b] = V[b];
+            if (tid == 0) {
+                A.iters[inst] = 0;
+                A.errs[inst] = 8;  // NotInitError
+            }
+            __syncthreads();
+            if (A.chain) {
+                for (int s2 = step + 1 + tid; s2 < count; s2 += blockDim.x) {
+                    A.iters[first + s2] = 0;
+                    A.errs[first + s2] = 8;
+                }
+                break;
+            }
+            continue;
+        }
         double norm;
         int bad;
         pr.mark(6);
@@ -717,7 +735,7 @@ __global__ void __launch_bounds__(512, 1) dc_batch_kernel(const DevPlan P, const
                     k0 = A.ovr_ptr[inst];
                     k1 = A.ovr_ptr[inst + 1];
                 }
-                S.novr = min(k1 - k0, kMaxOverrides);
+                S.novr = k1 - k0 > kMaxOverrides ? -1 : k1 - k0;  // -1: too many to stage
                 S.piv_err = 0;
             }
             __syncthreads();
@@ -727,6 +745,18 @@ __global__ void __launch_bounds__(512, 1) dc_batch_kernel(const DevPlan P, const
                 S.oval[tid] = A.ovr_val[k0 + tid];
             }
             __syncthreads();
+            if (S.novr < 0) {
+                // more Ybus overrides than the kernel stages: not computed (start voltages out)
+                const double2 *v0 = A.V0 + (long long)inst * A.v0_stride;
+                double2 *vo = A.Vout + (long long)inst * n;
+                for (int b = tid; b < n; b += blockDim.x) vo[b] = v0[b];
+                if (tid == 0) {
+                    A.iters[inst] = 0;
+                    A.errs[inst] = 8;  // NotInitError
+                }
+                __syncthreads();
+                continue;
+            }
             for (int p = tid; p < P.nnzY; p += blockDim.x) {
                 const int t = P.ytarget[p].x;
                 if (t >= 0) lu[t] = ybus_value(P, S, p).x;
@@ -948,7 +978,7 @@ __global__ void __launch_bounds__(MAXT, MINB) fdpf_batch_kernel(const DevPlan P0
                     k0 = A.ovr_ptr[inst];
                     k1 = A.ovr_ptr[inst + 1];
                 }
-                S.novr = min(k1 - k0, kMaxOverrides);
+                S.novr = k1 - k0 > kMaxOverrides ? -1 : k1 - k0;  // -1: too many to stage
             }
             __syncthreads();
             if (tid < S.novr) {
@@ -961,6 +991,24 @@ __global__ void __launch_bounds__(MAXT, MINB) fdpf_batch_kernel(const DevPlan P0
             const double tot = block_sum(S, ls);  // contains barriers
             if (tid == 0) S.slack_absorbed = tot;
             __syncthreads();
+            if (S.novr < 0) {
+                // more Ybus overrides than the kernel stages: not computed (start voltages out)
+                double2 *vo = A.Vout + (long long)inst * n;
+                for (int b = tid; b < n; b += blockDim.x) vo[b] = V[b];
+                if (tid == 0) {
+                    A.iters[inst] = 0;
+                    A.errs[inst] = 8;  // NotInitError
+                }
+                __syncthreads();
+                if (A.chain) {
+                    for (int s2 = step + 1 + tid; s2 < count; s2 += blockDim.x) {
+                        A.iters[first + s2] = 0;
+                        A.errs[first + s2] = 8;
+                    }
+                    break;
+                }
+                continue;
+            }
             double norm;
             int bad;
             fdpf_mismatch(P, S, V, Vm, Sb, L.x[0], 0, norm, bad);
