@@ -38,6 +38,12 @@ typedef struct pf_options {
                                the refinement threshold); <= 0: never (default).  Measured at
                                1e-5: 5-9 % faster, same iterations and flags, but results up
                                to 5e-8 pu from the FP64 ones instead of 3e-10               */
+    int batch_layout;       /* Newton batches of independent instances (no time-series chain):
+                               0 auto (one CTA per instance), 1 one CTA per instance, 2 batch-
+                               interleaved: 32 instances per CTA, one per lane, every value
+                               stored as 32 consecutive per-instance values (coalesced, the
+                               batch dimension amortises each phase); its per-CTA memory is
+                               allocated on first use                                         */
 } pf_options;
 
 /* DC power flow plan (BaseDCAlgo::compute_pf, src/powerflow_algorithm/BaseDCAlgo.tpp:5-175;

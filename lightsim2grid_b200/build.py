@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "liblightsim2grid_b200.so")
-SOURCES = ["pf_plan.cpp", "pf_capi.cpp", "pf_engine.cu", "pf_noalloc.cu", "pf_flows.cu", "pf_assembly.cu", "pf_server.cpp"]
+SOURCES = ["pf_plan.cpp", "pf_capi.cpp", "pf_engine.cu", "pf_noalloc.cu", "pf_flows.cu", "pf_assembly.cu", "pf_server.cpp", "pf_tile.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

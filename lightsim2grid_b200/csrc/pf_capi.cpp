@@ -77,6 +77,8 @@ struct pf_plan {
     // fast-decoupled plans: the B' and B'' systems
     l2g::DevPlan dsub[2]{};
     void *d_sub_int[2] = {nullptr, nullptr}, *d_sub_dbl[2] = {nullptr, nullptr};
+    // batch-interleaved kernel: per-CTA slabs (allocated on first use) and their size
+    DevBuf tile_scratch;
     // device work buffers
     DevBuf scratch, counter, V0, Sbus, optr, opos, oval, jfirst, jcount, Vout, iters, errs, Jout, cycles, Vcase,
         casemap;
@@ -290,6 +292,15 @@ int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl,
         l2g::compact_ops(P.forward, P.m, cw, lu_offset);
     }
     size_t ocf = push(bi, cf), ocb = push(bi, cb), ocw = push(bi, cw);
+    // the programs regrouped for the batch-interleaved kernel (Newton plans)
+    l2g::TileProgram tf, tb, tw;
+    if (!P.dc && !P.fdpf) {
+        l2g::build_tile_program(P.factor, l2g::kTileWarps, l2g::kTileChunk, tf);
+        l2g::build_tile_program(P.backward, l2g::kTileWarps, l2g::kTileChunk, tb);
+        l2g::build_tile_program(P.forward, l2g::kTileWarps, l2g::kTileChunk, tw);
+    }
+    size_t otfo = push(bi, tf.ops), otbo = push(bi, tb.ops), otwo = push(bi, tw.ops);
+    size_t otfp = push(bi, tf.phase), otbp = push(bi, tb.phase), otwp = push(bi, tw.phase);
     size_t odpos = push(bi, P.dpos);
     std::vector<double> rx(2 * (size_t)P.nnzY);
     for (int i = 0; i < P.nnzY; ++i) {
@@ -368,6 +379,13 @@ int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl,
     d.dc = P.dc ? 1 : 0;
     d.slack0 = P.slack0;
     d.luval = luval ? D(olu) : nullptr;
+    const bool tiled = !P.dc && !P.fdpf;
+    d.tfac_ops = tiled ? I4(otfo) : nullptr;
+    d.tbwd_ops = tiled ? I4(otbo) : nullptr;
+    d.tfwd_ops = tiled ? I4(otwo) : nullptr;
+    d.tfac_phase = tiled ? I(otfp) : nullptr;
+    d.tbwd_phase = tiled ? I(otbp) : nullptr;
+    d.tfwd_phase = tiled ? I(otwp) : nullptr;
     return 0;
 }
 
@@ -455,7 +473,7 @@ int configure(pf_plan *pl) {
 }
 
 void release(pf_plan *pl) {
-    for (DevBuf *b : {&pl->scratch, &pl->counter, &pl->V0, &pl->Sbus, &pl->optr, &pl->opos, &pl->oval,
+    for (DevBuf *b : {&pl->tile_scratch, &pl->scratch, &pl->counter, &pl->V0, &pl->Sbus, &pl->optr, &pl->opos, &pl->oval,
                       &pl->jfirst, &pl->jcount, &pl->Vout, &pl->iters, &pl->errs, &pl->Jout, &pl->cycles,
                       &pl->Vcase, &pl->casemap})
         b->release();
@@ -479,8 +497,34 @@ void release(pf_plan *pl) {
 // Launches the kernel for a batch whose device buffers are set up in `a` (no sync), with
 // the per-CTA slabs in `scratch` (`scratch_bytes` long) and the job counter at `counter`.
 // The number of CTAs is bounded by the slabs that fit in the scratch.
+// Whether a launch runs the batch-interleaved kernel: Newton plans, independent instances (no
+// chain), no per-launch diagnostics (J output, phase cycles or trace, LU reuse), and option
+// batch_layout 2 (auto keeps one CTA per instance, measured faster on every grid so far).
+bool use_tile(const pf_plan *pl, const l2g::BatchArgs &a) {
+    if (pl->P.dc || pl->P.fdpf || a.chain || a.Jout || a.phase_cycles || a.trace || a.reuse_below > 0) return false;
+    return pl->opt.batch_layout == 2;
+}
+
+int launch_tile(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, int *counter) {
+    const int lub = precision ? 4 : 8;
+    const size_t slab = l2g::tile_slab_bytes(pl->dp, lub);
+    const int grid = std::max(1, std::min(pl->num_sms, a.njobs));
+    cudaError_t e = pl->tile_scratch.ensure(slab * (size_t)grid);
+    if (e != cudaSuccess) return cuda_fail(e, "launch: batch-interleaved scratch allocation");
+    a.scratch = static_cast<unsigned char *>(pl->tile_scratch.p);
+    a.slab_bytes = (long long)slab;
+    a.job_counter = counter;
+    // spread the jobs over all CTAs: lanes per CTA
+    a.tile_lanes = std::max(1, std::min(32, (a.njobs + grid - 1) / grid));
+    e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
+    e = l2g::launch_nr_tile(pl->dp, a, precision, grid, st);
+    if (e != cudaSuccess) return cuda_fail(e, "launch: batch-interleaved kernel");
+    return 0;
+}
+
 int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, unsigned char *scratch,
-                size_t scratch_bytes, int *counter) {
+                size_t scratch_bytes, int *counter, bool allow_tile = false) {
     a.scratch = scratch;
     a.slab_bytes = (long long)pl->slab;
     a.job_counter = counter;
@@ -489,6 +533,7 @@ int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, u
     a.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
     a.reuse_below = lu_reuse_below(pl, a.refine_below);
     if (a.njobs <= 0) return 0;
+    if (allow_tile && use_tile(pl, a)) return launch_tile(pl, a, precision, st, counter);
     if (scratch_bytes < pl->slab) return fail(-1, "launch: the scratch memory holds no CTA slab");
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
@@ -531,7 +576,7 @@ int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, u
 
 int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
     return launch_into(pl, a, precision, st, static_cast<unsigned char *>(pl->scratch.p),
-                       pl->slab * (size_t)pl->grid, static_cast<int *>(pl->counter.p));
+                       pl->slab * (size_t)pl->grid, static_cast<int *>(pl->counter.p), true);
 }
 
 template <typename T>
@@ -1312,11 +1357,50 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
     auto scale = [&](std::vector<double> &v, const double *u) {
         for (int k = 0; k < m; ++k) v[k] = v[k] / u[P.dpos[k]];
     };
+    const std::vector<double> lu0 = lu, xs0 = xs;
     run(P.factor);
     for (int k = 0; k < m; ++k)
         if (lu[P.dpos[k]] == 0.0) return fail(l2g::SolverReFactor, "schedule check: zero pivot");
     run(P.backward);
     scale(xs, lu.data());
+    // the instance-interleaved batch programs (groups per warp, chunk after chunk) give the same
+    // bits: every written value sees its operations in the same order
+    {
+        std::vector<double> lt = lu0, xt = xs0;
+        auto run_tile = [&](const l2g::Plan::Program &pr, std::vector<double> &v) {
+            l2g::TileProgram tp;
+            l2g::build_tile_program(pr, l2g::kTileWarps, l2g::kTileChunk, tp);
+            for (size_t p = 0; p + 1 < tp.phase.size(); p += 2)
+                for (int w = 0; w < l2g::kTileWarps; ++w)
+                    for (int r = 0; r < tp.phase[p + 1]; ++r) {
+                        const size_t c = (size_t)tp.phase[p] + (size_t)r * l2g::kTileWarps + w;
+                        for (int q = 0; q < l2g::kTileChunk; ++q) {
+                            const int *o = &tp.ops[4 * (c * l2g::kTileChunk + q)];
+                            const int W = o[3] & 0x0fffffff, kind = (unsigned)o[3] >> 28;
+                            if (kind == 0) lt[o[0]] -= lt[o[1]] * (lt[o[2]] / lt[W]);
+                            else if (kind == 2) v[o[0]] -= lt[o[1]] * v[o[2]] / lt[W];
+                        }
+                    }
+        };
+        run_tile(P.factor, xt);
+        run_tile(P.backward, xt);
+        scale(xt, lt.data());
+        for (int k = 0; k < m; ++k)
+            if (xt[k] != xs[k]) return fail(-1, "schedule check: batch-interleaved programs disagree");
+        std::vector<double> y3(m, 0.0);
+        for (int f = 0; f < m; ++f) y3[P.pinv[f]] = b[f];
+        run_tile(P.forward, y3);
+        std::vector<double> y4(m, 0.0);
+        for (int f = 0; f < m; ++f) y4[P.pinv[f]] = b[f];
+        std::vector<double> lsave = lu;
+        lu = lt;
+        std::swap(xs, y4);
+        run(P.forward);
+        std::swap(xs, y4);
+        lu = lsave;
+        for (int k = 0; k < m; ++k)
+            if (y3[k] != y4[k]) return fail(-1, "schedule check: batch-interleaved forward program disagrees");
+    }
     if (!s0.empty()) {
         const int L = l2g::compact_lu_offset(m);
         run_packed(P.factor);

@@ -16,6 +16,7 @@
 // when they fit, else in the CTA's global slab (L2 resident).  The mixed form (FP32 LU)
 // refines every Newton step once against the FP64 Jacobian, computed on the fly from dS/dV.
 #include "pf_engine.cuh"
+#include "pf_device_math.cuh"
 
 #include <mutex>
 #include <set>
@@ -25,11 +26,7 @@ namespace l2g {
 
 namespace {
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
-__device__ __forceinline__ double cabs2(double2 a) { return sqrt(a.x * a.x + a.y * a.y); }
+
 
 struct Shared {
     double red[32];
@@ -94,26 +91,6 @@ __device__ __forceinline__ double2 ybus_value(const DevPlan &P, const Shared &S,
     return y;
 }
 
-// dS/dVa and dS/dVm of Ybus entry (r, c), as BaseNRAlgo::_dSbus_dV (BaseNRAlgo.tpp:228-257)
-__device__ __forceinline__ void dsbus(double2 y, double2 vr, double2 vc, bool diag, double2 ib, double &dvar,
-                                      double &dvai, double2 &dvm) {
-    const double ic = 1.0 / cabs2(vc);
-    const double2 vnc = make_double2(vc.x * ic, vc.y * ic);
-    double2 a = cmul(cconj(cmul(y, vnc)), vr);  // conj(Y * Vnorm_c) * V_r
-    double2 b = cmul(y, vc);                    // Y * V_c
-    if (diag) {
-        const double ir = 1.0 / cabs2(vr);
-        const double2 vnr = make_double2(vr.x * ir, vr.y * ir);
-        const double2 t = cmul(cconj(ib), vnr);
-        a.x += t.x;
-        a.y += t.y;
-        b.x -= ib.x;
-        b.y -= ib.y;
-    }
-    dvar = b.x * vr.y - b.y * vr.x;  // conj(-b) * (j V_r)
-    dvai = -(b.x * vr.x + b.y * vr.y);
-    dvm = a;
-}
 
 // (Ybus V)[r], over the row's entries in column order
 __device__ __forceinline__ double2 ybus_row_product(const DevPlan &P, const Shared &S, const double2 *__restrict__ V,
@@ -202,10 +179,7 @@ __device__ void jacobian_fill(const DevPlan &P, Shared &S, const double2 *__rest
     }
 }
 
-// a / b: correctly rounded in FP64; in FP32 (mixed form) the reciprocal-based quotient
-// (within 2 ulp), whose error the FP64-residual refinement of the Newton step absorbs
-__device__ __forceinline__ double lu_div(double a, double b) { return a / b; }
-__device__ __forceinline__ float lu_div(float a, float b) { return __fdividef(a, b); }
+
 
 template <typename LT, typename XT>
 __device__ __forceinline__ void run_op(const int4 o, LT *lu, XT *v) {
@@ -681,6 +655,8 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, cons
         for (int i = 0; i < kPhaseSlots; ++i) A0.phase_cycles[(size_t)blockIdx.x * kPhaseSlots + i] = pr.pc[i];
 }
 
+}  // namespace
+
 // Raises a kernel's dynamic shared-memory limit to everything the device allows, once per
 // kernel and device (launches then pass their own size; setting the attribute on every
 // launch would make concurrent launches on other streams wait on the driver).
@@ -703,6 +679,8 @@ cudaError_t allow_max_smem(const void *fn) {
     done.insert({fn, dev});
     return cudaSuccess;
 }
+
+namespace {
 
 // DC power flow of a batch (BaseDCAlgo::compute_pf, src/powerflow_algorithm/BaseDCAlgo.tpp:
 // 86-175), FP64, one CTA per instance: B from the real parts of the instance's Ybus (overrides

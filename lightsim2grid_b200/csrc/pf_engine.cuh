@@ -36,6 +36,10 @@ struct DevPlan {
     const int *dpos;         // pivot position per column (m)
     int dc, slack0;          // DC plan (B = Re(Ybus) without the slack) and its slack bus
     const double *luval;     // constant factor values (LU layout) of a fast-decoupled system
+    // the phase programs regrouped for the batch-interleaved kernel (TileProgram, pf_plan.hpp):
+    // operations (kind 7 padding) and, per phase, the first chunk and the number of rounds
+    const int4 *tfac_ops, *tbwd_ops, *tfwd_ops;
+    const int *tfac_phase, *tbwd_phase, *tfwd_phase;
 };
 
 // One batch launch.
@@ -70,6 +74,7 @@ struct BatchArgs {
     unsigned long long *trace;         // optional: CTA 0, first Newton iteration of its first
                                        // instance: clock after every phase of every program
     int trace_cap;
+    int tile_lanes;                    // batch-interleaved kernel: lanes (instances) per CTA
 };
 
 // One segment of a launch over several plans: a plan and its batch (device memory).
@@ -109,6 +114,16 @@ cudaError_t launch_scatter_case_rows(const double2 *src, const int *errs, const 
                                      double2 *dst, int num_sms, cudaStream_t st);
 // Resident CTAs per SM for a configuration (0 if it cannot launch).
 int nr_occupancy(int precision, bool lu_in_smem, bool refine, int threads, size_t smem);
+
+// Raises a kernel's dynamic shared-memory limit to the device's maximum (once per kernel and device).
+cudaError_t allow_max_smem(const void *fn);
+
+// Batch-interleaved Newton-Raphson (pf_tile.cu): 32 instances per CTA, one per lane, every value
+// stored as 32 consecutive per-instance values; one CTA of 512 threads per SM.  precision as
+// launch_nr_batch; A.scratch holds `grid` slabs of tile_slab_bytes; chain must be 0.
+cudaError_t launch_nr_tile(const DevPlan &P, const BatchArgs &A, int precision, int grid, cudaStream_t stream);
+size_t tile_slab_bytes(const DevPlan &P, int lu_bytes);
+size_t tile_smem_bytes(const DevPlan &P);
 
 // Fast decoupled power flow of a batch: P carries the Ybus rows, slack weights and bus maps,
 // B0 / B1 the substitution programs and constant factors of B' and B''.  lu_in_smem: both

@@ -179,6 +179,67 @@ void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out, int
     }
 }
 
+void build_tile_program(const Plan::Program &pr, int nwarps, int chunk, TileProgram &out) {
+    out.ops.clear();
+    out.phase.clear();
+    int nchunks = 0;
+    std::vector<int> idx;
+    std::vector<long long> key;
+    for (int p = 0; p < pr.nphases(); ++p) {
+        // the phase's operations in program order (slot after slot), padding dropped
+        idx.clear();
+        key.clear();
+        for (int k = pr.base[p]; k < pr.base[p + 1]; ++k) {
+            const unsigned kind = (unsigned)pr.ops[4 * (size_t)k + 3] >> 28;
+            if (kind == 7u) continue;
+            idx.push_back(k);
+            key.push_back(((long long)(kind == 0u ? 0 : 1) << 32) | (long long)pr.ops[4 * (size_t)k]);
+        }
+        const int n = (int)idx.size();
+        std::vector<int> ord(n);
+        for (int i = 0; i < n; ++i) ord[i] = i;
+        // a written value's operations sit on one slot in program order; the stable sort keeps
+        // that order inside each group
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return key[a] < key[b]; });
+        struct Group { int first, count; };
+        std::vector<Group> groups;
+        for (int i = 0; i < n;) {
+            int j = i;
+            while (j < n && key[ord[j]] == key[ord[i]]) ++j;
+            groups.push_back({i, j - i});
+            i = j;
+        }
+        std::stable_sort(groups.begin(), groups.end(), [](const Group &a, const Group &b) { return a.count > b.count; });
+        std::vector<std::vector<int>> per(nwarps);
+        std::vector<long long> load(nwarps, 0);
+        for (const Group &g : groups) {
+            int w = 0;
+            for (int t = 1; t < nwarps; ++t)
+                if (load[t] < load[w]) w = t;
+            for (int q = 0; q < g.count; ++q) per[w].push_back(idx[ord[g.first + q]]);
+            load[w] += g.count;
+        }
+        int rounds = 0;
+        for (auto &v : per) rounds = std::max(rounds, (int)((v.size() + chunk - 1) / chunk));
+        out.phase.push_back(nchunks);
+        out.phase.push_back(rounds);
+        for (int r = 0; r < rounds; ++r)
+            for (int w = 0; w < nwarps; ++w)
+                for (int c = 0; c < chunk; ++c) {
+                    const size_t q = (size_t)r * chunk + c;
+                    if (q < per[w].size()) {
+                        const int k = per[w][q];
+                        out.ops.insert(out.ops.end(), pr.ops.begin() + 4 * (size_t)k,
+                                       pr.ops.begin() + 4 * (size_t)k + 4);
+                    } else {
+                        const int none[4] = {0, 0, 0, 7 << 28};
+                        out.ops.insert(out.ops.end(), none, none + 4);
+                    }
+                }
+        nchunks += rounds * nwarps;
+    }
+}
+
 void fdpf_lu_offsets(const Plan &P, int &off0, int &off1, bool &fits) {
     const int x = std::max(compact_lu_offset(P.sub[0].m), compact_lu_offset(P.sub[1].m));
     off0 = x;

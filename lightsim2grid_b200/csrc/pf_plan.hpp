@@ -151,6 +151,20 @@ void fdpf_lu_offsets(const Plan &P, int &off0, int &off1, bool &fits);
 int build_dc_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, const int *slack_ids, int nslack,
                   const int *pv, int npv, const int *pq, int npq, const PlanOptions &opt, std::string &msg);
 
+// A phase program regrouped for the instance-interleaved batch kernel, where every operation
+// is run by a whole warp on 32 instances at once.  The operations of a phase are grouped by the
+// value they write (a group keeps its order), groups are bin-packed onto `nwarps` warps (a warp
+// runs whole groups, so no two warps write one value), and each warp's list is cut into chunks
+// of `chunk` operations: chunk (round r, warp w) of phase p is chunk number phase[2p] + r *
+// nwarps + w, `phase[2p+1]` rounds in all; padding operations have kind 7.
+constexpr int kTileWarps = 16;  // warps of the batch-interleaved kernel (512 threads)
+constexpr int kTileChunk = 8;   // operations per warp chunk
+struct TileProgram {
+    std::vector<int> ops;    // 4 ints per operation, as Plan::Program
+    std::vector<int> phase;  // 2 per phase: first chunk, rounds
+};
+void build_tile_program(const Plan::Program &pr, int nwarps, int chunk, TileProgram &out);
+
 // A real sparse matrix, CSC (n x n, canonical).
 struct RealCsc {
     const int *p, *i;

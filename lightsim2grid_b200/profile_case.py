@@ -32,6 +32,7 @@ def main():
     ap.add_argument("--dc", action="store_true", help="DC power flows (DC Ybus, DC outage coefficients)")
     ap.add_argument("--fdpf", type=int, default=-1, help="fast decoupled power flows: 0 XB, 1 BX (-1: Newton)")
     ap.add_argument("--max-iter", type=int, default=10)
+    ap.add_argument("--batch-layout", type=int, default=0, help="0 auto, 1 one CTA per instance, 2 batch-interleaved")
     args = ap.parse_args()
 
     import torch
@@ -52,7 +53,8 @@ def main():
     fdpf = g.get_Bp_Bpp(args.fdpf) if args.fdpf >= 0 else None
     plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, dc=args.dc, fdpf=fdpf, threads=args.threads,
                 lu_placement=args.lu_placement, fuse_forward=args.fuse_forward, max_ctas_per_sm=args.ctas_per_sm,
-                refine=args.refine, refine_threshold=args.refine_threshold, lu_reuse_threshold=args.lu_reuse)
+                refine=args.refine, refine_threshold=args.refine_threshold, lu_reuse_threshold=args.lu_reuse,
+                batch_layout=args.batch_layout)
     lib = plan._lib
     cp = np.zeros(nb + 1, np.int32)
     rows, cols, vals = [], [], []
