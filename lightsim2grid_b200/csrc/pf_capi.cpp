@@ -298,6 +298,13 @@ int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl,
         l2g::build_tile_program(P.factor, l2g::kTileWarps, l2g::kTileChunk, tf);
         l2g::build_tile_program(P.backward, l2g::kTileWarps, l2g::kTileChunk, tb);
         l2g::build_tile_program(P.forward, l2g::kTileWarps, l2g::kTileChunk, tw);
+        // padding becomes an update of the scratch LU row nnzLU (the kernel has no branch on it)
+        for (l2g::TileProgram *t : {&tf, &tb, &tw})
+            for (size_t o = 0; o < t->ops.size(); o += 4)
+                if (((unsigned)t->ops[o + 3] >> 28) == 7u) {
+                    t->ops[o] = t->ops[o + 1] = t->ops[o + 2] = P.nnzLU;
+                    t->ops[o + 3] = P.nnzLU;
+                }
     }
     size_t otfo = push(bi, tf.ops), otbo = push(bi, tb.ops), otwo = push(bi, tw.ops);
     size_t otfp = push(bi, tf.phase), otbp = push(bi, tb.phase), otwp = push(bi, tw.phase);

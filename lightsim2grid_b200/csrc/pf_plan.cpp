@@ -209,15 +209,24 @@ void build_tile_program(const Plan::Program &pr, int nwarps, int chunk, TileProg
             groups.push_back({i, j - i});
             i = j;
         }
-        std::stable_sort(groups.begin(), groups.end(), [](const Group &a, const Group &b) { return a.count > b.count; });
+        // operand locality: groups ordered by the pivot and the U entry of their first operation
+        // (consecutive groups then share the pivot, the U entry or the pivot's L column), and cut
+        // into nwarps contiguous runs of about equal operation counts
+        auto okey = [&](const Group &g) {
+            const int *o = &pr.ops[4 * (size_t)idx[ord[g.first]]];
+            return std::make_pair((long long)(o[3] & 0x0fffffff), ((long long)o[2] << 32) | (unsigned)o[1]);
+        };
+        std::stable_sort(groups.begin(), groups.end(), [&](const Group &a, const Group &b) { return okey(a) < okey(b); });
         std::vector<std::vector<int>> per(nwarps);
-        std::vector<long long> load(nwarps, 0);
-        for (const Group &g : groups) {
+        {
+            long long done = 0;
             int w = 0;
-            for (int t = 1; t < nwarps; ++t)
-                if (load[t] < load[w]) w = t;
-            for (int q = 0; q < g.count; ++q) per[w].push_back(idx[ord[g.first + q]]);
-            load[w] += g.count;
+            for (const Group &g : groups) {
+                // move to the next warp once this one holds its share of the phase's operations
+                while (w < nwarps - 1 && done >= (long long)n * (w + 1) / nwarps) ++w;
+                for (int q = 0; q < g.count; ++q) per[w].push_back(idx[ord[g.first + q]]);
+                done += g.count;
+            }
         }
         int rounds = 0;
         for (auto &v : per) rounds = std::max(rounds, (int)((v.size() + chunk - 1) / chunk));

@@ -157,8 +157,8 @@ int build_dc_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, 
 // runs whole groups, so no two warps write one value), and each warp's list is cut into chunks
 // of `chunk` operations: chunk (round r, warp w) of phase p is chunk number phase[2p] + r *
 // nwarps + w, `phase[2p+1]` rounds in all; padding operations have kind 7.
-constexpr int kTileWarps = 16;  // warps of the batch-interleaved kernel (512 threads)
-constexpr int kTileChunk = 8;   // operations per warp chunk
+constexpr int kTileWarps = 32;  // warps of the batch-interleaved kernel (1024 threads)
+constexpr int kTileChunk = 4;   // operations per warp chunk
 struct TileProgram {
     std::vector<int> ops;    // 4 ints per operation, as Plan::Program
     std::vector<int> phase;  // 2 per phase: first chunk, rounds

@@ -25,7 +25,7 @@ namespace {
 
 constexpr int kLanes = 32;
 constexpr int kW = kTileWarps;
-static_assert(kW * kLanes == 512, "the batch-interleaved kernel runs 512 threads");
+static_assert(kW * kLanes == 1024, "the batch-interleaved kernel runs 1024 threads");
 
 enum : int { kFree = 0, kNew = 1, kStep = 2, kDone = 3, kIdle = 4 };
 
@@ -40,7 +40,8 @@ struct TileLanes {
     int nactive, nstep, nrefine;
 };
 
-__device__ __forceinline__ size_t ix(int i, int lane) { return (size_t)i * kLanes + lane; }
+// 32-bit offsets: every slab array has fewer than 2^27 rows
+__device__ __forceinline__ unsigned ix(int i, int lane) { return ((unsigned)i << 5) | (unsigned)lane; }
 
 __host__ __device__ __forceinline__ size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -52,9 +53,10 @@ __device__ __forceinline__ double2 ybus_lane(const DevPlan &P, const TileLanes &
     return y;
 }
 
-// One chunk of a warp: up to kTileChunk operations, consecutive ones writing one value forming a
-// group.  Operands are loaded first (they are final in this phase), then each group accumulates
-// in a register and is stored once.
+// One chunk of a warp: kTileChunk operations, consecutive ones writing one value forming a
+// group.  All operands are loaded first (they are final in this phase), then each group
+// accumulates in a register and is stored once.  Kinds are 0 (LU update) and 2 (substitution
+// push); padding was turned into updates of a per-lane scratch row, so there is no branch.
 template <typename LT>
 __device__ __forceinline__ void tile_chunk(const int4 *__restrict__ c, LT *lu, LT *x, int lane) {
     int4 o[kTileChunk];
@@ -63,34 +65,24 @@ __device__ __forceinline__ void tile_chunk(const int4 *__restrict__ c, LT *lu, L
     LT a[kTileChunk], b[kTileChunk], d[kTileChunk], t[kTileChunk];
 #pragma unroll
     for (int i = 0; i < kTileChunk; ++i) {
-        const unsigned kind = (unsigned)o[i].w >> 28;
-        a[i] = b[i] = d[i] = t[i] = (LT)0;
-        if (kind == 7u) continue;
-        const int w = o[i].w & 0x0fffffff;
+        const bool push = ((unsigned)o[i].w >> 28) != 0u;
+        const LT *vsrc = push ? x : lu;
         a[i] = lu[ix(o[i].y, lane)];
-        d[i] = lu[ix(w, lane)];
-        b[i] = kind == 0u ? lu[ix(o[i].z, lane)] : x[ix(o[i].z, lane)];
-        const bool first = i == 0 || o[i].x != o[i - 1].x || ((unsigned)o[i - 1].w >> 28) != kind;
-        if (first) t[i] = kind == 0u ? lu[ix(o[i].x, lane)] : x[ix(o[i].x, lane)];
+        d[i] = lu[ix(o[i].w & 0x0fffffff, lane)];
+        b[i] = vsrc[ix(o[i].z, lane)];
+        const bool first = i == 0 || o[i].x != o[i - 1].x || o[i].w >> 28 != o[i - 1].w >> 28;
+        t[i] = first ? vsrc[ix(o[i].x, lane)] : (LT)0;
     }
     LT acc = (LT)0;
 #pragma unroll
     for (int i = 0; i < kTileChunk; ++i) {
-        const unsigned kind = (unsigned)o[i].w >> 28;
-        if (kind == 7u) continue;
-        const bool first = i == 0 || o[i].x != o[i - 1].x || ((unsigned)o[i - 1].w >> 28) != kind;
+        const bool push = ((unsigned)o[i].w >> 28) != 0u;
+        const bool first = i == 0 || o[i].x != o[i - 1].x || o[i].w >> 28 != o[i - 1].w >> 28;
         if (first) acc = t[i];
-        if (kind == 0u)
-            acc -= a[i] * lu_div(b[i], d[i]);  // LU update by an undivided L entry
-        else
-            acc -= lu_div(a[i] * b[i], d[i]);  // substitution push
-        const bool last = i == kTileChunk - 1 || o[i + 1].x != o[i].x || ((unsigned)o[i + 1].w >> 28) != kind;
-        if (last) {
-            if (kind == 0u)
-                lu[ix(o[i].x, lane)] = acc;
-            else
-                x[ix(o[i].x, lane)] = acc;
-        }
+        // LU update by an undivided L entry, or substitution push
+        acc -= push ? lu_div(a[i] * b[i], d[i]) : a[i] * lu_div(b[i], d[i]);
+        const bool last = i == kTileChunk - 1 || o[i + 1].x != o[i].x || o[i + 1].w >> 28 != o[i].w >> 28;
+        if (last) (push ? x : lu)[ix(o[i].x, lane)] = acc;
     }
 }
 
@@ -109,7 +101,7 @@ __device__ void tile_program(const int4 *__restrict__ ops, const int2 *ph, int n
 }
 
 template <typename LT, bool REFINE>
-__global__ void __launch_bounds__(512, 1) nr_tile_kernel(const DevPlan P, const BatchArgs A) {
+__global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const BatchArgs A) {
     extern __shared__ __align__(16) int tdyn[];
     __shared__ TileLanes S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -121,8 +113,8 @@ __global__ void __launch_bounds__(512, 1) nr_tile_kernel(const DevPlan P, const 
     for (int i = tid; i < P.bwd_nph; i += blockDim.x) phb[i] = make_int2(P.tbwd_phase[2 * i], P.tbwd_phase[2 * i + 1]);
     for (int i = tid; i < P.fwd_nph; i += blockDim.x) phw[i] = make_int2(P.tfwd_phase[2 * i], P.tfwd_phase[2 * i + 1]);
     unsigned char *q = A.scratch + (size_t)blockIdx.x * (size_t)A.slab_bytes;
-    LT *lu = reinterpret_cast<LT *>(q);
-    q += al256((size_t)P.nnzLU * kLanes * sizeof(LT));
+    LT *lu = reinterpret_cast<LT *>(q);  // nnzLU rows and a scratch row for padding operations
+    q += al256((size_t)(P.nnzLU + 1) * kLanes * sizeof(LT));
     LT *x = reinterpret_cast<LT *>(q);
     q += al256((size_t)m * kLanes * sizeof(LT));
     double *dxg = reinterpret_cast<double *>(q);
@@ -445,7 +437,7 @@ cudaError_t launch_tile_variant(const DevPlan &P, const BatchArgs &A, int grid, 
 
 size_t tile_slab_bytes(const DevPlan &P, int lu_bytes) {
     const size_t L = kLanes;
-    return al256((size_t)P.nnzLU * L * lu_bytes) + al256((size_t)P.m * L * lu_bytes) + al256((size_t)P.m * L * 8) +
+    return al256((size_t)(P.nnzLU + 1) * L * lu_bytes) + al256((size_t)P.m * L * lu_bytes) + al256((size_t)P.m * L * 8) +
            3 * al256((size_t)P.n * L * 16) + 2 * al256((size_t)P.n * L * 8);
 }
 
