@@ -147,6 +147,16 @@ int pf_solve(pf_plan *plan, const double *V0_ri, const double *Sbus_ri, int max_
    the number of entries (returned).  Replaces get_J_python (src/main.cpp:230). */
 int pf_get_J(pf_plan *plan, int *m, int *Jp, int *Ji, double *Jx);
 
+/* Job order for an N-1 batch prepared by pf_n1_prepare (ninst solvable instances, their
+   overrides ovr_ptr / ovr_pos / ovr_val_ri): instance indices by decreasing power mismatch of the
+   outage at the start voltages, max over buses of |V_r conj(sum dY_rc V_c)|, a predictor of the
+   iterations an instance takes.  Passing this order as the job list of a device batch starts the
+   long instances first, so they do not extend the end of the launch (results do not depend on
+   the order).  No counterpart in the reference (it solves the cases one after the other);
+   pf_batch_n1 uses it for its own jobs. */
+int pf_n1_order(const pf_plan *plan, int ninst, const int *ovr_ptr, const int *ovr_pos, const double *ovr_val_ri,
+                const double *V0_ri, int *order);
+
 /* N-1 / N-k batch: ContingencyAnalysis::compute (src/batch_algorithm/ContingencyAnalysis.cpp:166-233)
    after the base power flow.  Case c removes coef_{row,col,val}[case_ptr[c] .. case_ptr[c+1])
    from Ybus (entries must exist in the pattern).  Islanded cases (check_invertible,

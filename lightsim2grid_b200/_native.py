@@ -73,7 +73,7 @@ SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_g
            "pf_scratch_bytes", "pf_multi_create", "pf_multi_launch", "pf_multi_info", "pf_multi_destroy",
            "pf_flows_device", "pf_flows_host", "pf_ybus_positions", "pf_assemble_ybus_device",
            "pf_set_ybus_values_device", "pf_assemble_sbus_device", "pf_dc_plan_create", "pf_server_create",
-           "pf_server_submit", "pf_server_poll", "pf_server_state", "pf_server_destroy", "pf_fdpf_plan_create")
+           "pf_server_submit", "pf_server_poll", "pf_server_state", "pf_server_destroy", "pf_fdpf_plan_create", "pf_n1_order")
 
 
 def load(path=None):
@@ -156,6 +156,8 @@ def load(path=None):
     lib.pf_dc_plan_create.restype = ctypes.c_int
     lib.pf_dc_plan_create.argtypes = [ctypes.c_int, i32p, i32p, f64p, i32p, ctypes.c_int, i32p, ctypes.c_int, i32p,
                                       ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    lib.pf_n1_order.restype = ctypes.c_int
+    lib.pf_n1_order.argtypes = [ctypes.c_void_p, ctypes.c_int, i32p, i32p, f64p, f64p, i32p]
     lib.pf_fdpf_plan_create.restype = ctypes.c_int
     lib.pf_fdpf_plan_create.argtypes = [ctypes.c_int, i32p, i32p, f64p, i32p, i32p, f64p, i32p, i32p, f64p, i32p,
                                         ctypes.c_int, f64p, i32p, ctypes.c_int, i32p, ctypes.c_int, ctypes.c_void_p,

@@ -32,6 +32,7 @@ def main():
     ap.add_argument("--dc", action="store_true", help="DC power flows (DC Ybus, DC outage coefficients)")
     ap.add_argument("--fdpf", type=int, default=-1, help="fast decoupled power flows: 0 XB, 1 BX (-1: Newton)")
     ap.add_argument("--max-iter", type=int, default=10)
+    ap.add_argument("--order", action="store_true", help="also time hardest-first job orders")
     ap.add_argument("--batch-layout", type=int, default=0, help="0 auto, 1 one CTA per instance, 2 batch-interleaved")
     args = ap.parse_args()
 
@@ -98,6 +99,35 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
+    order_times = {}
+    if args.order:
+        # job orders: by the iterations each instance took (ideal), and by the outage's power
+        # mismatch at the start voltages (|V o conj(dY V)|, known before solving)
+        it0 = bufs[8].cpu().numpy().copy()
+        er0 = bufs[9].cpu().numpy().copy()
+        sol = np.nonzero(solv)[0]
+        dS = np.zeros(ns)
+        for i, cidx in enumerate(sol):
+            acc = {}
+            for (r, cc, y) in coeffs[cidx]:
+                acc[r] = acc.get(r, 0) + Vn[r] * np.conj(y * Vn[cc])
+            dS[i] = max(abs(v) for v in acc.values()) if acc else 0.0
+        for label, key in (("by_iterations", -(it0 + 100 * (er0 != 0))), ("by_mismatch", -dS)):
+            order = np.argsort(key, kind="stable").astype(np.int32)
+            bufs[5].copy_(torch.from_numpy(order).to(dev))
+            for _ in range(args.warmup):
+                assert lib.pf_batch_device(plan.handle, nat.ctypes.byref(b), stream.cuda_stream) == 0
+            ts = []
+            for _ in range(args.repeat):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                assert lib.pf_batch_device(plan.handle, nat.ctypes.byref(b), stream.cuda_stream) == 0
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            order_times[label] = ts
+            assert np.array_equal(bufs[8].cpu().numpy(), it0) and np.array_equal(bufs[9].cpu().numpy(), er0)
+        bufs[5].copy_(torch.from_numpy(np.arange(ns, dtype=np.int32)).to(dev))
     cyc = np.zeros(8)
     assert lib.pf_batch_device_phase_cycles(plan.handle, nat.ctypes.byref(b), stream.cuda_stream,
                                             nat.ptr(cyc, nat.f64p)) == 0, nat.last_error(lib)
@@ -132,7 +162,8 @@ def main():
         check = {"flags_equal": bool(np.array_equal(er == 0, ef == 0)),
                  "max_abs_dV_vs_fp64": float(np.abs(Vm[both] - Vr[both]).max()) if both.any() else None,
                  "iterations_fp64": int(itf.cpu().numpy().sum())}
-    out = {"grid": args.grid, "cases": ns, "precision": args.precision, "ms": times, "check": check,
+    out = {"grid": args.grid, "cases": ns, "precision": args.precision, "ms": times, "ms_ordered": order_times,
+           "check": check,
            "converged": int((er == 0).sum()), "iterations": int(it.sum()),
            "pf_per_s": float((er == 0).sum() / (np.mean(times) * 1e-3)),
            "cycles_per_iteration_per_cta": float(tot / max(1, int(it.sum()))) if tot > 0 else None,

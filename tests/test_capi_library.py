@@ -36,3 +36,12 @@ def test_missing_library_fails_loudly(tmp_path):
 
     with pytest.raises(ImportError):
         _native.load(str(tmp_path / "nope.so"))
+
+
+
+def test_n1_order_rejects_null_arguments():
+    """pf_n1_order validates its arguments before touching a plan (no GPU needed)."""
+    from lightsim2grid_b200 import _native as nat
+
+    lib = nat.load()
+    assert lib.pf_n1_order(None, 0, None, None, None, None, None) != 0

@@ -267,3 +267,50 @@ def test_device_batch_matches_host_batch():
     ok = conv[idx]
     assert np.array_equal(der.cpu().numpy() == 0, ok)
     assert np.array_equal(Vd[ok], V[idx[ok]])
+
+
+def test_n1_order_is_hardest_first():
+    """pf_n1_order: a permutation of the solvable instances by decreasing power mismatch of the
+    outage at V0 (restated here with numpy); device batches in that order give the same results."""
+    from lightsim2grid_b200 import Plan, _native as nat
+
+    c = grid_problem("grid118")
+    g = c["grid"]
+    coeffs = _n1(c)
+    plan = Plan(c["Ybus"], c["V0"], c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=0)
+    lib = plan._lib
+    cp = np.zeros(len(coeffs) + 1, np.int32)
+    rows, cols, vals = [], [], []
+    for k, lst in enumerate(coeffs):
+        cp[k + 1] = cp[k] + len(lst)
+        for (r, cc, y) in lst:
+            rows.append(r)
+            cols.append(cc)
+            vals.append(y)
+    rows, cols, vals = nat.as_i32(rows), nat.as_i32(cols), nat.as_c128(vals).ravel()
+    solv = np.zeros(len(coeffs), np.int32)
+    optr = np.zeros(len(coeffs) + 1, np.int32)
+    opos = np.zeros(cp[-1], np.int32)
+    oval = np.zeros(cp[-1], np.complex128)
+    w = lib.pf_n1_prepare(plan.handle, len(coeffs), nat.ptr(cp, nat.i32p), nat.ptr(rows, nat.i32p),
+                          nat.ptr(cols, nat.i32p), nat.cptr(vals), nat.ptr(solv, nat.i32p), nat.ptr(optr, nat.i32p),
+                          nat.ptr(opos, nat.i32p), nat.cptr(oval), int(cp[-1]))
+    ns = int(solv.sum())
+    V0 = nat.as_c128(c["V0"]).ravel()
+    order = np.zeros(ns, np.int32)
+    assert lib.pf_n1_order(plan.handle, ns, nat.ptr(optr, nat.i32p), nat.ptr(opos, nat.i32p), nat.cptr(oval),
+                           nat.cptr(V0), nat.ptr(order, nat.i32p)) == 0
+    assert np.array_equal(np.sort(order), np.arange(ns))
+    # the score restated: dS_r = V_r conj(sum dY_rc V_c) over the instance's changed entries
+    Yc = c["Ybus"].tocsr()
+    Yc.sort_indices()
+    r_of = np.repeat(np.arange(Yc.shape[0]), np.diff(Yc.indptr))
+    score = np.zeros(ns)
+    for i in range(ns):
+        acc = {}
+        for k in range(optr[i], optr[i + 1]):
+            p = opos[k]
+            r, cc = r_of[p], Yc.indices[p]
+            acc[r] = acc.get(r, 0) + (oval[k] - Yc.data[p]) * V0[cc]
+        score[i] = max(abs(V0[r] * np.conj(v)) for r, v in acc.items())
+    assert np.all(np.diff(score[order]) <= 1e-12 * max(1.0, score.max()))
