@@ -27,8 +27,9 @@ typedef struct pf_options {
     int fuse_forward;       /* forward substitution fused into the refactorisation program.
                                0: default (on), 1: on, 2: off                                  */
     double pivot_threshold; /* diagonal preference of the first factorisation; 0: 1e-3      */
-    int fp64_fallback;      /* mixed form: re-run instances that did not converge in FP64.
-                               0: default (on), 1: on, 2: off                                  */
+    int fp64_fallback;      /* mixed form: re-run instances that did not converge in FP64
+                               (inside the launch on the plan's own scratch, else by a second
+                               launch).  0: default (on), 1: on, 2: off                         */
     int max_ctas_per_sm;    /* cap on resident CTAs per SM; 0: occupancy limit               */
     int refine;             /* mixed form: refine Newton steps once against the FP64
                                Jacobian.  0: default (on), 1: on, 2: off                       */
@@ -161,7 +162,10 @@ int pf_n1_order(const pf_plan *plan, int ninst, const int *ovr_ptr, const int *o
    after the base power flow.  Case c removes coef_{row,col,val}[case_ptr[c] .. case_ptr[c+1])
    from Ybus (entries must exist in the pattern).  Islanded cases (check_invertible,
    ContingencyAnalysis.cpp:14-45) are skipped: err = SingularMatrix, V row 0.  Every other case
-   starts from V0.  V_out is ncases x n complex, zero for cases that did not converge. */
+   starts from V0.  V_out is ncases x n complex, zero for cases that did not converge.  When V_out
+   is pinned host memory mapped into the device address space (cudaHostAlloc, which unified
+   addressing maps), the kernel writes the rows straight into it as the cases finish; otherwise
+   the rows are copied after the kernel. */
 int pf_batch_n1(pf_plan *plan, int ncases, const int *case_ptr, const int *coef_row, const int *coef_col,
                 const double *coef_val_ri, const double *V0_ri, const double *Sbus_ri, int max_iter, double tol,
                 double *V_out_ri, int *converged, int *iters, int *errs);

@@ -70,6 +70,10 @@ struct pf_plan {
     int ctas_per_sm = 1;
     int grid = 1;
     size_t slab = 0, smem = 0;
+    // mixed form: FP64 fallback inside launches on the plan's own scratch (slab and shared
+    // memory sized for it), and whether the last launch ran it
+    bool inline_fb = false, last_inline = false;
+    size_t slab_fb = 0, smem_fb = 0;
     // device structure
     void *d_int = nullptr;
     void *d_dbl = nullptr;
@@ -443,6 +447,9 @@ int configure(pf_plan *pl) {
         pl->lu_in_smem = pl->opt.lu_placement == 2 ? false : fits;
         pl->smem = pl->lu_in_smem ? sm_in : sm_out;
         pl->slab = l2g::fdpf_slab_bytes(pl->dp);
+        pl->slab_fb = pl->slab;
+        pl->smem_fb = pl->smem;
+        pl->inline_fb = false;
         const int want = pl->opt.max_ctas_per_sm;
         int occ = l2g::fdpf_occupancy(pl->lu_in_smem, thr, want > 0 ? want : 8, pl->smem);
         if (occ <= 0) return fail(-1, "pf_plan_create: the kernel cannot be launched with this configuration");
@@ -472,7 +479,21 @@ int configure(pf_plan *pl) {
     if (pl->opt.max_ctas_per_sm > 0) occ = std::min(occ, pl->opt.max_ctas_per_sm);
     pl->ctas_per_sm = occ;
     pl->grid = pl->num_sms * occ;
-    e = pl->scratch.ensure(pl->slab * (size_t)pl->grid);
+    // mixed form with refinement: the FP64 fallback runs inside launches on the plan's own
+    // scratch, whose slabs then also hold an FP64 LU and whose shared memory an FP64 solve vector
+    pl->slab_fb = pl->slab;
+    pl->smem_fb = pl->smem;
+    pl->inline_fb = false;
+    if (pl->precision == 1 && pl->refine && pl->opt.fp64_fallback != 2) {
+        const size_t sfb = std::max(pl->smem, l2g::smem_bytes(pl->dp, 8, 8, false));
+        if (sfb + static_smem <= (size_t)optin &&
+            l2g::nr_occupancy(pl->precision, pl->lu_in_smem, pl->refine, thr, sfb) >= pl->ctas_per_sm) {
+            pl->inline_fb = true;
+            pl->smem_fb = sfb;
+            pl->slab_fb = std::max(pl->slab, l2g::slab_bytes(pl->dp, 8, false));
+        }
+    }
+    e = pl->scratch.ensure(pl->slab_fb * (size_t)pl->grid);
     if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: scratch allocation");
     e = pl->counter.ensure(256);
     if (e != cudaSuccess) return cuda_fail(e, "pf_plan_create: counter allocation");
@@ -539,8 +560,23 @@ int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, u
     a.refine = (precision == 1 && pl->refine) ? 1 : 0;
     a.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
     a.reuse_below = lu_reuse_below(pl, a.refine_below);
+    pl->last_inline = false;
     if (a.njobs <= 0) return 0;
     if (allow_tile && use_tile(pl, a)) return launch_tile(pl, a, precision, st, counter);
+    if (allow_tile && pl->inline_fb && precision == pl->precision && a.refine && !pl->P.dc && !pl->P.fdpf) {
+        // the plan's own scratch: FP64 fallback inside the launch
+        a.fp64_inline = 1;
+        a.slab_bytes = (long long)pl->slab_fb;
+        cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+        if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
+        int grid = std::min(pl->grid, a.njobs);
+        grid = std::min<long long>(grid, (long long)(scratch_bytes / pl->slab_fb));
+        if (grid <= 0) return fail(-1, "launch: the scratch memory holds no CTA slab");
+        e = l2g::launch_nr_batch(pl->dp, a, precision, pl->threads, grid, pl->smem_fb, st);
+        if (e != cudaSuccess) return cuda_fail(e, "launch: kernel");
+        pl->last_inline = true;
+        return 0;
+    }
     if (scratch_bytes < pl->slab) return fail(-1, "launch: the scratch memory holds no CTA slab");
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
@@ -583,7 +619,7 @@ int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, u
 
 int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
     return launch_into(pl, a, precision, st, static_cast<unsigned char *>(pl->scratch.p),
-                       pl->slab * (size_t)pl->grid, static_cast<int *>(pl->counter.p), true);
+                       pl->slab_fb * (size_t)pl->grid, static_cast<int *>(pl->counter.p), true);
 }
 
 template <typename T>
@@ -595,11 +631,21 @@ cudaError_t h2d(DevBuf &b, const T *src, size_t count, cudaStream_t st) {
 
 // runs instances [0, n_inst) described by host arrays; results into host arrays.
 // V0: shared (v0_stride 0) or per instance; Sbus likewise.
+// Where a batch writes its voltage rows when not into the plan's device buffer: `vout` (device
+// address, e.g. of mapped host memory), row `rows[i]` for instance i, zero rows for instances
+// that did not converge; `during` runs on the host while the kernel runs.
+struct RowsOut {
+    double2 *vout = nullptr;
+    const int *rows = nullptr;
+    const std::function<void()> *during = nullptr;
+};
+
 int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, const cplx *Sbus, long long sbus_stride,
               const std::vector<int> &optr, const std::vector<int> &opos, const std::vector<cplx> &oval,
               const std::vector<int> &jfirst, const std::vector<int> &jcount, int chain, int max_iter, double tol,
               cplx *Vout, int *iters, int *errs, bool want_J,
-              const std::function<int(const std::vector<char> &)> *settled = nullptr) {
+              const std::function<int(const std::vector<char> &)> *settled = nullptr,
+              const RowsOut *rows_out = nullptr) {
     const int n = pl->P.n;
     cudaStream_t st = pl->stream;
     double t0 = now();
@@ -616,7 +662,8 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
     }
     if ((e = h2d(pl->jfirst, jfirst.data(), jfirst.size(), st)) != cudaSuccess) return cuda_fail(e, "batch: upload");
     if ((e = h2d(pl->jcount, jcount.data(), jcount.size(), st)) != cudaSuccess) return cuda_fail(e, "batch: upload");
-    if ((e = pl->Vout.ensure((size_t)n_inst * n * sizeof(cplx))) != cudaSuccess) return cuda_fail(e, "batch: alloc");
+    if (!rows_out && (e = pl->Vout.ensure((size_t)n_inst * n * sizeof(cplx))) != cudaSuccess)
+        return cuda_fail(e, "batch: alloc");
     if ((e = pl->iters.ensure((size_t)n_inst * sizeof(int))) != cudaSuccess) return cuda_fail(e, "batch: alloc");
     if ((e = pl->errs.ensure((size_t)n_inst * sizeof(int))) != cudaSuccess) return cuda_fail(e, "batch: alloc");
     if (want_J && (e = pl->Jout.ensure(pl->P.Ji.size() * sizeof(double))) != cudaSuccess)
@@ -637,7 +684,11 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
     a.job_count = static_cast<const int *>(pl->jcount.p);
     a.njobs = (int)jfirst.size();
     a.chain = chain;
-    a.Vout = static_cast<double2 *>(pl->Vout.p);
+    a.Vout = rows_out ? rows_out->vout : static_cast<double2 *>(pl->Vout.p);
+    if (rows_out) {
+        a.vout_row = rows_out->rows;
+        a.zero_failed = 1;
+    }
     a.iters = static_cast<int *>(pl->iters.p);
     a.errs = static_cast<int *>(pl->errs.p);
     a.Jout = want_J ? static_cast<double *>(pl->Jout.p) : nullptr;
@@ -646,6 +697,8 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
     int rc = launch(pl, a, pl->precision, st);
     if (rc) return rc;
     cudaEventRecord(pl->ev1, st);
+    // host work that overlaps the kernel (before any copy that would wait for it)
+    if (rows_out && rows_out->during) (*rows_out->during)();
     if ((e = cudaMemcpyAsync(iters, pl->iters.p, (size_t)n_inst * sizeof(int), cudaMemcpyDeviceToHost, st)) !=
         cudaSuccess)
         return cuda_fail(e, "batch: download");
@@ -662,7 +715,7 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
     int rerun = 0;
     std::vector<char> again;
     if (settled) again.assign((size_t)n_inst, 0);
-    if (pl->precision == 1 && pl->opt.fp64_fallback != 2) {
+    if (pl->precision == 1 && pl->opt.fp64_fallback != 2 && !pl->last_inline) {
         std::vector<int> rf, rc2;
         for (size_t j = 0; j < jfirst.size(); ++j) {
             bool bad = false;
@@ -1115,9 +1168,50 @@ int pf_batch_n1(pf_plan *pl, int ncases, const int *case_ptr, const int *coef_ro
     std::vector<int> it(std::max(ns, 1)), er(std::max(ns, 1));
     double t1 = now();
     cplx *Vo = reinterpret_cast<cplx *>(V_out_ri);
-    // result rows in case order on the device, then one copy into the caller's array, on the copy
-    // stream: issued as soon as the rows are final, so the copy overlaps the FP64 re-run of the
-    // instances that failed in the mixed form; their rows follow once the re-run is done
+    // voltage rows straight into the caller's array when it is pinned and mapped into the device
+    // address space: each instance's row is written (over the host link) as it finishes, the
+    // islanded rows are zeroed on the host while the kernel runs, and nothing is copied after it
+    {
+        cudaPointerAttributes at{};
+        const bool mapped = cudaPointerGetAttributes(&at, V_out_ri) == cudaSuccess &&
+                            at.type == cudaMemoryTypeHost && at.devicePointer != nullptr;
+        if (!mapped) cudaGetLastError();  // pageable memory: not an error
+        if (mapped && ns > 0) {
+            cudaError_t e = pl->casemap.ensure((size_t)ns * sizeof(int));
+            if (e != cudaSuccess) return cuda_fail(e, "pf_batch_n1: alloc");
+            e = cudaMemcpy(pl->casemap.p, idx.data(), (size_t)ns * sizeof(int), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return cuda_fail(e, "pf_batch_n1: upload");
+            const std::function<void()> zero_islanded = [&]() {
+                for (int c = 0; c < ncases; ++c)
+                    if (!solv[c]) std::memset(Vo + (size_t)c * n, 0, (size_t)n * sizeof(cplx));
+            };
+            RowsOut ro;
+            ro.vout = static_cast<double2 *>(at.devicePointer);
+            ro.rows = static_cast<const int *>(pl->casemap.p);
+            ro.during = &zero_islanded;
+            int rc = run_batch(pl, ns, reinterpret_cast<const cplx *>(V0_ri), 0,
+                               reinterpret_cast<const cplx *>(Sbus_ri), 0, optr, opos, oval, jf, jc, 0, max_iter,
+                               tol, nullptr, it.data(), er.data(), false, nullptr, &ro);
+            if (rc) return rc;
+            for (int c = 0; c < ncases; ++c) {
+                converged[c] = 0;
+                iters[c] = 0;
+                errs[c] = 1;  // SingularMatrix: islanded, not computed
+            }
+            for (int i = 0; i < ns; ++i) {
+                const int c = idx[i];
+                iters[c] = it[i];
+                errs[c] = er[i];
+                converged[c] = er[i] == 0;
+            }
+            pl->timers[0] = now() - t0;
+            pl->timers[1] = t1 - t0;
+            return 0;
+        }
+    }
+    // otherwise: result rows in case order on the device, then one copy into the caller's array,
+    // on the copy stream: issued as soon as the rows are final, so the copy overlaps the FP64
+    // re-run of the instances that failed in the mixed form; their rows follow once it is done
     cudaStream_t cs = pl->copy_stream;
     std::vector<int> map(ncases, -1);
     for (int i = 0; i < ns; ++i) map[idx[i]] = i;

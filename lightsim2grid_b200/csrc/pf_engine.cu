@@ -36,6 +36,7 @@ struct Shared {
     int novr;
     int job;
     int piv_err;
+    int job_failed;
     double slack_absorbed;
 };
 
@@ -474,8 +475,8 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
         __syncthreads();
         if (S.novr < 0) {
             // more Ybus overrides than the kernel stages: not computed (start voltages out)
-            double2 *vo = A.Vout + (long long)inst * n;
-            for (int b = tid; b < n; b += blockDim.x) vo[b] = V[b];
+            double2 *vo = out_row(A, inst, n);
+            for (int b = tid; b < n; b += blockDim.x) vo[b] = A.zero_failed ? make_double2(0.0, 0.0) : V[b];
             if (tid == 0) {
                 A.iters[inst] = 0;
                 A.errs[inst] = 8;  // NotInitError
@@ -587,8 +588,9 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
             conv = norm < A.tol;
         }
         if (!conv && err == 0) err = 2;  // TooManyIterations
-        double2 *vo = A.Vout + (long long)inst * n;
-        for (int b = tid; b < n; b += blockDim.x) vo[b] = V[b];
+        double2 *vo = out_row(A, inst, n);
+        const bool zero = A.zero_failed && err != 0;
+        for (int b = tid; b < n; b += blockDim.x) vo[b] = zero ? make_double2(0.0, 0.0) : V[b];
         if (tid == 0) {
             A.iters[inst] = it;
             A.errs[inst] = err;
@@ -604,6 +606,21 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
             break;
         }
     }
+}
+
+// The mixed form's FP64 fallback inside the launch: a job with an instance that did not converge
+// in FP32 is solved again in FP64 by the same CTA, with the solve vector in the shared memory
+// the FP32 LU used (the next job refills it) and the FP64 LU in the CTA's slab.  The same code
+// as a separate FP64 launch (solve_job with FP64 LU in global memory); a function of its own so
+// that its registers do not add to the FP32 path's.
+__device__ __noinline__ void fp64_rerun(const DevPlan &P, const BatchArgs &A, Shared &S, unsigned char *dyn,
+                                        int first, int count) {
+    const Layout<double, double> L = make_layout<double, double, false>(P, A, dyn);
+    stage_tables<double, double>(P, L);
+    __syncthreads();
+    Prof pr;
+    pr.start(false);
+    solve_job<double, double, false, false>(P, A, S, L, first, count, pr);
 }
 
 template <typename LT, typename XT, bool LU_SMEM, bool REFINE>
@@ -650,6 +667,22 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, cons
         const int count = multi ? M.job_count[job] : A0.job_count[job];
         solve_job<LT, XT, LU_SMEM, REFINE>(seg.P, seg.A, S, L, first, count, pr);
         __syncthreads();
+        if constexpr (REFINE) {
+            if (seg.A.fp64_inline) {
+                if (tid == 0) {
+                    int bad = 0;
+                    for (int i = first; i < first + count; ++i) bad |= seg.A.errs[i] != 0;
+                    S.job_failed = bad;
+                }
+                __syncthreads();
+                if (S.job_failed) {
+                    fp64_rerun(seg.P, seg.A, S, dyn, first, count);
+                    __syncthreads();
+                    stage_tables<LT, XT>(seg.P, L);  // the FP64 solve vector covered them
+                    __syncthreads();
+                }
+            }
+        }
     }
     if (pr.on)
         for (int i = 0; i < kPhaseSlots; ++i) A0.phase_cycles[(size_t)blockIdx.x * kPhaseSlots + i] = pr.pc[i];
@@ -726,8 +759,8 @@ __global__ void __launch_bounds__(512, 1) dc_batch_kernel(const DevPlan P, const
             if (S.novr < 0) {
                 // more Ybus overrides than the kernel stages: not computed (start voltages out)
                 const double2 *v0 = A.V0 + (long long)inst * A.v0_stride;
-                double2 *vo = A.Vout + (long long)inst * n;
-                for (int b = tid; b < n; b += blockDim.x) vo[b] = v0[b];
+                double2 *vo = out_row(A, inst, n);
+                for (int b = tid; b < n; b += blockDim.x) vo[b] = A.zero_failed ? make_double2(0.0, 0.0) : v0[b];
                 if (tid == 0) {
                     A.iters[inst] = 0;
                     A.errs[inst] = 8;  // NotInitError
@@ -768,7 +801,7 @@ __global__ void __launch_bounds__(512, 1) dc_batch_kernel(const DevPlan P, const
                 if (bad || nrm >= 1e6) err = 7;  // SolverSolve
             }
             const double2 *v0 = A.V0 + (long long)inst * A.v0_stride;
-            double2 *vo = A.Vout + (long long)inst * n;
+            double2 *vo = out_row(A, inst, n);
             const double2 vs = v0[P.slack0];
             const double a0 = atan2(vs.y, vs.x);
             for (int b = tid; b < n; b += blockDim.x) {
@@ -971,8 +1004,8 @@ __global__ void __launch_bounds__(MAXT, MINB) fdpf_batch_kernel(const DevPlan P0
             __syncthreads();
             if (S.novr < 0) {
                 // more Ybus overrides than the kernel stages: not computed (start voltages out)
-                double2 *vo = A.Vout + (long long)inst * n;
-                for (int b = tid; b < n; b += blockDim.x) vo[b] = V[b];
+                double2 *vo = out_row(A, inst, n);
+                for (int b = tid; b < n; b += blockDim.x) vo[b] = A.zero_failed ? make_double2(0.0, 0.0) : V[b];
                 if (tid == 0) {
                     A.iters[inst] = 0;
                     A.errs[inst] = 8;  // NotInitError
@@ -1042,8 +1075,9 @@ __global__ void __launch_bounds__(MAXT, MINB) fdpf_batch_kernel(const DevPlan P0
                 conv = norm < A.tol;
             }
             if (!conv && err == 0) err = 2;  // TooManyIterations
-            double2 *vo = A.Vout + (long long)inst * n;
-            for (int b = tid; b < n; b += blockDim.x) vo[b] = V[b];
+            double2 *vo = out_row(A, inst, n);
+            const bool zero = A.zero_failed && err != 0;
+            for (int b = tid; b < n; b += blockDim.x) vo[b] = zero ? make_double2(0.0, 0.0) : V[b];
             if (tid == 0) {
                 A.iters[inst] = it;
                 A.errs[inst] = err;

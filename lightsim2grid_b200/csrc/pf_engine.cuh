@@ -75,7 +75,18 @@ struct BatchArgs {
                                        // instance: clock after every phase of every program
     int trace_cap;
     int tile_lanes;                    // batch-interleaved kernel: lanes (instances) per CTA
+    const int *vout_row;               // optional: output row of each instance (default: the instance)
+    int zero_failed;                   // 1: an instance that did not converge writes a zero row
+    int fp64_inline;                   // mixed form: a job that failed in FP32 is solved again in FP64
+                                       // by the same CTA (slab_bytes then holds an FP64 LU, and the
+                                       // dynamic shared memory an FP64 solve vector)
 };
+
+// The output row of an instance (Vout may be mapped host memory: rows stream out as instances
+// finish).
+__device__ __forceinline__ double2 *out_row(const BatchArgs &A, int inst, int n) {
+    return A.Vout + (long long)(A.vout_row ? A.vout_row[inst] : inst) * n;
+}
 
 // One segment of a launch over several plans: a plan and its batch (device memory).
 struct alignas(16) Segment {

@@ -414,8 +414,9 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
         }
         // ---- results of the instances that finished in this round
         if (S.state[lane] == kDone) {
-            double2 *vo = A.Vout + (long long)inst * n;
-            for (int r = warp; r < n; r += kW) vo[r] = V[ix(r, lane)];
+            double2 *vo = out_row(A, inst, n);
+            const bool zero = A.zero_failed && S.err[lane] != 0;
+            for (int r = warp; r < n; r += kW) vo[r] = zero ? make_double2(0.0, 0.0) : V[ix(r, lane)];
             if (warp == 0) {
                 A.iters[inst] = S.it[lane];
                 A.errs[inst] = S.err[lane];

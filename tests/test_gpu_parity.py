@@ -314,3 +314,39 @@ def test_n1_order_is_hardest_first():
             acc[r] = acc.get(r, 0) + (oval[k] - Yc.data[p]) * V0[cc]
         score[i] = max(abs(V0[r] * np.conj(v)) for r, v in acc.items())
     assert np.all(np.diff(score[order]) <= 1e-12 * max(1.0, score.max()))
+
+
+def test_n1_rows_into_pinned_output_match_pageable():
+    """pf_batch_n1 writes the rows straight into a pinned, device-mapped output array (zero rows
+    for islanded and failed cases, FP64 re-run rows included): the same arrays as through the
+    device buffer and copy used for pageable outputs."""
+    import torch
+    from lightsim2grid_b200 import Plan
+
+    c = grid_problem("grid2848")
+    o_n = OracleNR(False)
+    assert o_n.compute_pf(c["Ybus"], c["V0"], c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], 10, 1e-8)
+    Vn = o_n.get_V()
+    g = c["grid"]
+    coeffs = [g.branch_coeffs([b]) for b in range(g.nb_powerline())]
+    plan = Plan(c["Ybus"], Vn, c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=1)
+    Vp, convp, itp, errp = plan.batch_n1(coeffs, Vn, c["Sbus"], 10, 1e-8)
+    nc, n = len(coeffs), g.n_bus
+    pinned = torch.empty(nc * n * 2, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
+    pinned = pinned.reshape(nc, n)
+    pinned[:] = 7.0  # every row must be written
+    ints = [torch.full((nc,), -5, dtype=torch.int32, pin_memory=True).numpy() for _ in range(3)]
+    cp = np.zeros(nc + 1, np.int32)
+    rows, cols, vals = [], [], []
+    for k, lst in enumerate(coeffs):
+        cp[k + 1] = cp[k] + len(lst)
+        for (r, cc, y) in lst:
+            rows.append(r)
+            cols.append(cc)
+            vals.append(y)
+    for _ in range(2):
+        V, conv, it, err = plan.batch_n1_arrays(cp, rows, cols, vals, Vn, c["Sbus"], 10, 1e-8,
+                                                out=(pinned, *ints))
+        assert np.array_equal(err, errp) and np.array_equal(it, itp) and np.array_equal(conv, convp)
+        assert np.array_equal(V, Vp)
+    assert (errp == 1).any() and (errp > 1).any()  # islanded and failed cases are exercised
