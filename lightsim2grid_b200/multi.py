@@ -120,6 +120,13 @@ class GridCases:
             raise RuntimeError(nat.last_error(lib))
         self.solvable = solv.astype(bool)
         ns = self.ninst = int(solv.sum())
+        # the instances hardest first (power mismatch of the outage at the start voltages)
+        self.order = np.zeros(max(ns, 1), np.int32)
+        rc = lib.pf_n1_order(self.plan.handle, ns, nat.ptr(optr, nat.i32p), nat.ptr(opos, nat.i32p), nat.cptr(oval),
+                             nat.cptr(self.Vbase), nat.ptr(self.order, nat.i32p))
+        if rc != 0:
+            raise RuntimeError(nat.last_error(lib))
+        self.order = self.order[:ns]
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
         self.dev = dict(V0=t(self.Vbase.view(np.float64)), S=t(self.Sbase.view(np.float64)), optr=t(optr[:ns + 1]),
                         opos=t(opos[:max(nw, 1)]), oval=t(oval[:max(nw, 1)].view(np.float64)),
@@ -153,7 +160,8 @@ class GridCases:
 
 def build_uneven(parts, device, precision=1, max_iter=10, tol=1e-8, **plan_options):
     """``parts``: list of (name, GridModel, drawn branches).  Returns (MultiBatch, [GridCases]).
-    Jobs: one per solvable instance, grids ordered by decreasing size (costliest first)."""
+    Jobs: one per solvable instance, grids ordered by decreasing size (costliest first), each
+    grid's instances hardest first (pf_n1_order)."""
     import torch
 
     cases = [GridCases(nm, g, br, device, precision, max_iter, tol, **plan_options) for nm, g, br in parts]
@@ -161,7 +169,7 @@ def build_uneven(parts, device, precision=1, max_iter=10, tol=1e-8, **plan_optio
     seg, first = [], []
     for i in order:
         seg.extend([i] * cases[i].ninst)
-        first.extend(range(cases[i].ninst))
+        first.extend(cases[i].order.tolist())
     t = lambda a: torch.from_numpy(np.asarray(a, np.int32)).to(device)
     js, jf, jc = t(seg if seg else [0]), t(first if first else [0]), t(np.ones(max(len(seg), 1), np.int32))
     mb = MultiBatch([c.plan for c in cases], [c.batch for c in cases], js[:len(seg)], jf[:len(seg)],
