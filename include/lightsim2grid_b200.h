@@ -187,7 +187,9 @@ int pf_batch_ts(pf_plan *plan, int nsteps, const double *Sbus_ri, const double *
                 double tol, double *V_out_ri, int *converged, int *iters, int *errs, int *status);
 
 /* Device-resident batch on `stream` (a cudaStream_t, NULL for the default stream).  No
-   host synchronisation; capturable in a CUDA graph once the plan exists. */
+   host synchronisation; capturable in a CUDA graph once the plan exists.  Mixed form: a job
+   with an instance that does not converge in FP32 is solved again in FP64 inside the launch
+   (option fp64_fallback), so the outputs are the FP64 outcome for those instances. */
 int pf_batch_device(pf_plan *plan, const pf_device_batch *batch, void *stream);
 
 /* pf_batch_device without any allocation, for callers that cannot let the library call
@@ -208,7 +210,9 @@ int pf_batch_device_noalloc(pf_plan *plan, const pf_device_batch *batch, void *s
    (pf_scratch_bytes gives the size for a number of CTAs; the launch uses as many CTAs as fit).
    Launches of one plan on different streams with disjoint scratch may overlap on the GPU: the
    plan's device data is only read.  Used by the serving loop, which admits requests against a
-   device-memory budget.  No counterpart in the reference (its solvers own their memory). */
+   device-memory budget.  Its slabs hold the FP32 solve only: instances that fail in FP32 are
+   reported as they are (no FP64 fallback).  No counterpart in the reference (its solvers own
+   their memory). */
 int pf_batch_device_scratch(pf_plan *plan, const pf_device_batch *batch, void *scratch, long long scratch_bytes,
                             void *stream);
 
