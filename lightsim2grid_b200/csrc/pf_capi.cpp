@@ -1313,10 +1313,19 @@ int pf_batch_ts(pf_plan *pl, int nsteps, const double *Sbus_ri, const double *V0
     std::vector<int> empty;
     std::vector<cplx> ev;
     int rc = 0;
+    // a pinned, device-mapped output takes each step's row straight from the kernel (as in
+    // pf_batch_n1); otherwise the rows are copied after the kernel
+    cudaPointerAttributes at{};
+    const bool mapped = cudaPointerGetAttributes(&at, V_out_ri) == cudaSuccess && at.type == cudaMemoryTypeHost &&
+                        at.devicePointer != nullptr;
+    if (!mapped) cudaGetLastError();
+    RowsOut ro;
+    ro.vout = mapped ? static_cast<double2 *>(at.devicePointer) : nullptr;
     if (nsteps > 0)
         rc = run_batch(pl, nsteps, reinterpret_cast<const cplx *>(V0_ri), 0, reinterpret_cast<const cplx *>(Sbus_ri), n,
-                       empty, empty, ev, jf, jc, 1, max_iter, tol, reinterpret_cast<cplx *>(V_out_ri), iters, errs,
-                       false);
+                       empty, empty, ev, jf, jc, 1, max_iter, tol,
+                       mapped ? nullptr : reinterpret_cast<cplx *>(V_out_ri), iters, errs, false, nullptr,
+                       mapped ? &ro : nullptr);
     if (rc) return rc;
     int first_bad = nsteps;
     for (int s = 0; s < nsteps; ++s)

@@ -282,14 +282,24 @@ class Plan:
         nat.check(rc, "pf_batch_n1", self._lib)
         return Vout, conv[:ncases].astype(bool), iters[:ncases], errs[:ncases]
 
-    def batch_ts(self, Sbuses, V0, nchunks, max_iter, tol):
+    def batch_ts(self, Sbuses, V0, nchunks, max_iter, tol, out=None):
+        """Time series.  ``out``: optional ``(V[nsteps, n] complex128, conv, iters, errs int32)``
+        arrays to write into (pinned host memory takes the rows straight from the kernel)."""
         Sb = nat.as_c128(Sbuses)
         nsteps = Sb.shape[0]
         V0 = nat.as_c128(V0).ravel()
-        Vout = np.zeros((nsteps, self.n), dtype=np.complex128)
-        conv = np.zeros(max(nsteps, 1), dtype=np.int32)
-        iters = np.zeros(max(nsteps, 1), dtype=np.int32)
-        errs = np.zeros(max(nsteps, 1), dtype=np.int32)
+        if out is not None:
+            Vout, conv, iters, errs = out
+            ok = (Vout.dtype == np.complex128 and Vout.shape == (nsteps, self.n) and Vout.flags.c_contiguous
+                  and all(a.dtype == np.int32 and a.size >= max(nsteps, 1) and a.flags.c_contiguous
+                          for a in (conv, iters, errs)))
+            if not ok:
+                raise ValueError("out arrays must be V[nsteps, n] complex128 and three int32[nsteps], contiguous")
+        else:
+            Vout = np.zeros((nsteps, self.n), dtype=np.complex128)
+            conv = np.zeros(max(nsteps, 1), dtype=np.int32)
+            iters = np.zeros(max(nsteps, 1), dtype=np.int32)
+            errs = np.zeros(max(nsteps, 1), dtype=np.int32)
         status = nat.ctypes.c_int(0)
         rc = self._lib.pf_batch_ts(self._h, nsteps, nat.cptr(Sb), nat.cptr(V0), int(nchunks), int(max_iter),
                                    float(tol), nat.cptr(Vout), nat.ptr(conv, nat.i32p), nat.ptr(iters, nat.i32p),

@@ -10,8 +10,10 @@ chunk heads, not the answer beyond the tolerance.
 
 ``python -m lightsim2grid_b200.timeseries`` measures the 8,760-snapshot series on the 2,848-bus
 synthetic grid (per-bus AR(1) profiles, phi 0.9, sigma 0.03, times a shared daily +-15%
-sinusoid) in FP64 and in mixed precision, and reports the error of both against the FP64
-oracle's exact chain over the first snapshots.
+sinusoid) in FP64 and in mixed precision on the device, the mixed form's distance to the FP64
+results, and the whole series through the host API (``pf_batch_ts`` into pinned arrays).  The
+parity of both forms against the CPU oracle's exact chain is the test suite's
+(``tests/test_gpu_parity.py``).
 """
 import argparse
 import json
@@ -69,7 +71,6 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=8760)
     ap.add_argument("--chunks", type=int, default=0, help="0: one per resident CTA")
     ap.add_argument("--repeat", type=int, default=5)
-    ap.add_argument("--oracle-steps", type=int, default=400, help="snapshots checked against the oracle chain")
     ap.add_argument("--seed", type=int, default=8760)
     ap.add_argument("--level", type=float, default=0.9,
                     help="profiles around this fraction of the base injections: at 1.0 the daily peak drives "
@@ -78,7 +79,6 @@ def main(argv=None):
     import torch
 
     from . import synthetic
-    from oracle.oracle import time_series as oracle_ts
 
     dev = torch.device("cuda:0")
     g, _ = synthetic.make_named_grid(args.grid)
@@ -88,14 +88,9 @@ def main(argv=None):
     base = Plan(Y, g.flat_start(), S, sl, w, pv, pq, precision=0)
     V0, conv, _, _ = base.solve(g.flat_start(), S, 10, 1e-8)
     assert conv, "base case must converge"
-    K = min(args.oracle_steps, args.steps)
-    t0 = time.perf_counter()
-    _, Vo, conv_o, it_o, _ = oracle_ts(Y, S, Sb[:K], V0, sl, w, pv, pq, 10, 1e-8)
-    oracle_s = time.perf_counter() - t0
     out = {"workload": "time series, {} snapshots on synthetic {} (AR(1) phi 0.9 sigma 0.03 x daily +-15%, around "
-                       "{:.2f} x base injections), warm start, tol 1e-8 pu".format(args.steps, args.grid, args.level),
-           "oracle": {"steps": K, "converged": int(conv_o.sum()), "seconds": oracle_s,
-                      "pf_per_s_1core": K / oracle_s}}
+                       "{:.2f} x base injections), warm start, tol 1e-8 pu".format(args.steps, args.grid, args.level)}
+    results = {}
     st = torch.cuda.current_stream()
     flush = torch.empty(256 << 20 >> 2, dtype=torch.float32, device=dev)
     for label, prec in (("fp64", 0), ("mixed", 1)):
@@ -114,11 +109,30 @@ def main(argv=None):
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) * 1e-3)
         V, it, er = ds.results()
-        ok = (er[:K] == 0) & conv_o
+        results[label] = (V, er)
         out[label] = {"chunks": ds.nchunks, "ms": 1e3 * float(np.mean(times)), "converged": int((er == 0).sum()),
-                      "pf_per_s": float((er == 0).sum() / np.mean(times)), "iterations_mean": float(it.mean()),
-                      "flags_equal_oracle_first_steps": bool(np.array_equal(er[:K] == 0, conv_o)),
-                      "max_abs_dV_vs_oracle": float(np.abs(V[:K][ok] - Vo[ok]).max()) if ok.any() else None}
+                      "pf_per_s": float((er == 0).sum() / np.mean(times)), "iterations_mean": float(it.mean())}
+        if label == "mixed":
+            # the whole series through the host API, injections from and results into pinned arrays
+            nst = Sb.shape[0]
+            Sp = torch.empty(nst * g.n_bus * 2, dtype=torch.float64, pin_memory=True).numpy()
+            Sp = Sp.view(np.complex128).reshape(nst, g.n_bus)
+            Sp[:] = Sb
+            Vp = torch.empty(nst * g.n_bus * 2, dtype=torch.float64, pin_memory=True).numpy()
+            Vp = Vp.view(np.complex128).reshape(nst, g.n_bus)
+            ints = [torch.empty(nst, dtype=torch.int32, pin_memory=True).numpy() for _ in range(3)]
+            plan.batch_ts(Sp, V0, nch, 10, 1e-8, out=(Vp, *ints))
+            e2e = []
+            for _ in range(max(2, args.repeat // 2)):
+                t0 = time.perf_counter()
+                st_h, _, conv_h, _, _ = plan.batch_ts(Sp, V0, nch, 10, 1e-8, out=(Vp, *ints))
+                e2e.append(time.perf_counter() - t0)
+            out[label]["e2e"] = {"ms": 1e3 * float(np.mean(e2e)), "pf_per_s": float(conv_h.sum() / np.mean(e2e)),
+                                 "h2d_bytes": int(nst * g.n_bus * 16), "d2h_bytes": int(nst * g.n_bus * 16)}
+    (Vf, ef), (Vm, em) = results["fp64"], results["mixed"]
+    both = (ef == 0) & (em == 0)
+    out["flags_equal_mixed_fp64"] = bool(np.array_equal(ef == 0, em == 0))
+    out["max_abs_dV_mixed_vs_fp64"] = float(np.abs(Vm[both] - Vf[both]).max()) if both.any() else None
     out["mixed_over_fp64"] = out["mixed"]["pf_per_s"] / out["fp64"]["pf_per_s"]
     print(json.dumps(out))
     return 0

@@ -350,3 +350,31 @@ def test_n1_rows_into_pinned_output_match_pageable():
         assert np.array_equal(err, errp) and np.array_equal(it, itp) and np.array_equal(conv, convp)
         assert np.array_equal(V, Vp)
     assert (errp == 1).any() and (errp > 1).any()  # islanded and failed cases are exercised
+
+
+@pytest.mark.parametrize("diverge", [False, True])
+def test_time_series_rows_into_pinned_output_match_pageable(diverge):
+    """pf_batch_ts with a pinned, device-mapped output (rows written by the kernel, zero rows
+    after the first divergence) gives the same arrays as the copy path of pageable outputs."""
+    import torch
+    from lightsim2grid_b200 import Plan, synthetic
+
+    c = grid_problem("grid118")
+    g = c["grid"]
+    gen_p, sgen_p, load_p, load_q = synthetic.time_series_injections(g, 40, seed=11)
+    Sb = g.sbuses_from_injections(gen_p, sgen_p, load_p, load_q)
+    if diverge:
+        Sb[25] *= 40.0
+    plan = Plan(c["Ybus"], c["V0"], c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=1)
+    ref = plan.batch_ts(Sb, c["V0"], 4, 10, 1e-8)
+    n = g.n_bus
+    Vp = torch.empty(40 * n * 2, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(40, n)
+    Vp[:] = 7.0
+    ints = [torch.full((40,), -5, dtype=torch.int32, pin_memory=True).numpy() for _ in range(3)]
+    for _ in range(2):
+        st, V, conv, it, er = plan.batch_ts(Sb, c["V0"], 4, 10, 1e-8, out=(Vp, *ints))
+        assert st == ref[0]
+        assert np.array_equal(conv, ref[2]) and np.array_equal(it, ref[3]) and np.array_equal(er, ref[4])
+        assert np.array_equal(V, ref[1])
+    if diverge:
+        assert st == 0 and np.all(V[25:] == 0)
