@@ -32,7 +32,8 @@ def main():
     ap.add_argument("--dc", action="store_true", help="DC power flows (DC Ybus, DC outage coefficients)")
     ap.add_argument("--fdpf", type=int, default=-1, help="fast decoupled power flows: 0 XB, 1 BX (-1: Newton)")
     ap.add_argument("--max-iter", type=int, default=10)
-    ap.add_argument("--order", action="store_true", help="also time hardest-first job orders")
+    ap.add_argument("--order", action="store_true", help="also time job orders by iterations and by mismatch")
+    ap.add_argument("--case-order", action="store_true", help="jobs in case order (default: hardest first)")
     ap.add_argument("--batch-layout", type=int, default=0, help="0 auto, 1 one CTA per instance, 2 batch-interleaved")
     args = ap.parse_args()
 
@@ -82,6 +83,13 @@ def main():
             t(optr[:ns + 1]), t(opos[:nw]), t(oval[:nw].view(np.float64)), t(np.arange(ns, dtype=np.int32)),
             t(np.ones(ns, np.int32)), torch.zeros(ns * g.n_bus * 2, dtype=torch.float64, device=dev),
             torch.zeros(ns, dtype=torch.int32, device=dev), torch.zeros(ns, dtype=torch.int32, device=dev)]
+    if not args.case_order and not args.dc and args.fdpf < 0:
+        # jobs hardest first (pf_n1_order), as pf_batch_n1 and the bench run them
+        order = np.zeros(max(ns, 1), np.int32)
+        V0c = nat.as_c128(Vn).ravel()
+        assert lib.pf_n1_order(plan.handle, ns, nat.ptr(optr, nat.i32p), nat.ptr(opos, nat.i32p), nat.cptr(oval),
+                               nat.cptr(V0c), nat.ptr(order, nat.i32p)) == 0, nat.last_error(lib)
+        bufs[5] = t(order[:ns])
     b = nat.PfDeviceBatch(n_inst=ns, V0=bufs[0].data_ptr(), v0_stride=0, Sbus=bufs[1].data_ptr(), sbus_stride=0,
                           ovr_ptr=bufs[2].data_ptr(), ovr_pos=bufs[3].data_ptr(), ovr_val=bufs[4].data_ptr(),
                           max_iter=args.max_iter, tol=1e-8, chain=0, job_first=bufs[5].data_ptr(),
@@ -127,7 +135,6 @@ def main():
                 ts.append(e0.elapsed_time(e1))
             order_times[label] = ts
             assert np.array_equal(bufs[8].cpu().numpy(), it0) and np.array_equal(bufs[9].cpu().numpy(), er0)
-        bufs[5].copy_(torch.from_numpy(np.arange(ns, dtype=np.int32)).to(dev))
     cyc = np.zeros(8)
     assert lib.pf_batch_device_phase_cycles(plan.handle, nat.ctypes.byref(b), stream.cuda_stream,
                                             nat.ptr(cyc, nat.f64p)) == 0, nat.last_error(lib)
