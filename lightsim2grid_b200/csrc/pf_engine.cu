@@ -432,6 +432,14 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
     LT *lu = L.lu;
     double2 *V = L.V, *Ibus = L.Ibus, *Fbus = L.Fbus;
     double *Vm = L.Vm, *Va = L.Va, *dxg = L.dxg;
+    // With the LU in shared memory, the LU region is dead from the voltage update to the next
+    // Jacobian fill: the voltages are also written there (Vs) and the mismatch gathers them from
+    // shared memory instead of the slab.  Not when the LU must survive the mismatch (LU reuse).
+    double2 *Vs = nullptr;
+    if constexpr (LU_SMEM) {
+        if (!(REFINE && A.reuse_below > 0.0) && (size_t)n * sizeof(double2) <= (size_t)P.nnzLU * sizeof(LT))
+            Vs = reinterpret_cast<double2 *>(lu);
+    }
     for (int step = 0; step < count; ++step) {
         const int inst = first + step;
         const double2 *Sb = A.Sbus + (long long)inst * A.sbus_stride;
@@ -440,12 +448,14 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
             for (int b = tid; b < n; b += blockDim.x) {
                 const double2 v = v0[b];
                 V[b] = v;
+                if (Vs) Vs[b] = v;
                 Vm[b] = cabs2(v);
                 Va[b] = atan2(v.y, v.x);
             }
         } else {
             for (int b = tid; b < n; b += blockDim.x) {
                 const double2 v = V[b];
+                if (Vs) Vs[b] = v;
                 Vm[b] = cabs2(v);
                 Va[b] = atan2(v.y, v.x);
             }
@@ -494,7 +504,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
         double norm;
         int bad;
         pr.mark(6);
-        mismatch<XT>(P, S, V, Ibus, Fbus, Sb, x, norm, bad);
+        mismatch<XT>(P, S, Vs ? Vs : V, Ibus, Fbus, Sb, x, norm, bad);
         pr.mark(0);
         bool conv = !bad && norm < A.tol;
         int it = 0, err = 0;
@@ -558,6 +568,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 double sn, cs;
                 sincos(va, &sn, &cs);
                 V[b] = make_double2(vm * cs, vm * sn);
+                if (Vs) Vs[b] = make_double2(vm * cs, vm * sn);
                 Vm[b] = vm;
                 Va[b] = va;
                 lmin = fmin(lmin, vm);
@@ -579,7 +590,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
             tr.mark();
             tr.buf = nullptr;
             pr.mark(6);
-            mismatch<XT>(P, S, V, Ibus, Fbus, Sb, x, norm, bad);
+            mismatch<XT>(P, S, Vs ? Vs : V, Ibus, Fbus, Sb, x, norm, bad);
             pr.mark(0);
             if (bad) {
                 err = 3;  // InifiniteValue
