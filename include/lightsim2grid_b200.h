@@ -45,6 +45,9 @@ typedef struct pf_options {
                                stored as 32 consecutive per-instance values (coalesced, the
                                batch dimension amortises each phase); its per-CTA memory is
                                allocated on first use                                         */
+    int ordering;           /* elimination order of the first factorisation.  0: default, minimum
+                               degree followed by its equivalent reordering of least depth (no
+                               added fill, fewer dependent phases); 1: minimum degree only     */
 } pf_options;
 
 /* DC power flow plan (BaseDCAlgo::compute_pf, src/powerflow_algorithm/BaseDCAlgo.tpp:5-175;

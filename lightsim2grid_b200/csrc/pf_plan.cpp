@@ -80,6 +80,89 @@ std::vector<int> minimum_degree(int m, const std::vector<int> &Ap, const std::ve
     return order;
 }
 
+// Equivalent reordering of low elimination height (Jess & Kees 1982): the filled graph of A + A^T
+// under `order` is chordal, and eliminating in rounds a maximal independent set of its
+// simplicial vertices is a perfect elimination ordering of it (no fill beyond the filled
+// graph's) whose rounds bound the dependency depth.  Within a round vertices keep their
+// position in `order`.
+std::vector<int> low_height_order(int m, const std::vector<int> &Ap, const std::vector<int> &Ai,
+                                  const std::vector<int> &order) {
+    std::vector<int> pos(m);
+    for (int k = 0; k < m; ++k) pos[order[k]] = k;
+    // symbolic elimination in `order`: the later neighbours of step k, merged into its parent's
+    std::vector<std::vector<int>> up(m);
+    for (int j = 0; j < m; ++j)
+        for (int p = Ap[j]; p < Ap[j + 1]; ++p) {
+            const int a = pos[j], b = pos[Ai[p]];
+            if (a == b) continue;
+            up[std::min(a, b)].push_back(std::max(a, b));
+        }
+    std::vector<std::vector<int>> adj(m);  // filled graph, step numbering
+    std::vector<int> merged;
+    for (int k = 0; k < m; ++k) {
+        auto &u = up[k];
+        std::sort(u.begin(), u.end());
+        u.erase(std::unique(u.begin(), u.end()), u.end());
+        if (u.empty()) continue;
+        const int par = u[0];
+        for (int i : u) {
+            adj[k].push_back(i);
+            adj[i].push_back(k);
+        }
+        up[par].insert(up[par].end(), u.begin() + 1, u.end());
+        std::vector<int>().swap(u);
+    }
+    for (auto &a : adj) std::sort(a.begin(), a.end());
+    std::vector<char> alive(m, 1), simp(m, 0), taken(m, 0);
+    std::vector<int> mark(m, -1), deg(m);
+    int stamp = 0;
+    for (int v = 0; v < m; ++v) deg[v] = (int)adj[v].size();
+    auto simplicial = [&](int v) {
+        ++stamp;
+        for (int a : adj[v])
+            if (alive[a]) mark[a] = stamp;
+        for (int a : adj[v]) {
+            if (!alive[a]) continue;
+            int c = 0;
+            for (int z : adj[a])
+                if (alive[z] && mark[z] == stamp) ++c;
+            if (c != deg[v] - 1) return false;
+        }
+        return true;
+    };
+    for (int v = 0; v < m; ++v) simp[v] = simplicial(v);
+    std::vector<int> out;
+    out.reserve(m);
+    std::vector<int> round, touched;
+    while ((int)out.size() < m) {
+        round.clear();
+        for (int v = 0; v < m; ++v) {
+            if (!alive[v] || !simp[v]) continue;
+            bool free = true;
+            for (int a : adj[v])
+                if (alive[a] && taken[a]) { free = false; break; }
+            if (!free) continue;
+            taken[v] = 1;
+            round.push_back(v);
+        }
+        if (round.empty()) return order;  // not chordal: cannot happen for a filled graph
+        touched.clear();
+        for (int v : round) {
+            alive[v] = 0;
+            out.push_back(order[v]);
+        }
+        for (int v : round)
+            for (int a : adj[v])
+                if (alive[a]) {
+                    --deg[a];
+                    touched.push_back(a);
+                }
+        for (int v : round) taken[v] = 0;
+        for (int a : touched) simp[a] = simplicial(a);
+    }
+    return out;
+}
+
 // Builds one phase program, level after level.  All operations of a level that write the
 // same value form a cluster and run on one thread, in the order they were added (so there
 // are no write conflicts, no atomics and a deterministic summation order); clusters are
@@ -339,6 +422,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
     std::ostringstream err;
     // ---------------------------------------------------------------- ordering
     P.q = minimum_degree(m, P.Jp, P.Ji);
+    if (opt.low_height) P.q = low_height_order(m, P.Jp, P.Ji, P.q);
     P.qinv.assign(m, 0);
     for (int k = 0; k < m; ++k) P.qinv[P.q[k]] = k;
 

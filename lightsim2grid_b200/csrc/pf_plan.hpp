@@ -125,6 +125,7 @@ struct PlanOptions {
     double pivot_threshold = 1e-3;    // diagonal preference of the first factorisation
     bool fuse_forward = true;         // fuse the forward substitution into the refactorisation
     int threads = 512;                // CTA size the phase programs are laid out for
+    bool low_height = true;           // minimum degree followed by its low-height equivalent
 };
 
 // Builds a plan.  Ybus CSC (n x n, complex), V0 and Sbus (used for the first

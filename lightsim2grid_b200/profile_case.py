@@ -35,6 +35,8 @@ def main():
     ap.add_argument("--order", action="store_true", help="also time job orders by iterations and by mismatch")
     ap.add_argument("--case-order", action="store_true", help="jobs in case order (default: hardest first)")
     ap.add_argument("--batch-layout", type=int, default=0, help="0 auto, 1 one CTA per instance, 2 batch-interleaved")
+    ap.add_argument("--ordering", type=int, default=0,
+                    help="0: minimum degree + least-depth equivalent reordering, 1: minimum degree only")
     args = ap.parse_args()
 
     import torch
@@ -56,7 +58,7 @@ def main():
     plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, dc=args.dc, fdpf=fdpf, threads=args.threads,
                 lu_placement=args.lu_placement, fuse_forward=args.fuse_forward, max_ctas_per_sm=args.ctas_per_sm,
                 refine=args.refine, refine_threshold=args.refine_threshold, lu_reuse_threshold=args.lu_reuse,
-                batch_layout=args.batch_layout)
+                batch_layout=args.batch_layout, ordering=args.ordering)
     lib = plan._lib
     cp = np.zeros(nb + 1, np.int32)
     rows, cols, vals = [], [], []

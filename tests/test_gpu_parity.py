@@ -161,6 +161,33 @@ def test_n1_batch_matches_oracle(precision):
         assert np.all(V[~conv] == 0)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_n1_batch_ordering_options_agree(precision):
+    """The default elimination order (minimum degree, then its least-depth equivalent) and
+    minimum degree alone: the same flags and iteration counts on the N-1 batch of the 1354-bus
+    grid, and voltages within the precision's bar of each other."""
+    from lightsim2grid_b200 import Plan
+
+    c = grid_problem("grid1354")
+    o_n = OracleNR(False)
+    assert o_n.compute_pf(c["Ybus"], c["V0"], c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], 10, 1e-8)
+    Vn = o_n.get_V()
+    coeffs = _n1(c, 400)
+    out = []
+    for ordering in (0, 1):
+        plan = Plan(c["Ybus"], Vn, c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=precision,
+                    ordering=ordering)
+        out.append((plan.info()["levels_refactor"],) + tuple(plan.batch_n1(coeffs, Vn, c["Sbus"], 10, 1e-8)))
+    (l0, V0, c0, i0, e0), (l1, V1, c1, i1, e1) = out
+    assert l0 < l1
+    assert np.array_equal(e0, e1) and np.array_equal(c0, c1)
+    if precision == 0:
+        assert np.array_equal(i0, i1)
+    tol = TOL_FP64 if precision == 0 else TOL_MIXED
+    for k in np.nonzero(c0)[0]:
+        assert _vdiff(V0[k], V1[k]) <= tol, k
+
+
 def test_n1_computer_api():
     from lightsim2grid_b200 import ContingencyAnalysisCPP, SolverType
 
