@@ -175,8 +175,13 @@ struct ProgramBuilder {
     std::vector<int> ops;          // 4 ints per operation of the current level
     std::vector<long long> key;    // written value: space (0 lu, 1 v) and index
 
+    int lu_base = -1;              // index-space offset of the LU in the packed layout; >= 0:
+                                   // order each thread's operations for few bank conflicts
+    int vdummy = 0;                // index of the empty operations' scratch slot
+
     ProgramBuilder(Plan::Program &p, int threads) : prog(p), nt(threads) {
         prog.ops.clear();
+        prog.ops_banked.clear();
         prog.base.assign(1, 0);
         prog.width.clear();
     }
@@ -223,18 +228,121 @@ struct ProgramBuilder {
         }
         int len = 0;
         for (auto &v : per) len = std::max(len, (int)v.size());
-        for (int j = 0; j < len; ++j)
-            for (int t = 0; t < width; ++t) {
-                if (j < (int)per[t].size()) {
-                    const int o = per[t][j];
-                    prog.ops.insert(prog.ops.end(), ops.begin() + 4 * o, ops.begin() + 4 * o + 4);
-                } else {
-                    const int none[4] = {0, 0, 0, 7 << 28};
-                    prog.ops.insert(prog.ops.end(), none, none + 4);
-                }
+        for (auto &v : per) v.resize(len, -1);
+        emit(prog.ops, per, width, len);
+        if (lu_base >= 0) {
+            std::vector<int> cfirst, ccount;
+            for (const Cl &c : cl) {
+                cfirst.push_back(c.first);
+                ccount.push_back(c.count);
             }
+            const auto slot = assign_banked(cfirst, ccount, idx, width, len);
+            emit(prog.ops_banked, slot.empty() ? per : slot, width, len);
+        }
         prog.width.push_back(width);
         prog.base.push_back((int)(prog.ops.size() / 4));
+    }
+
+    // appends a phase: slot j of thread t at j * width + t (-1: empty operation)
+    void emit(std::vector<int> &out, const std::vector<std::vector<int>> &slot, int width, int len) const {
+        for (int j = 0; j < len; ++j)
+            for (int t = 0; t < width; ++t) {
+                const int o = slot[t][j];
+                if (o >= 0) out.insert(out.end(), ops.begin() + 4 * o, ops.begin() + 4 * o + 4);
+                else {
+                    const int none[4] = {0, 0, 0, 7 << 28};
+                    out.insert(out.end(), none, none + 4);
+                }
+            }
+    }
+
+    // shared-memory word of field f (0 x, 1 y, 2 z, 3 w) of operation o in the packed layout
+    unsigned word(int o, int f) const {
+        const int kind = (unsigned)ops[4 * o + 3] >> 28;
+        const int v = f == 3 ? (ops[4 * o + 3] & 0x0fffffff) : ops[4 * o + f];
+        if (kind == 0) return (unsigned)(lu_base + v);
+        if (kind == 2) return (unsigned)((f == 0 || f == 2) ? v : lu_base + v);
+        return (unsigned)vdummy;
+    }
+
+    // Places the level's operations on (thread, slot), `len` slots per thread, so that the 32
+    // operations a warp runs together touch few shared-memory words per bank (4-byte words, 32
+    // banks; lanes reading one word share it).  Operations writing one value (clusters of two or
+    // more) run consecutively on one thread, placed first onto the least loaded threads as in the
+    // LPT placement; the single operations then fill the free slots warp-slot by warp-slot, each
+    // lane taking the candidate that adds the fewest conflicts (the written word counts twice:
+    // loaded and stored).  Greedy, with the search cut where a bank's written-word conflicts alone
+    // reach the best cost found.
+    std::vector<std::vector<int>> assign_banked(const std::vector<int> &cfirst, const std::vector<int> &ccount,
+                                                const std::vector<int> &idx, int width, int len) const {
+        const int ncl = (int)cfirst.size();
+        std::vector<std::vector<int>> slot(width);
+        std::vector<int> fill(width, 0);
+        std::vector<std::pair<int, int>> heap;
+        for (int t = 0; t < width; ++t) heap.push_back({0, t});
+        auto cmp = [](const std::pair<int, int> &a, const std::pair<int, int> &b) {
+            return a.first != b.first ? a.first > b.first : a.second > b.second;
+        };
+        std::make_heap(heap.begin(), heap.end(), cmp);
+        for (int c = 0; c < ncl && ccount[c] > 1; ++c) {
+            std::pop_heap(heap.begin(), heap.end(), cmp);
+            auto &h = heap.back();
+            for (int q = 0; q < ccount[c]; ++q) slot[h.second].push_back(idx[cfirst[c] + q]);
+            h.first += ccount[c];
+            fill[h.second] = h.first;
+            std::push_heap(heap.begin(), heap.end(), cmp);
+        }
+        for (auto &v : slot) v.resize(len, -1);
+        // single operations, bucketed by the bank of the word they write
+        std::vector<std::vector<int>> bucket(32);
+        for (int c = 0; c < ncl; ++c)
+            if (ccount[c] == 1) bucket[word(idx[cfirst[c]], 0) % 32].push_back(idx[cfirst[c]]);
+        for (auto &b : bucket) std::reverse(b.begin(), b.end());  // pop from the back in order
+        int left = 0;
+        for (auto &b : bucket) left += (int)b.size();
+        for (int j = 0; j < len && left > 0; ++j)
+            for (int q0 = 0; q0 < width && left > 0; q0 += 32) {
+                const int q1 = std::min(width, q0 + 32);
+                std::vector<unsigned> seen[4][32];
+                auto add = [&](int o) {
+                    for (int f = 0; f < 4; ++f) {
+                        const unsigned a = word(o, f);
+                        auto &s2 = seen[f][a % 32];
+                        if (std::find(s2.begin(), s2.end(), a) == s2.end()) s2.push_back(a);
+                    }
+                };
+                for (int t = q0; t < q1; ++t)
+                    if (slot[t][j] >= 0) add(slot[t][j]);
+                for (int t = q0; t < q1 && left > 0; ++t) {
+                    if (slot[t][j] >= 0) continue;
+                    int bb = -1, bi = -1;
+                    long long bc = 0;
+                    for (int bk = 0; bk < 32 && !(bb >= 0 && bc == 0); ++bk) {
+                        auto &b = bucket[bk];
+                        if (!seen[0][bk].empty() && bb >= 0 && bc <= 2 * (long long)seen[0][bk].size()) continue;
+                        for (int u = 0; u < (int)b.size(); ++u) {
+                            const int o = b[b.size() - 1 - u];
+                            long long cost = 0;
+                            for (int f = 0; f < 4; ++f) {
+                                const unsigned a = word(o, f);
+                                const auto &s2 = seen[f][a % 32];
+                                if (std::find(s2.begin(), s2.end(), a) == s2.end()) cost += (f == 0 ? 2 : 1) * (long long)s2.size();
+                            }
+                            if (bb < 0 || cost < bc) { bb = bk; bi = u; bc = cost; }
+                            if (bc == 0) break;
+                        }
+                    }
+                    auto &b = bucket[bb];
+                    const size_t at = b.size() - 1 - bi;
+                    const int o = b[at];
+                    b.erase(b.begin() + at);
+                    --left;
+                    slot[t][j] = o;
+                    add(o);
+                }
+            }
+        if (left > 0) return {};  // cannot happen: the free slots hold every single operation
+        return slot;
     }
 };
 
@@ -246,11 +354,13 @@ bool compact_fits(const Plan &P) { return (long long)compact_lu_offset(P.m) + P.
 
 void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out, int lu_offset) {
     const unsigned L = (unsigned)(lu_offset >= 0 ? lu_offset : compact_lu_offset(m)), dummy = (unsigned)m;
+    // the bank-conflict placement assumes the default layout
+    const std::vector<int> &ops = lu_offset < 0 && !pr.ops_banked.empty() ? pr.ops_banked : pr.ops;
     const int n = pr.nops();
     out.resize(2 * (size_t)n);
     for (int o = 0; o < n; ++o) {
-        const unsigned x = (unsigned)pr.ops[4 * o], y = (unsigned)pr.ops[4 * o + 1], z = (unsigned)pr.ops[4 * o + 2];
-        const unsigned w = (unsigned)pr.ops[4 * o + 3] & 0x0fffffffu, kind = (unsigned)pr.ops[4 * o + 3] >> 28;
+        const unsigned x = (unsigned)ops[4 * o], y = (unsigned)ops[4 * o + 1], z = (unsigned)ops[4 * o + 2];
+        const unsigned w = (unsigned)ops[4 * o + 3] & 0x0fffffffu, kind = (unsigned)ops[4 * o + 3] >> 28;
         unsigned X = dummy, Y = dummy, Z = dummy, W = dummy;
         if (kind == 0u) {
             X = L + x; Y = L + y; Z = L + z; W = L + w;
@@ -585,6 +695,8 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
     std::vector<int> rowpos(m, -1);
     {
         ProgramBuilder B(P.factor, opt.threads);
+        B.lu_base = compact_lu_offset(m);
+        B.vdummy = m;
         for (int l = 0; l < nplev; ++l) {
             B.begin();
             if (l < nlev)
@@ -623,6 +735,8 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         // z(k) is kept undivided by U(k, k): a push divides by the pivot, and one scaling pass
         // after the program divides every z(k) (no per-pivot division operations)
         ProgramBuilder B(P.backward, opt.threads);
+        B.lu_base = compact_lu_offset(m);
+        B.vdummy = m;
         for (int l = 0; l < nb; ++l) {
             B.begin();
             for (int k : byb[l])
@@ -644,6 +758,8 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         for (int k = 0; k < m; ++k) byf[flev[k]].push_back(k);
         P.levels_fwd = nf;
         ProgramBuilder B(P.forward, opt.threads);
+        B.lu_base = compact_lu_offset(m);
+        B.vdummy = m;
         for (int l = 0; l < nf; ++l) {
             B.begin();
             for (int k : byf[l])

@@ -88,6 +88,10 @@ struct Plan {
         //   kind 2: v[x]  -= LU[y] * v[z] / LU[w]    (substitution push)
         //   kind 7: empty slot
         std::vector<int> ops;
+        // the same operations placed for few shared-memory bank conflicts in the packed layout
+        // (same phases and widths; every written value keeps its thread and order, so the
+        // results are bit-identical); empty when not built
+        std::vector<int> ops_banked;
         std::vector<int> base;         // phase p = operations [base[p], base[p+1])
         std::vector<int> width;        // phase p: threads with work (the operation stride)
         int nphases() const { return (int)base.size() - 1; }
