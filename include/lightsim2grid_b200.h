@@ -46,8 +46,10 @@ typedef struct pf_options {
                                batch dimension amortises each phase); its per-CTA memory is
                                allocated on first use                                         */
     int ordering;           /* elimination order of the first factorisation.  0: default, minimum
-                               degree followed by its equivalent reordering of least depth (no
-                               added fill, fewer dependent phases); 1: minimum degree only     */
+                               degree of 8 relabellings of the pattern, each followed by its
+                               equivalent reordering of least depth (no added fill, fewer
+                               dependent phases), the shallowest kept; 1: minimum degree only;
+                               2: minimum degree and its least-depth equivalent, one labelling */
 } pf_options;
 
 /* DC power flow plan (BaseDCAlgo::compute_pf, src/powerflow_algorithm/BaseDCAlgo.tpp:5-175;

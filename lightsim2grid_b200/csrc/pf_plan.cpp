@@ -163,6 +163,75 @@ std::vector<int> low_height_order(int m, const std::vector<int> &Ap, const std::
     return out;
 }
 
+// Depth (longest dependency chain) and fill of the symbolic factorisation of A + A^T eliminated
+// in `order`: the diagonal-pivot estimate of the refactorisation's levels.
+int symbolic_depth(int m, const std::vector<int> &Ap, const std::vector<int> &Ai, const std::vector<int> &order,
+                   long long &fill) {
+    std::vector<int> pos(m);
+    for (int k = 0; k < m; ++k) pos[order[k]] = k;
+    std::vector<std::vector<int>> up(m);
+    for (int j = 0; j < m; ++j)
+        for (int p = Ap[j]; p < Ap[j + 1]; ++p) {
+            const int a = pos[j], b = pos[Ai[p]];
+            if (a != b) up[std::min(a, b)].push_back(std::max(a, b));
+        }
+    std::vector<int> lev(m, 0);
+    int depth = 0;
+    fill = 0;
+    for (int k = 0; k < m; ++k) {
+        auto &u = up[k];
+        std::sort(u.begin(), u.end());
+        u.erase(std::unique(u.begin(), u.end()), u.end());
+        fill += (long long)u.size();
+        depth = std::max(depth, lev[k] + 1);
+        for (int i : u) lev[i] = std::max(lev[i], lev[k] + 1);
+        if (!u.empty()) up[u[0]].insert(up[u[0]].end(), u.begin() + 1, u.end());
+        std::vector<int>().swap(u);
+    }
+    return depth;
+}
+
+// Minimum degree breaks ties by vertex label, and the depth of the equivalent least-depth order
+// varies with those choices: orders of `trials` relabellings (the identity first, then seeded
+// shuffles) are compared and the shallowest kept (then the least fill).
+std::vector<int> shallow_order(int m, const std::vector<int> &Ap, const std::vector<int> &Ai, int trials) {
+    std::vector<int> best;
+    int bdepth = 0;
+    long long bfill = 0;
+    unsigned seed = 0x2545f491u;
+    std::vector<int> perm(m), inv(m);
+    for (int t = 0; t < std::max(1, trials); ++t) {
+        for (int i = 0; i < m; ++i) perm[i] = i;
+        if (t > 0)
+            for (int i = m - 1; i > 0; --i) {
+                seed = seed * 1664525u + 1013904223u;
+                std::swap(perm[i], perm[(seed >> 8) % (unsigned)(i + 1)]);
+            }
+        for (int i = 0; i < m; ++i) inv[perm[i]] = i;
+        // the pattern with vertex i labelled perm[i]
+        std::vector<std::vector<int>> cols(m);
+        for (int j = 0; j < m; ++j)
+            for (int p = Ap[j]; p < Ap[j + 1]; ++p) cols[perm[j]].push_back(perm[Ai[p]]);
+        std::vector<int> Bp(m + 1, 0), Bi;
+        Bi.reserve(Ai.size());
+        for (int j = 0; j < m; ++j) {
+            std::sort(cols[j].begin(), cols[j].end());
+            Bi.insert(Bi.end(), cols[j].begin(), cols[j].end());
+            Bp[j + 1] = (int)Bi.size();
+        }
+        std::vector<int> q = low_height_order(m, Bp, Bi, minimum_degree(m, Bp, Bi));
+        for (int &v : q) v = inv[v];
+        long long fill;
+        const int depth = symbolic_depth(m, Ap, Ai, q, fill);
+        if (best.empty() || depth < bdepth || (depth == bdepth && fill < bfill)) {
+            best = q;
+            bdepth = depth;
+            bfill = fill;
+        }
+    }
+    return best;
+}
+
 // Builds one phase program, level after level.  All operations of a level that write the
 // same value form a cluster and run on one thread, in the order they were added (so there
 // are no write conflicts, no atomics and a deterministic summation order); clusters are
@@ -531,8 +600,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
     const int m = P.m;
     std::ostringstream err;
     // ---------------------------------------------------------------- ordering
-    P.q = minimum_degree(m, P.Jp, P.Ji);
-    if (opt.low_height) P.q = low_height_order(m, P.Jp, P.Ji, P.q);
+    P.q = opt.order_trials > 0 ? shallow_order(m, P.Jp, P.Ji, opt.order_trials) : minimum_degree(m, P.Jp, P.Ji);
     P.qinv.assign(m, 0);
     for (int k = 0; k < m; ++k) P.qinv[P.q[k]] = k;
 

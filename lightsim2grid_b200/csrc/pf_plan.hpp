@@ -129,7 +129,9 @@ struct PlanOptions {
     double pivot_threshold = 1e-3;    // diagonal preference of the first factorisation
     bool fuse_forward = true;         // fuse the forward substitution into the refactorisation
     int threads = 512;                // CTA size the phase programs are laid out for
-    bool low_height = true;           // minimum degree followed by its low-height equivalent
+    int order_trials = 8;             // > 0: minimum degree of this many relabellings, each followed
+                                      // by its least-depth equivalent, the shallowest kept; 0:
+                                      // minimum degree only
 };
 
 // Builds a plan.  Ybus CSC (n x n, complex), V0 and Sbus (used for the first
