@@ -1511,6 +1511,44 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         for (int k = 0; k < m; ++k) v[k] = v[k] / u[P.dpos[k]];
     };
     const std::vector<double> lu0 = lu, xs0 = xs;
+    // the bank-conflict placement of the packed programs gives the same bits: every written
+    // value keeps its thread and the order of its operations
+    {
+        std::vector<double> lb = lu, xb = xs;
+        auto run_banked = [&](const l2g::Plan::Program &pr) {
+            const std::vector<int> &ops = pr.ops_banked.empty() ? pr.ops : pr.ops_banked;
+            for (int o = 0; o < pr.nops(); ++o) {
+                const int X = ops[4 * o], Y = ops[4 * o + 1], Z = ops[4 * o + 2];
+                const int W = ops[4 * o + 3] & 0x0fffffff, kind = (unsigned)ops[4 * o + 3] >> 28;
+                if (kind == 0) lb[X] -= lb[Y] * (lb[Z] / lb[W]);
+                else if (kind == 2) xb[X] -= lb[Y] * xb[Z] / lb[W];
+            }
+        };
+        run_banked(P.factor);
+        run_banked(P.backward);
+        std::vector<double> la = lu, xa = xs;
+        std::swap(la, lu);
+        std::swap(xa, xs);
+        run(P.factor);
+        run(P.backward);
+        std::swap(la, lu);
+        std::swap(xa, xs);
+        for (int p = 0; p < P.nnzLU; ++p)
+            if (lb[p] != la[p]) return fail(-1, "schedule check: bank-placed factor program disagrees");
+        for (int k = 0; k < m; ++k)
+            if (xb[k] != xa[k]) return fail(-1, "schedule check: bank-placed substitution programs disagree");
+        // the stand-alone forward program, on the factor just computed
+        xb = xs;
+        run_banked(P.forward);
+        std::swap(la, lu);
+        xa = xs;
+        std::swap(xa, xs);
+        run(P.forward);
+        std::swap(xa, xs);
+        std::swap(la, lu);
+        for (int k = 0; k < m; ++k)
+            if (xb[k] != xa[k]) return fail(-1, "schedule check: bank-placed forward program disagrees");
+    }
     run(P.factor);
     for (int k = 0; k < m; ++k)
         if (lu[P.dpos[k]] == 0.0) return fail(l2g::SolverReFactor, "schedule check: zero pivot");
