@@ -863,6 +863,7 @@ int pf_plan_create(int n, const int *colptr, const int *rowind, const double *yb
     l2g::PlanOptions po;
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
+    po.elem_bytes = pl->opt.precision ? 4 : 8;
     {
         const int m_est = npv + (distributed && nslack > 1 ? nslack - 1 : 0) + 2 * npq + (distributed ? 1 : 0);
         int thr = pl->opt.threads;
@@ -901,6 +902,7 @@ int pf_dc_plan_create(int n, const int *colptr, const int *rowind, const double 
     l2g::PlanOptions po;
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
+    po.elem_bytes = pl->opt.precision ? 4 : 8;
     int thr = pl->opt.threads;
     if (thr <= 0) thr = n > 2000 ? 512 : (n > 300 ? 256 : 128);
     thr = std::max(32, std::min(512, (thr / 32) * 32));
@@ -936,6 +938,7 @@ int pf_fdpf_plan_create(int n, const int *colptr, const int *rowind, const doubl
     l2g::PlanOptions po;
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
+    po.elem_bytes = pl->opt.precision ? 4 : 8;
     int thr = pl->opt.threads;
     if (thr <= 0) {
         // factors in global memory, read through L1 by every CTA of an SM, and several small

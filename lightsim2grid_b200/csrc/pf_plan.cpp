@@ -247,6 +247,8 @@ struct ProgramBuilder {
     int lu_base = -1;              // index-space offset of the LU in the packed layout; >= 0:
                                    // order each thread's operations for few bank conflicts
     int vdummy = 0;                // index of the empty operations' scratch slot
+    int lanes = 32;                // lanes served together by the shared-memory banks: a warp for
+                                   // 4-byte words, a half-warp for 8-byte words (16 bank pairs)
 
     ProgramBuilder(Plan::Program &p, int threads) : prog(p), nt(threads) {
         prog.ops.clear();
@@ -335,8 +337,9 @@ struct ProgramBuilder {
     }
 
     // Places the level's operations on (thread, slot), `len` slots per thread, so that the 32
-    // operations a warp runs together touch few shared-memory words per bank (4-byte words, 32
-    // banks; lanes reading one word share it).  Operations writing one value (clusters of two or
+    // operations a warp runs together touch few shared-memory words per bank (4-byte words: 32
+    // banks per warp; 8-byte words: 16 bank pairs per half-warp; lanes reading one word share
+    // it).  Operations writing one value (clusters of two or
     // more) run consecutively on one thread, placed first onto the least loaded threads as in the
     // LPT placement; the single operations then fill the free slots warp-slot by warp-slot, each
     // lane taking the candidate that adds the fewest conflicts (the written word counts twice:
@@ -363,20 +366,22 @@ struct ProgramBuilder {
         }
         for (auto &v : slot) v.resize(len, -1);
         // single operations, bucketed by the bank of the word they write
-        std::vector<std::vector<int>> bucket(32);
+        const unsigned nb = (unsigned)lanes;  // banks (or bank pairs) per group of lanes
+        std::vector<std::vector<int>> bucket(nb);
         for (int c = 0; c < ncl; ++c)
-            if (ccount[c] == 1) bucket[word(idx[cfirst[c]], 0) % 32].push_back(idx[cfirst[c]]);
+            if (ccount[c] == 1) bucket[word(idx[cfirst[c]], 0) % nb].push_back(idx[cfirst[c]]);
         for (auto &b : bucket) std::reverse(b.begin(), b.end());  // pop from the back in order
         int left = 0;
         for (auto &b : bucket) left += (int)b.size();
         for (int j = 0; j < len && left > 0; ++j)
-            for (int q0 = 0; q0 < width && left > 0; q0 += 32) {
-                const int q1 = std::min(width, q0 + 32);
-                std::vector<unsigned> seen[4][32];
+            for (int q0 = 0; q0 < width && left > 0; q0 += lanes) {
+                const int q1 = std::min(width, q0 + lanes);
+                std::vector<std::vector<unsigned>> seen[4];
+                for (auto &sf : seen) sf.assign(nb, {});
                 auto add = [&](int o) {
                     for (int f = 0; f < 4; ++f) {
                         const unsigned a = word(o, f);
-                        auto &s2 = seen[f][a % 32];
+                        auto &s2 = seen[f][a % nb];
                         if (std::find(s2.begin(), s2.end(), a) == s2.end()) s2.push_back(a);
                     }
                 };
@@ -386,7 +391,7 @@ struct ProgramBuilder {
                     if (slot[t][j] >= 0) continue;
                     int bb = -1, bi = -1;
                     long long bc = 0;
-                    for (int bk = 0; bk < 32 && !(bb >= 0 && bc == 0); ++bk) {
+                    for (int bk = 0; bk < (int)nb && !(bb >= 0 && bc == 0); ++bk) {
                         auto &b = bucket[bk];
                         if (!seen[0][bk].empty() && bb >= 0 && bc <= 2 * (long long)seen[0][bk].size()) continue;
                         for (int u = 0; u < (int)b.size(); ++u) {
@@ -394,7 +399,7 @@ struct ProgramBuilder {
                             long long cost = 0;
                             for (int f = 0; f < 4; ++f) {
                                 const unsigned a = word(o, f);
-                                const auto &s2 = seen[f][a % 32];
+                                const auto &s2 = seen[f][a % nb];
                                 if (std::find(s2.begin(), s2.end(), a) == s2.end()) cost += (f == 0 ? 2 : 1) * (long long)s2.size();
                             }
                             if (bb < 0 || cost < bc) { bb = bk; bi = u; bc = cost; }
@@ -765,6 +770,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         ProgramBuilder B(P.factor, opt.threads);
         B.lu_base = compact_lu_offset(m);
         B.vdummy = m;
+        B.lanes = opt.elem_bytes == 8 ? 16 : 32;
         for (int l = 0; l < nplev; ++l) {
             B.begin();
             if (l < nlev)
@@ -805,6 +811,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         ProgramBuilder B(P.backward, opt.threads);
         B.lu_base = compact_lu_offset(m);
         B.vdummy = m;
+        B.lanes = opt.elem_bytes == 8 ? 16 : 32;
         for (int l = 0; l < nb; ++l) {
             B.begin();
             for (int k : byb[l])
@@ -828,6 +835,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         ProgramBuilder B(P.forward, opt.threads);
         B.lu_base = compact_lu_offset(m);
         B.vdummy = m;
+        B.lanes = opt.elem_bytes == 8 ? 16 : 32;
         for (int l = 0; l < nf; ++l) {
             B.begin();
             for (int k : byf[l])

@@ -129,6 +129,7 @@ struct PlanOptions {
     double pivot_threshold = 1e-3;    // diagonal preference of the first factorisation
     bool fuse_forward = true;         // fuse the forward substitution into the refactorisation
     int threads = 512;                // CTA size the phase programs are laid out for
+    int elem_bytes = 4;               // LU element size of the packed programs' bank placement
     int order_trials = 8;             // > 0: minimum degree of this many relabellings, each followed
                                       // by its least-depth equivalent, the shallowest kept; 0:
                                       // minimum degree only
