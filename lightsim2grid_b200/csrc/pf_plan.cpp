@@ -727,6 +727,11 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         msg = "build_plan: LU too large for the operation encoding";
         return SolverAnalyze;
     }
+    // the bank placement serves the packed layout: only where its 16-bit indices fit and the
+    // LU, at the plan's element size, can fit the 227 KB of shared memory of a CTA
+    const int packed_lu_base = compact_fits(P) && (size_t)(compact_lu_offset(m) + P.nnzLU) * opt.elem_bytes <= 232448
+                                   ? compact_lu_offset(m)
+                                   : -1;
     // U row lists: for pivot c, the columns j > c with U(c, j) != 0 and the position of U(c, j)
     std::vector<std::vector<std::pair<int, int>>> urows(m);
     for (int k = 0; k < m; ++k)
@@ -768,7 +773,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
     std::vector<int> rowpos(m, -1);
     {
         ProgramBuilder B(P.factor, opt.threads);
-        B.lu_base = compact_lu_offset(m);
+        B.lu_base = packed_lu_base;
         B.vdummy = m;
         B.lanes = opt.elem_bytes == 8 ? 16 : 32;
         for (int l = 0; l < nplev; ++l) {
@@ -809,7 +814,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         // z(k) is kept undivided by U(k, k): a push divides by the pivot, and one scaling pass
         // after the program divides every z(k) (no per-pivot division operations)
         ProgramBuilder B(P.backward, opt.threads);
-        B.lu_base = compact_lu_offset(m);
+        B.lu_base = packed_lu_base;
         B.vdummy = m;
         B.lanes = opt.elem_bytes == 8 ? 16 : 32;
         for (int l = 0; l < nb; ++l) {
@@ -833,7 +838,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         for (int k = 0; k < m; ++k) byf[flev[k]].push_back(k);
         P.levels_fwd = nf;
         ProgramBuilder B(P.forward, opt.threads);
-        B.lu_base = compact_lu_offset(m);
+        B.lu_base = packed_lu_base;
         B.vdummy = m;
         B.lanes = opt.elem_bytes == 8 ? 16 : 32;
         for (int l = 0; l < nf; ++l) {
