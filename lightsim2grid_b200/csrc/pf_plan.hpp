@@ -5,12 +5,15 @@
 //     (src/powerflow_algorithm/BaseNRSingleSlackAlgo.tpp:247-378 for a single slack,
 //     BaseNRAlgo.tpp:396-555 for a distributed slack) and the value map from Ybus entries
 //     to J entries (BaseNRSingleSlackAlgo.tpp:385-447, BaseNRAlgo.tpp:562-635);
-//   * a fill-reducing column order (minimum degree on J + J^T) and the row pivots of a
+//   * a fill-reducing column order (minimum degree on J + J^T, then the equivalent order of
+//     least elimination depth, the shallowest of several relabellings) and the row pivots of a
 //     threshold-partial-pivoting Gilbert-Peierls factorisation of the first Jacobian --
 //     the same contract as the reference's KLU::initialize (src/linear_solvers/KLUSolver.cpp:24-45):
 //     later Jacobians are refactorised with these pivots;
 //   * the device schedules: the LU value layout and the phase programs of the
-//     refactorisation and of both triangular solves.
+//     refactorisation and of both triangular solves (longest-first placement for the global-LU
+//     kernels, a bank-conflict placement of the same operations for the packed shared-memory
+//     layout).
 #pragma once
 
 #include <complex>
