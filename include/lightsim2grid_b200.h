@@ -90,6 +90,11 @@ typedef struct pf_plan_info {
     long long flops_refactor;  /* multiply-adds of one refactorisation */
     int precision, threads, lu_in_shared, ctas_per_sm, grid;
     long long slab_bytes, shared_bytes;
+    /* shared-memory wavefronts of one run of the factor, backward and forward programs in the
+       packed layout (the LU in shared memory), from the bank model the programs are placed
+       for: per group of lanes the banks serve together and per operand, the most distinct
+       words in one bank.  0 when the plan's LU is not in shared memory.                       */
+    long long smem_wavefronts_factor, smem_wavefronts_backward, smem_wavefronts_forward;
 } pf_plan_info;
 
 /* A batch whose inputs and outputs are already in device memory (pointers from

@@ -31,7 +31,9 @@ class PfPlanInfo(ctypes.Structure):
                 ("groups_forward", ctypes.c_int), ("groups_backward", ctypes.c_int),
                 ("flops_refactor", ctypes.c_longlong), ("precision", ctypes.c_int), ("threads", ctypes.c_int),
                 ("lu_in_shared", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("grid", ctypes.c_int),
-                ("slab_bytes", ctypes.c_longlong), ("shared_bytes", ctypes.c_longlong)]
+                ("slab_bytes", ctypes.c_longlong), ("shared_bytes", ctypes.c_longlong),
+                ("smem_wavefronts_factor", ctypes.c_longlong), ("smem_wavefronts_backward", ctypes.c_longlong),
+                ("smem_wavefronts_forward", ctypes.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -1019,6 +1019,10 @@ int pf_plan_info_get(const pf_plan *pl, pf_plan_info *info) {
     info->grid = pl->grid;
     info->slab_bytes = (long long)pl->slab;
     info->shared_bytes = (long long)pl->smem;
+    const bool packed = pl->lu_in_smem && !P.fdpf;
+    info->smem_wavefronts_factor = packed ? l2g::smem_wavefronts(P, P.factor) : 0;
+    info->smem_wavefronts_backward = packed ? l2g::smem_wavefronts(P, P.backward) : 0;
+    info->smem_wavefronts_forward = packed ? l2g::smem_wavefronts(P, P.forward) : 0;
     return 0;
 }
 
@@ -1641,6 +1645,10 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         info->groups_forward = P.forward.nphases();
         info->groups_backward = P.backward.nphases();
         info->flops_refactor = P.flops_refactor;
+        // the packed layout's bank model, where the plan has one (FP32 element size here)
+        info->smem_wavefronts_factor = l2g::smem_wavefronts(P, P.factor);
+        info->smem_wavefronts_backward = l2g::smem_wavefronts(P, P.backward);
+        info->smem_wavefronts_forward = l2g::smem_wavefronts(P, P.forward);
     }
     return 0;
 }

@@ -446,6 +446,34 @@ void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out, int
     }
 }
 
+long long smem_wavefronts(const Plan &P, const Plan::Program &pr) {
+    const int G = P.bank_lanes;
+    if (G <= 0) return 0;
+    std::vector<unsigned> c;
+    compact_ops(pr, P.m, c, -1);
+    long long total = 0;
+    std::vector<unsigned> u;
+    for (int p = 0; p < pr.nphases(); ++p) {
+        const int b0 = pr.base[p], w = pr.width[p], len = (pr.base[p + 1] - b0) / w;
+        for (int j = 0; j < len; ++j)
+            for (int q = 0; q < w; q += G)
+                for (int f = 0; f < 4; ++f) {
+                    u.clear();
+                    for (int t = q; t < std::min(w, q + G); ++t) {
+                        const size_t o = (size_t)b0 + t + (size_t)j * w;
+                        const unsigned v = (f & 1) ? c[2 * o + (f >> 1)] >> 16 : c[2 * o + (f >> 1)] & 0xffffu;
+                        u.push_back(v);
+                    }
+                    std::sort(u.begin(), u.end());
+                    u.erase(std::unique(u.begin(), u.end()), u.end());
+                    int cnt[32] = {0}, mx = 0;
+                    for (unsigned v : u) mx = std::max(mx, ++cnt[v % G]);
+                    total += (f == 0 ? 2 : 1) * (long long)mx;
+                }
+    }
+    return total;
+}
+
 void build_tile_program(const Plan::Program &pr, int nwarps, int chunk, TileProgram &out) {
     out.ops.clear();
     out.phase.clear();
@@ -732,6 +760,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
     const int packed_lu_base = compact_fits(P) && (size_t)(compact_lu_offset(m) + P.nnzLU) * opt.elem_bytes <= 232448
                                    ? compact_lu_offset(m)
                                    : -1;
+    P.bank_lanes = packed_lu_base >= 0 ? (opt.elem_bytes == 8 ? 16 : 32) : 0;
     // U row lists: for pivot c, the columns j > c with U(c, j) != 0 and the position of U(c, j)
     std::vector<std::vector<std::pair<int, int>>> urows(m);
     for (int k = 0; k < m; ++k)

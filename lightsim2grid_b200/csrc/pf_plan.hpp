@@ -117,6 +117,7 @@ struct Plan {
     // statistics
     long long flops_refactor = 0;     // multiply-adds of one refactorisation
     int levels_refactor = 0, levels_fwd = 0, levels_bwd = 0;
+    int bank_lanes = 0;               // lanes per bank group of the packed placement; 0: none built
 
     // ------------------------------------------------------------ fast decoupled
     // FDPF plan: the Ybus data above drive the mismatch; sub[0] is B' over pvpq, sub[1] B''
@@ -155,6 +156,10 @@ void compact_ops(const Plan::Program &pr, int m, std::vector<unsigned> &out, int
 // Index-space offsets of the B' and B'' LUs of a fast-decoupled plan behind their shared solve
 // vector, and whether both fit the 16-bit packed indices.
 void fdpf_lu_offsets(const Plan &P, int &off0, int &off1, bool &fits);
+// Shared-memory wavefronts of one run of a packed program (the plan's default layout): per
+// group of P.bank_lanes lanes and slot, per operand (the written word twice: loaded and stored),
+// the most distinct words in one bank.  0 when the plan has no packed placement.
+long long smem_wavefronts(const Plan &P, const Plan::Program &pr);
 
 // Builds a DC plan (BaseDCAlgo, src/powerflow_algorithm/BaseDCAlgo.tpp): the matrix is
 // B = Re(Ybus) over every bus except the first slack (the other slacks count as PV), factorised

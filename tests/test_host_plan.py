@@ -109,6 +109,19 @@ def test_default_order_is_shallow():
     assert np.all(np.isfinite(x))
 
 
+def test_packed_programs_are_placed_for_few_bank_conflicts():
+    """The packed factor program of the 2848-bus plan (FP32, LU in shared memory) makes about
+    35k shared-memory wavefronts per run under the bank model it is placed for; the longest-first
+    placement made 52k, and no placement can go below one wavefront per operand and warp-slot."""
+    c = grid_problem("grid2848")
+    m = 2 * len(c["pq"]) + len(c["pv"])
+    _, info = host_schedule_solve(c, c["V0"], np.ones(m), False)
+    floor = 5 * (info.flops_refactor + info.nnz_lu) // 32  # operations (updates + pushes) / warp
+    assert floor < info.smem_wavefronts_factor <= 37000
+    assert 0 < info.smem_wavefronts_backward <= 8500
+    assert 0 < info.smem_wavefronts_forward <= 10000
+
+
 def test_invalid_inputs_are_rejected():
     lib = nat.load()
     c = grid_problem("grid14")
