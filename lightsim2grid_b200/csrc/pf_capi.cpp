@@ -1519,42 +1519,56 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
     };
     const std::vector<double> lu0 = lu, xs0 = xs;
     // the bank-conflict placement of the packed programs gives the same bits: every written
-    // value keeps its thread and the order of its operations
+    // value keeps its thread and the order of its operations.  Checked for the placement of this
+    // plan (4-byte words) and for the one of the same plan built for 8-byte words (FP64).
     {
-        std::vector<double> lb = lu, xb = xs;
-        auto run_banked = [&](const l2g::Plan::Program &pr) {
-            const std::vector<int> &ops = pr.ops_banked.empty() ? pr.ops : pr.ops_banked;
-            for (int o = 0; o < pr.nops(); ++o) {
-                const int X = ops[4 * o], Y = ops[4 * o + 1], Z = ops[4 * o + 2];
-                const int W = ops[4 * o + 3] & 0x0fffffff, kind = (unsigned)ops[4 * o + 3] >> 28;
-                if (kind == 0) lb[X] -= lb[Y] * (lb[Z] / lb[W]);
-                else if (kind == 2) xb[X] -= lb[Y] * xb[Z] / lb[W];
-            }
-        };
-        run_banked(P.factor);
-        run_banked(P.backward);
-        std::vector<double> la = lu, xa = xs;
+        std::vector<double> la = lu, xa = xs, xf = xs;  // longest-first: factor + backward; forward
         std::swap(la, lu);
         std::swap(xa, xs);
         run(P.factor);
         run(P.backward);
-        std::swap(la, lu);
         std::swap(xa, xs);
-        for (int p = 0; p < P.nnzLU; ++p)
-            if (lb[p] != la[p]) return fail(-1, "schedule check: bank-placed factor program disagrees");
-        for (int k = 0; k < m; ++k)
-            if (xb[k] != xa[k]) return fail(-1, "schedule check: bank-placed substitution programs disagree");
-        // the stand-alone forward program, on the factor just computed
-        xb = xs;
-        run_banked(P.forward);
+        std::swap(xf, xs);
+        run(P.forward);  // on the factor just computed
+        std::swap(xf, xs);
         std::swap(la, lu);
-        xa = xs;
-        std::swap(xa, xs);
-        run(P.forward);
-        std::swap(xa, xs);
-        std::swap(la, lu);
-        for (int k = 0; k < m; ++k)
-            if (xb[k] != xa[k]) return fail(-1, "schedule check: bank-placed forward program disagrees");
+        l2g::Plan P8;
+        const l2g::Plan *variants[2] = {&P, nullptr};
+        if (P.bank_lanes > 0) {
+            l2g::PlanOptions po8 = po;
+            po8.elem_bytes = 8;
+            std::string msg8;
+            if (l2g::build_plan(P8, n, colptr, rowind, reinterpret_cast<const cplx *>(ybus_ri),
+                                reinterpret_cast<const cplx *>(V0_ri), S.data(), slack_ids, nslack, slack_weights, pv,
+                                npv, pq, npq, distributed != 0, po8, msg8) == 0 &&
+                P8.factor.ops == P.factor.ops && P8.backward.ops == P.backward.ops && P8.forward.ops == P.forward.ops)
+                variants[1] = &P8;
+            else
+                return fail(-1, "schedule check: the plan built for 8-byte words differs");
+        }
+        for (const l2g::Plan *Q : variants) {
+            if (!Q) continue;
+            std::vector<double> lb = lu, xb = xs;
+            auto run_banked = [&](const l2g::Plan::Program &pr) {
+                const std::vector<int> &ops = pr.ops_banked.empty() ? pr.ops : pr.ops_banked;
+                for (int o = 0; o < pr.nops(); ++o) {
+                    const int X = ops[4 * o], Y = ops[4 * o + 1], Z = ops[4 * o + 2];
+                    const int W = ops[4 * o + 3] & 0x0fffffff, kind = (unsigned)ops[4 * o + 3] >> 28;
+                    if (kind == 0) lb[X] -= lb[Y] * (lb[Z] / lb[W]);
+                    else if (kind == 2) xb[X] -= lb[Y] * xb[Z] / lb[W];
+                }
+            };
+            run_banked(Q->factor);
+            run_banked(Q->backward);
+            for (int p = 0; p < P.nnzLU; ++p)
+                if (lb[p] != la[p]) return fail(-1, "schedule check: bank-placed factor program disagrees");
+            for (int k = 0; k < m; ++k)
+                if (xb[k] != xa[k]) return fail(-1, "schedule check: bank-placed substitution programs disagree");
+            xb = xs;
+            run_banked(Q->forward);
+            for (int k = 0; k < m; ++k)
+                if (xb[k] != xf[k]) return fail(-1, "schedule check: bank-placed forward program disagrees");
+        }
     }
     run(P.factor);
     for (int k = 0; k < m; ++k)
