@@ -375,8 +375,10 @@ int pf_host_jacobian_pattern(int n, const int *colptr, const int *rowind, const 
 
 /* Runs the device schedules (refactorisation update lists and level order, forward and
    backward substitution level order) sequentially on the host: factorises J(V) with the pivots
-   chosen at V0 and solves J x = b.  b and x are in J row / column numbering (length m).  Used
-   to test a plan's schedules on machines without a GPU. */
+   chosen at V0 and solves J x = b.  b and x are in J row / column numbering (length m).  Also
+   checks that the packed, bank-placed (for 4- and 8-byte words) and batch-interleaved forms of
+   the programs give the results of the plain ones.  Used to test a plan's schedules on machines
+   without a GPU. */
 int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const double *ybus_ri, const double *V0_ri,
                            const double *V_ri, const int *slack_ids, int nslack, const double *slack_weights,
                            const int *pv, int npv, const int *pq, int npq, int distributed, const double *b,
