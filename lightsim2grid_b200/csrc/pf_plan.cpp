@@ -237,7 +237,9 @@ std::vector<int> shallow_order(int m, const std::vector<int> &Ap, const std::vec
 // are no write conflicts, no atomics and a deterministic summation order); clusters are
 // spread over the threads longest-first onto the least loaded thread.  A phase is stored
 // with stride `width` (threads that have work): thread t < width runs operations
-// base + t, base + t + width, ...; shorter threads are padded with empty operations.
+// base + t, base + t + width, ...; shorter threads are padded with empty operations.  With
+// `lu_base` set, the same operations are also stored in a second placement (`ops_banked`, same
+// phases, widths and lengths) chosen for few shared-memory bank conflicts in the packed layout.
 struct ProgramBuilder {
     Plan::Program &prog;
     int nt;
