@@ -2,12 +2,38 @@
 #include "pf_plan.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <sstream>
+#include <system_error>
+#include <thread>
 
 namespace l2g {
 
 namespace {
+
+// Runs f(0) ... f(n-1) on up to 8 host threads (the calls must be independent); on one thread
+// when threads cannot be started.
+template <typename F>
+void parallel_for(int n, F f) {
+    const int nt = std::min<int>(n, std::max(1, std::min(8, (int)std::thread::hardware_concurrency())));
+    if (nt <= 1) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<int> next(0);
+    auto worker = [&]() {
+        for (int i = next++; i < n; i = next++) f(i);
+    };
+    std::vector<std::thread> pool;
+    try {
+        for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    } catch (const std::system_error &) {
+        // fewer threads: the calling thread and those started share the rest
+    }
+    worker();
+    for (auto &th : pool) th.join();
+}
 
 // -------------------------------------------------------------------------------------
 // Minimum-degree ordering on the symmetric pattern of A + A^T.
@@ -195,23 +221,29 @@ int symbolic_depth(int m, const std::vector<int> &Ap, const std::vector<int> &Ai
 // varies with those choices: orders of `trials` relabellings (the identity first, then seeded
 // shuffles) are compared and the shallowest kept (then the least fill).
 std::vector<int> shallow_order(int m, const std::vector<int> &Ap, const std::vector<int> &Ai, int trials) {
-    std::vector<int> best;
-    int bdepth = 0;
-    long long bfill = 0;
+    const int T = std::max(1, trials);
+    // the relabellings, drawn in sequence from one seed (the identity first)
+    std::vector<std::vector<int>> perm(T, std::vector<int>(m));
     unsigned seed = 0x2545f491u;
-    std::vector<int> perm(m), inv(m);
-    for (int t = 0; t < std::max(1, trials); ++t) {
-        for (int i = 0; i < m; ++i) perm[i] = i;
+    for (int t = 0; t < T; ++t) {
+        for (int i = 0; i < m; ++i) perm[t][i] = i;
         if (t > 0)
             for (int i = m - 1; i > 0; --i) {
                 seed = seed * 1664525u + 1013904223u;
-                std::swap(perm[i], perm[(seed >> 8) % (unsigned)(i + 1)]);
+                std::swap(perm[t][i], perm[t][(seed >> 8) % (unsigned)(i + 1)]);
             }
-        for (int i = 0; i < m; ++i) inv[perm[i]] = i;
-        // the pattern with vertex i labelled perm[i]
+    }
+    std::vector<std::vector<int>> q(T);
+    std::vector<int> depth(T);
+    std::vector<long long> fill(T);
+    parallel_for(T, [&](int t) {
+        const std::vector<int> &pm = perm[t];
+        std::vector<int> inv(m);
+        for (int i = 0; i < m; ++i) inv[pm[i]] = i;
+        // the pattern with vertex i labelled pm[i]
         std::vector<std::vector<int>> cols(m);
         for (int j = 0; j < m; ++j)
-            for (int p = Ap[j]; p < Ap[j + 1]; ++p) cols[perm[j]].push_back(perm[Ai[p]]);
+            for (int p = Ap[j]; p < Ap[j + 1]; ++p) cols[pm[j]].push_back(pm[Ai[p]]);
         std::vector<int> Bp(m + 1, 0), Bi;
         Bi.reserve(Ai.size());
         for (int j = 0; j < m; ++j) {
@@ -219,17 +251,14 @@ std::vector<int> shallow_order(int m, const std::vector<int> &Ap, const std::vec
             Bi.insert(Bi.end(), cols[j].begin(), cols[j].end());
             Bp[j + 1] = (int)Bi.size();
         }
-        std::vector<int> q = low_height_order(m, Bp, Bi, minimum_degree(m, Bp, Bi));
-        for (int &v : q) v = inv[v];
-        long long fill;
-        const int depth = symbolic_depth(m, Ap, Ai, q, fill);
-        if (best.empty() || depth < bdepth || (depth == bdepth && fill < bfill)) {
-            best = q;
-            bdepth = depth;
-            bfill = fill;
-        }
-    }
-    return best;
+        q[t] = low_height_order(m, Bp, Bi, minimum_degree(m, Bp, Bi));
+        for (int &v : q[t]) v = inv[v];
+        depth[t] = symbolic_depth(m, Ap, Ai, q[t], fill[t]);
+    });
+    int best = 0;
+    for (int t = 1; t < T; ++t)
+        if (depth[t] < depth[best] || (depth[t] == depth[best] && fill[t] < fill[best])) best = t;
+    return q[best];
 }
 
 // Builds one phase program, level after level.  All operations of a level that write the
@@ -251,6 +280,14 @@ struct ProgramBuilder {
     int vdummy = 0;                // index of the empty operations' scratch slot
     int lanes = 32;                // lanes served together by the shared-memory banks: a warp for
                                    // 4-byte words, a half-warp for 8-byte words (16 bank pairs)
+    // one bank placement per phase, computed by finish() on host threads
+    struct BankJob {
+        std::vector<int> ops, cfirst, ccount, idx;
+        std::vector<std::vector<int>> per;  // the longest-first placement (the fallback)
+        int width = 0, len = 0;
+        size_t at = 0;  // first int of the phase in ops_banked
+    };
+    std::vector<BankJob> jobs;
 
     ProgramBuilder(Plan::Program &p, int threads) : prog(p), nt(threads) {
         prog.ops.clear();
@@ -302,35 +339,53 @@ struct ProgramBuilder {
         int len = 0;
         for (auto &v : per) len = std::max(len, (int)v.size());
         for (auto &v : per) v.resize(len, -1);
-        emit(prog.ops, per, width, len);
+        prog.ops.resize(prog.ops.size() + 4 * (size_t)width * len);
+        emit(prog.ops.data() + prog.ops.size() - 4 * (size_t)width * len, ops, per, width, len);
         if (lu_base >= 0) {
-            std::vector<int> cfirst, ccount;
+            BankJob jb;
+            jb.ops = ops;
             for (const Cl &c : cl) {
-                cfirst.push_back(c.first);
-                ccount.push_back(c.count);
+                jb.cfirst.push_back(c.first);
+                jb.ccount.push_back(c.count);
             }
-            const auto slot = assign_banked(cfirst, ccount, idx, width, len);
-            emit(prog.ops_banked, slot.empty() ? per : slot, width, len);
+            jb.idx = idx;
+            jb.per = std::move(per);
+            jb.width = width;
+            jb.len = len;
+            jb.at = prog.ops_banked.size();
+            prog.ops_banked.resize(prog.ops_banked.size() + 4 * (size_t)width * len);
+            jobs.push_back(std::move(jb));
         }
         prog.width.push_back(width);
         prog.base.push_back((int)(prog.ops.size() / 4));
     }
 
-    // appends a phase: slot j of thread t at j * width + t (-1: empty operation)
-    void emit(std::vector<int> &out, const std::vector<std::vector<int>> &slot, int width, int len) const {
+    // the bank placements of all phases, each into its own range of ops_banked
+    void finish() {
+        parallel_for((int)jobs.size(), [&](int i) {
+            const BankJob &jb = jobs[i];
+            const auto slot = assign_banked(jb.ops, jb.cfirst, jb.ccount, jb.idx, jb.width, jb.len);
+            emit(prog.ops_banked.data() + jb.at, jb.ops, slot.empty() ? jb.per : slot, jb.width, jb.len);
+        });
+        jobs.clear();
+    }
+
+    // writes a phase: slot j of thread t at j * width + t (-1: empty operation)
+    static void emit(int *out, const std::vector<int> &src, const std::vector<std::vector<int>> &slot, int width,
+                     int len) {
         for (int j = 0; j < len; ++j)
-            for (int t = 0; t < width; ++t) {
+            for (int t = 0; t < width; ++t, out += 4) {
                 const int o = slot[t][j];
-                if (o >= 0) out.insert(out.end(), ops.begin() + 4 * o, ops.begin() + 4 * o + 4);
+                if (o >= 0) std::copy(src.begin() + 4 * o, src.begin() + 4 * o + 4, out);
                 else {
                     const int none[4] = {0, 0, 0, 7 << 28};
-                    out.insert(out.end(), none, none + 4);
+                    std::copy(none, none + 4, out);
                 }
             }
     }
 
     // shared-memory word of field f (0 x, 1 y, 2 z, 3 w) of operation o in the packed layout
-    unsigned word(int o, int f) const {
+    unsigned word(const std::vector<int> &ops, int o, int f) const {
         const int kind = (unsigned)ops[4 * o + 3] >> 28;
         const int v = f == 3 ? (ops[4 * o + 3] & 0x0fffffff) : ops[4 * o + f];
         if (kind == 0) return (unsigned)(lu_base + v);
@@ -347,8 +402,9 @@ struct ProgramBuilder {
     // lane taking the candidate that adds the fewest conflicts (the written word counts twice:
     // loaded and stored).  Greedy, with the search cut where a bank's written-word conflicts alone
     // reach the best cost found.
-    std::vector<std::vector<int>> assign_banked(const std::vector<int> &cfirst, const std::vector<int> &ccount,
-                                                const std::vector<int> &idx, int width, int len) const {
+    std::vector<std::vector<int>> assign_banked(const std::vector<int> &ops, const std::vector<int> &cfirst,
+                                                const std::vector<int> &ccount, const std::vector<int> &idx,
+                                                int width, int len) const {
         const int ncl = (int)cfirst.size();
         std::vector<std::vector<int>> slot(width);
         std::vector<int> fill(width, 0);
@@ -371,7 +427,7 @@ struct ProgramBuilder {
         const unsigned nb = (unsigned)lanes;  // banks (or bank pairs) per group of lanes
         std::vector<std::vector<int>> bucket(nb);
         for (int c = 0; c < ncl; ++c)
-            if (ccount[c] == 1) bucket[word(idx[cfirst[c]], 0) % nb].push_back(idx[cfirst[c]]);
+            if (ccount[c] == 1) bucket[word(ops, idx[cfirst[c]], 0) % nb].push_back(idx[cfirst[c]]);
         for (auto &b : bucket) std::reverse(b.begin(), b.end());  // pop from the back in order
         int left = 0;
         for (auto &b : bucket) left += (int)b.size();
@@ -382,7 +438,7 @@ struct ProgramBuilder {
                 for (auto &sf : seen) sf.assign(nb, {});
                 auto add = [&](int o) {
                     for (int f = 0; f < 4; ++f) {
-                        const unsigned a = word(o, f);
+                        const unsigned a = word(ops, o, f);
                         auto &s2 = seen[f][a % nb];
                         if (std::find(s2.begin(), s2.end(), a) == s2.end()) s2.push_back(a);
                     }
@@ -400,7 +456,7 @@ struct ProgramBuilder {
                             const int o = b[b.size() - 1 - u];
                             long long cost = 0;
                             for (int f = 0; f < 4; ++f) {
-                                const unsigned a = word(o, f);
+                                const unsigned a = word(ops, o, f);
                                 const auto &s2 = seen[f][a % nb];
                                 if (std::find(s2.begin(), s2.end(), a) == s2.end()) cost += (f == 0 ? 2 : 1) * (long long)s2.size();
                             }
@@ -828,6 +884,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
                 for (int t = 0; t < P.lcount[k]; ++t) B.add(Lrows[k][t], P.lstart[k] + t, k, P.dpos[k], 2);
             B.end();
         }
+        B.finish();
     }
     {
         // backward substitution U z = y, from the last pivot: blevel(k) = 1 + max over U(k, j)
@@ -854,6 +911,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
                 for (int p = P.colstart[k]; p < P.dpos[k]; ++p) B.add(P.Urow_k[p], p, k, P.dpos[k], 2);
             B.end();
         }
+        B.finish();
     }
     {
         // forward substitution L y = b on its own: flevel(k) = 1 + max over L(k, k')
@@ -878,6 +936,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
                 for (int t = 0; t < P.lcount[k]; ++t) B.add(Lrows[k][t], P.lstart[k] + t, k, P.dpos[k], 2);
             B.end();
         }
+        B.finish();
     }
 
     // ---------------------------------------------------------------- J fill maps
