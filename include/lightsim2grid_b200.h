@@ -50,6 +50,10 @@ typedef struct pf_options {
                                equivalent reordering of least depth (no added fill, fewer
                                dependent phases), the shallowest kept; 1: minimum degree only;
                                2: minimum degree and its least-depth equivalent, one labelling */
+    int placement;          /* packed programs (LU in shared memory): 0 default, clusters of
+                               operations writing one value in their thread's first slots; 1
+                               clusters spread over the phase's slots (fewer bank conflicts in
+                               the host model, longer plan build).  Same results either way     */
 } pf_options;
 
 /* DC power flow plan (BaseDCAlgo::compute_pf, src/powerflow_algorithm/BaseDCAlgo.tpp:5-175;

@@ -21,7 +21,7 @@ class PfOptions(ctypes.Structure):
                 ("fuse_forward", ctypes.c_int), ("pivot_threshold", ctypes.c_double),
                 ("fp64_fallback", ctypes.c_int), ("max_ctas_per_sm", ctypes.c_int), ("refine", ctypes.c_int),
                 ("refine_threshold", ctypes.c_double), ("lu_reuse_threshold", ctypes.c_double),
-                ("batch_layout", ctypes.c_int), ("ordering", ctypes.c_int)]
+                ("batch_layout", ctypes.c_int), ("ordering", ctypes.c_int), ("placement", ctypes.c_int)]
 
 
 class PfPlanInfo(ctypes.Structure):

@@ -864,6 +864,7 @@ int pf_plan_create(int n, const int *colptr, const int *rowind, const double *yb
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
     po.elem_bytes = pl->opt.precision ? 4 : 8;
+    po.spread_clusters = pl->opt.placement == 1;
     {
         const int m_est = npv + (distributed && nslack > 1 ? nslack - 1 : 0) + 2 * npq + (distributed ? 1 : 0);
         int thr = pl->opt.threads;
@@ -903,6 +904,7 @@ int pf_dc_plan_create(int n, const int *colptr, const int *rowind, const double 
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
     po.elem_bytes = pl->opt.precision ? 4 : 8;
+    po.spread_clusters = pl->opt.placement == 1;
     int thr = pl->opt.threads;
     if (thr <= 0) thr = n > 2000 ? 512 : (n > 300 ? 256 : 128);
     thr = std::max(32, std::min(512, (thr / 32) * 32));
@@ -939,6 +941,7 @@ int pf_fdpf_plan_create(int n, const int *colptr, const int *rowind, const doubl
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
     po.elem_bytes = pl->opt.precision ? 4 : 8;
+    po.spread_clusters = pl->opt.placement == 1;
     int thr = pl->opt.threads;
     if (thr <= 0) {
         // factors in global memory, read through L1 by every CTA of an SM, and several small
@@ -1520,7 +1523,7 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
     const std::vector<double> lu0 = lu, xs0 = xs;
     // the bank-conflict placement of the packed programs gives the same bits: every written
     // value keeps its thread and the order of its operations.  Checked for the placement of this
-    // plan (4-byte words) and for the one of the same plan built for 8-byte words (FP64).
+    // plan (4-byte words), for the one built for 8-byte words (FP64) and for the spread clusters.
     {
         std::vector<double> la = lu, xa = xs, xf = xs;  // longest-first: factor + backward; forward
         std::swap(la, lu);
@@ -1532,19 +1535,24 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         run(P.forward);  // on the factor just computed
         std::swap(xf, xs);
         std::swap(la, lu);
-        l2g::Plan P8;
-        const l2g::Plan *variants[2] = {&P, nullptr};
+        // the same plan built for 8-byte words, and with the clusters spread over the slots
+        l2g::Plan P8, Ps;
+        const l2g::Plan *variants[3] = {&P, nullptr, nullptr};
         if (P.bank_lanes > 0) {
-            l2g::PlanOptions po8 = po;
-            po8.elem_bytes = 8;
-            std::string msg8;
-            if (l2g::build_plan(P8, n, colptr, rowind, reinterpret_cast<const cplx *>(ybus_ri),
-                                reinterpret_cast<const cplx *>(V0_ri), S.data(), slack_ids, nslack, slack_weights, pv,
-                                npv, pq, npq, distributed != 0, po8, msg8) == 0 &&
-                P8.factor.ops == P.factor.ops && P8.backward.ops == P.backward.ops && P8.forward.ops == P.forward.ops)
-                variants[1] = &P8;
-            else
-                return fail(-1, "schedule check: the plan built for 8-byte words differs");
+            l2g::Plan *Q[2] = {&P8, &Ps};
+            for (int v = 0; v < 2; ++v) {
+                l2g::PlanOptions pv2 = po;
+                if (v == 0) pv2.elem_bytes = 8;
+                else pv2.spread_clusters = true;
+                std::string msg2;
+                if (l2g::build_plan(*Q[v], n, colptr, rowind, reinterpret_cast<const cplx *>(ybus_ri),
+                                    reinterpret_cast<const cplx *>(V0_ri), S.data(), slack_ids, nslack, slack_weights,
+                                    pv, npv, pq, npq, distributed != 0, pv2, msg2) != 0 ||
+                    Q[v]->factor.ops != P.factor.ops || Q[v]->backward.ops != P.backward.ops ||
+                    Q[v]->forward.ops != P.forward.ops)
+                    return fail(-1, "schedule check: a placement variant of the plan differs");
+                variants[1 + v] = Q[v];
+            }
         }
         for (const l2g::Plan *Q : variants) {
             if (!Q) continue;

@@ -280,6 +280,7 @@ struct ProgramBuilder {
     int vdummy = 0;                // index of the empty operations' scratch slot
     int lanes = 32;                // lanes served together by the shared-memory banks: a warp for
                                    // 4-byte words, a half-warp for 8-byte words (16 bank pairs)
+    bool spread = false;           // clusters spread over the phase's slots (else first slots)
     // one bank placement per phase, computed by finish() on host threads
     struct BankJob {
         std::vector<int> ops, cfirst, ccount, idx;
@@ -396,35 +397,108 @@ struct ProgramBuilder {
     // Places the level's operations on (thread, slot), `len` slots per thread, so that the 32
     // operations a warp runs together touch few shared-memory words per bank (4-byte words: 32
     // banks per warp; 8-byte words: 16 bank pairs per half-warp; lanes reading one word share
-    // it).  Operations writing one value (clusters of two or
-    // more) run consecutively on one thread, placed first onto the least loaded threads as in the
-    // LPT placement; the single operations then fill the free slots warp-slot by warp-slot, each
-    // lane taking the candidate that adds the fewest conflicts (the written word counts twice:
-    // loaded and stored).  Greedy, with the search cut where a bank's written-word conflicts alone
-    // reach the best cost found.
+    // it).  Operations writing one value (clusters of two or more) run on one thread in order,
+    // placed first onto the least loaded threads as in the LPT placement: in the thread's first
+    // slots, or (`spread`) each in the slot of least conflict after the previous one.  The single
+    // operations then fill the free slots warp-slot by warp-slot, each lane taking the candidate
+    // that adds the fewest conflicts (the written word counts twice: loaded and stored).  Greedy,
+    // with the search cut where a bank's written-word conflicts alone reach the best cost found.
     std::vector<std::vector<int>> assign_banked(const std::vector<int> &ops, const std::vector<int> &cfirst,
                                                 const std::vector<int> &ccount, const std::vector<int> &idx,
                                                 int width, int len) const {
         const int ncl = (int)cfirst.size();
+        const unsigned nb = (unsigned)lanes;  // banks (or bank pairs) per group of lanes
         std::vector<std::vector<int>> slot(width);
         std::vector<int> fill(width, 0);
-        std::vector<std::pair<int, int>> heap;
-        for (int t = 0; t < width; ++t) heap.push_back({0, t});
-        auto cmp = [](const std::pair<int, int> &a, const std::pair<int, int> &b) {
-            return a.first != b.first ? a.first > b.first : a.second > b.second;
-        };
-        std::make_heap(heap.begin(), heap.end(), cmp);
-        for (int c = 0; c < ncl && ccount[c] > 1; ++c) {
-            std::pop_heap(heap.begin(), heap.end(), cmp);
-            auto &h = heap.back();
-            for (int q = 0; q < ccount[c]; ++q) slot[h.second].push_back(idx[cfirst[c] + q]);
-            h.first += ccount[c];
-            fill[h.second] = h.first;
-            std::push_heap(heap.begin(), heap.end(), cmp);
+        if (!spread) {
+            // clusters in the first slots of the least loaded lanes, longest first
+            std::vector<std::pair<int, int>> heap;
+            for (int t = 0; t < width; ++t) heap.push_back({0, t});
+            auto cmp = [](const std::pair<int, int> &a, const std::pair<int, int> &b) {
+                return a.first != b.first ? a.first > b.first : a.second > b.second;
+            };
+            std::make_heap(heap.begin(), heap.end(), cmp);
+            for (int c = 0; c < ncl && ccount[c] > 1; ++c) {
+                std::pop_heap(heap.begin(), heap.end(), cmp);
+                auto &h = heap.back();
+                for (int q = 0; q < ccount[c]; ++q) slot[h.second].push_back(idx[cfirst[c] + q]);
+                h.first += ccount[c];
+                fill[h.second] = h.first;
+                std::push_heap(heap.begin(), heap.end(), cmp);
+            }
+            for (auto &v : slot) v.resize(len, -1);
+        } else {
+            // clusters, longest first, onto a least loaded lane (as above); one lane per group
+            // is tried, and the cluster's operations take, in order, the slots of least conflict
+            // (cluster operations already in a warp-slot count against it, to spread them)
+            for (auto &v : slot) v.assign(len, -1);
+            const int ngroups = (width + lanes - 1) / lanes;
+            std::vector<std::vector<unsigned>> used((size_t)ngroups * len * 4);  // distinct words
+            std::vector<int> nchain((size_t)ngroups * len, 0);
+            auto op_cost = [&](int o, int g, int j) {
+                long long cost = 0;
+                for (int f = 0; f < 4; ++f) {
+                    const unsigned a = word(ops, o, f);
+                    int same = 0;
+                    bool present = false;
+                    for (unsigned v : used[(((size_t)g * len) + j) * 4 + f]) {
+                        if (v == a) { present = true; break; }
+                        same += v % nb == a % nb;
+                    }
+                    if (!present) cost += (f == 0 ? 2 : 1) * (long long)same;
+                }
+                return 4 * cost + nchain[(size_t)g * len + j];
+            };
+            std::vector<int> pick, bpick, freeafter(len + 1);
+            for (int c = 0; c < ncl && ccount[c] > 1; ++c) {
+                const int k = ccount[c];
+                int fmin = len;
+                for (int t = 0; t < width; ++t) fmin = std::min(fmin, fill[t]);
+                int bt = -1;
+                long long bcost = 0;
+                for (int g = 0; g < ngroups; ++g) {
+                    int t = -1;
+                    for (int u = g * lanes; u < std::min(width, (g + 1) * lanes); ++u)
+                        if (fill[u] == fmin) { t = u; break; }
+                    if (t < 0) continue;
+                    // slots in order, each after the previous, leaving room for the rest
+                    freeafter[len] = 0;  // free slots of this lane from j on
+                    for (int j = len - 1; j >= 0; --j) freeafter[j] = freeafter[j + 1] + (slot[t][j] < 0);
+                    pick.clear();
+                    long long cost = 0;
+                    int prev = -1;
+                    for (int q = 0; q < k; ++q) {
+                        int bj = -1;
+                        long long bc = 0;
+                        for (int j = prev + 1; j < len; ++j) {
+                            if (slot[t][j] >= 0) continue;
+                            if (freeafter[j + 1] < k - 1 - q) break;
+                            const long long cc = op_cost(idx[cfirst[c] + q], g, j);
+                            if (bj < 0 || cc < bc) { bj = j; bc = cc; }
+                        }
+                        if (bj < 0) return {};  // cannot happen: the lane has k free slots
+                        pick.push_back(bj);
+                        cost += bc;
+                        prev = bj;
+                    }
+                    if (bt < 0 || cost < bcost) { bt = t; bcost = cost; bpick = pick; }
+                }
+                if (bt < 0) return {};
+                const int g = bt / lanes;
+                for (int q = 0; q < k; ++q) {
+                    const int o = idx[cfirst[c] + q], j = bpick[q];
+                    slot[bt][j] = o;
+                    ++nchain[(size_t)g * len + j];
+                    for (int f = 0; f < 4; ++f) {
+                        const unsigned a = word(ops, o, f);
+                        auto &l = used[(((size_t)g * len) + j) * 4 + f];
+                        if (std::find(l.begin(), l.end(), a) == l.end()) l.push_back(a);
+                    }
+                }
+                fill[bt] += k;
+            }
         }
-        for (auto &v : slot) v.resize(len, -1);
         // single operations, bucketed by the bank of the word they write
-        const unsigned nb = (unsigned)lanes;  // banks (or bank pairs) per group of lanes
         std::vector<std::vector<int>> bucket(nb);
         for (int c = 0; c < ncl; ++c)
             if (ccount[c] == 1) bucket[word(ops, idx[cfirst[c]], 0) % nb].push_back(idx[cfirst[c]]);
@@ -863,6 +937,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         B.lu_base = packed_lu_base;
         B.vdummy = m;
         B.lanes = opt.elem_bytes == 8 ? 16 : 32;
+        B.spread = opt.spread_clusters;
         for (int l = 0; l < nplev; ++l) {
             B.begin();
             if (l < nlev)
@@ -905,6 +980,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         B.lu_base = packed_lu_base;
         B.vdummy = m;
         B.lanes = opt.elem_bytes == 8 ? 16 : 32;
+        B.spread = opt.spread_clusters;
         for (int l = 0; l < nb; ++l) {
             B.begin();
             for (int k : byb[l])
@@ -930,6 +1006,7 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         B.lu_base = packed_lu_base;
         B.vdummy = m;
         B.lanes = opt.elem_bytes == 8 ? 16 : 32;
+        B.spread = opt.spread_clusters;
         for (int l = 0; l < nf; ++l) {
             B.begin();
             for (int k : byf[l])

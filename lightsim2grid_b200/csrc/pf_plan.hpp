@@ -134,6 +134,7 @@ struct PlanOptions {
     bool fuse_forward = true;         // fuse the forward substitution into the refactorisation
     int threads = 512;                // CTA size the phase programs are laid out for
     int elem_bytes = 4;               // LU element size of the packed programs' bank placement
+    bool spread_clusters = false;     // bank placement: clusters spread over a phase's slots
     int order_trials = 8;             // > 0: minimum degree of this many relabellings, each followed
                                       // by its least-depth equivalent, the shallowest kept; 0:
                                       // minimum degree only

@@ -37,6 +37,8 @@ def main():
     ap.add_argument("--batch-layout", type=int, default=0, help="0 auto, 1 one CTA per instance, 2 batch-interleaved")
     ap.add_argument("--ordering", type=int, default=0,
                     help="0: minimum degree + least-depth equivalent reordering, 1: minimum degree only")
+    ap.add_argument("--placement", type=int, default=0,
+                    help="packed programs: 0 clusters in first slots, 1 clusters spread")
     args = ap.parse_args()
 
     import torch
@@ -58,7 +60,7 @@ def main():
     plan = Plan(Y, Vn, S, sl, w, pv, pq, precision=args.precision, dc=args.dc, fdpf=fdpf, threads=args.threads,
                 lu_placement=args.lu_placement, fuse_forward=args.fuse_forward, max_ctas_per_sm=args.ctas_per_sm,
                 refine=args.refine, refine_threshold=args.refine_threshold, lu_reuse_threshold=args.lu_reuse,
-                batch_layout=args.batch_layout, ordering=args.ordering)
+                batch_layout=args.batch_layout, ordering=args.ordering, placement=args.placement)
     lib = plan._lib
     cp = np.zeros(nb + 1, np.int32)
     rows, cols, vals = [], [], []
