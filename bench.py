@@ -449,8 +449,12 @@ def run_ours(args):
                 "l2": "flushed (256 MB write) before every timed step",
                 "job_order": "hardest outages first (pf_n1_order: power mismatch of the outage at the start voltages)",
                 "parallelism": "replicas" if ws > 1 else "single GPU",
-                "plan": {k: info[k] for k in ("m", "nnz_j", "nnz_lu", "flops_refactor", "levels_refactor",
-                                              "groups_refactor", "threads", "lu_in_shared", "ctas_per_sm", "grid")},
+                "plan": dict({k: info[k] for k in ("m", "nnz_j", "nnz_lu", "flops_refactor", "levels_refactor",
+                                                   "groups_refactor", "threads", "lu_in_shared", "ctas_per_sm",
+                                                   "grid", "smem_wavefronts_factor", "smem_wavefronts_backward",
+                                                   "smem_wavefronts_forward")},
+                             ordering="minimum degree of 8 relabellings, each with its least-depth equivalent",
+                             placement="packed programs placed for few shared-memory bank conflicts"),
                 "iterations_mean": float(np.mean(mixed["iters"])),
             },
             "fp64": {"value": fp64["value"], "unit": "PF/s", "ms_per_step": 1e3 * fp64["total"] / args.steps,
