@@ -46,10 +46,12 @@ typedef struct pf_options {
                                batch dimension amortises each phase); its per-CTA memory is
                                allocated on first use                                         */
     int ordering;           /* elimination order of the first factorisation.  0: default, minimum
-                               degree of 8 relabellings of the pattern, each followed by its
-                               equivalent reordering of least depth (no added fill, fewer
-                               dependent phases), the shallowest kept; 1: minimum degree only;
-                               2: minimum degree and its least-depth equivalent, one labelling */
+                               degree preferring low elimination levels (among the vertices of
+                               degree up to the minimum + 2, the lowest level) on 8 relabellings
+                               of the pattern, each followed by its equivalent reordering of least
+                               depth (no added fill, fewer dependent phases), the shallowest kept;
+                               1: plain minimum degree only; 2: as 0 with one labelling; 3: as 0
+                               without the level preference                                    */
     int placement;          /* packed programs (LU in shared memory): 0 default, clusters of
                                operations writing one value in their thread's first slots; 1
                                clusters spread over the phase's slots (fewer bank conflicts in

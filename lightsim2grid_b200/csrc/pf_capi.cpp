@@ -863,6 +863,7 @@ int pf_plan_create(int n, const int *colptr, const int *rowind, const double *yb
     l2g::PlanOptions po;
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
+    po.level_slack = pl->opt.ordering == 1 || pl->opt.ordering == 3 ? 0 : 2;
     po.elem_bytes = pl->opt.precision ? 4 : 8;
     po.spread_clusters = pl->opt.placement == 1;
     {
@@ -903,6 +904,7 @@ int pf_dc_plan_create(int n, const int *colptr, const int *rowind, const double 
     l2g::PlanOptions po;
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
+    po.level_slack = pl->opt.ordering == 1 || pl->opt.ordering == 3 ? 0 : 2;
     po.elem_bytes = pl->opt.precision ? 4 : 8;
     po.spread_clusters = pl->opt.placement == 1;
     int thr = pl->opt.threads;
@@ -940,6 +942,7 @@ int pf_fdpf_plan_create(int n, const int *colptr, const int *rowind, const doubl
     l2g::PlanOptions po;
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
+    po.level_slack = pl->opt.ordering == 1 || pl->opt.ordering == 3 ? 0 : 2;
     po.elem_bytes = pl->opt.precision ? 4 : 8;
     po.spread_clusters = pl->opt.placement == 1;
     int thr = pl->opt.threads;

@@ -41,8 +41,13 @@ void parallel_for(int n, F f) {
 // Explicit elimination graph (Rose 1972; Tinney & Walker scheme 2): eliminating v joins
 // its neighbours into a clique.  Degrees are kept in bucket lists so that the next
 // minimum is found in O(1); ties go to the most recently touched node of the bucket.
+// With level_slack > 0 the choice also looks at depth: every vertex carries the elimination
+// level it would get (one more than the highest level of its eliminated neighbours), and among
+// the vertices of degree at most the minimum + level_slack the one of lowest level is taken
+// (first found on ties), which keeps the elimination tree shallow at little cost in fill.
 // -------------------------------------------------------------------------------------
-std::vector<int> minimum_degree(int m, const std::vector<int> &Ap, const std::vector<int> &Ai) {
+std::vector<int> minimum_degree(int m, const std::vector<int> &Ap, const std::vector<int> &Ai,
+                                int level_slack = 0) {
     std::vector<std::vector<int>> adj(m);
     for (int j = 0; j < m; ++j)
         for (int p = Ap[j]; p < Ap[j + 1]; ++p) {
@@ -77,13 +82,20 @@ std::vector<int> minimum_degree(int m, const std::vector<int> &Ap, const std::ve
     order.reserve(m);
     int mindeg = 0, stamp = 0;
     std::vector<int> merged;
+    std::vector<int> lev(m, 0);
     for (int k = 0; k < m; ++k) {
         while (mindeg <= m && head[mindeg] < 0) ++mindeg;
         int v = head[mindeg];
+        if (level_slack > 0)
+            for (int d = mindeg; d <= std::min(m, mindeg + level_slack); ++d)
+                for (int u = head[d]; u >= 0; u = next[u])
+                    if (lev[u] < lev[v]) v = u;
         unlink(v);
         alive[v] = 0;
         order.push_back(v);
         const std::vector<int> nb = adj[v];
+        for (int u : nb)
+            if (alive[u]) lev[u] = std::max(lev[u], lev[v] + 1);
         for (int u : nb) {
             if (!alive[u]) continue;
             merged.clear();
@@ -220,7 +232,8 @@ int symbolic_depth(int m, const std::vector<int> &Ap, const std::vector<int> &Ai
 // Minimum degree breaks ties by vertex label, and the depth of the equivalent least-depth order
 // varies with those choices: orders of `trials` relabellings (the identity first, then seeded
 // shuffles) are compared and the shallowest kept (then the least fill).
-std::vector<int> shallow_order(int m, const std::vector<int> &Ap, const std::vector<int> &Ai, int trials) {
+std::vector<int> shallow_order(int m, const std::vector<int> &Ap, const std::vector<int> &Ai, int trials,
+                               int level_slack) {
     const int T = std::max(1, trials);
     // the relabellings, drawn in sequence from one seed (the identity first)
     std::vector<std::vector<int>> perm(T, std::vector<int>(m));
@@ -251,7 +264,7 @@ std::vector<int> shallow_order(int m, const std::vector<int> &Ap, const std::vec
             Bi.insert(Bi.end(), cols[j].begin(), cols[j].end());
             Bp[j + 1] = (int)Bi.size();
         }
-        q[t] = low_height_order(m, Bp, Bi, minimum_degree(m, Bp, Bi));
+        q[t] = low_height_order(m, Bp, Bi, minimum_degree(m, Bp, Bi, level_slack));
         for (int &v : q[t]) v = inv[v];
         depth[t] = symbolic_depth(m, Ap, Ai, q[t], fill[t]);
     });
@@ -765,7 +778,8 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
     const int m = P.m;
     std::ostringstream err;
     // ---------------------------------------------------------------- ordering
-    P.q = opt.order_trials > 0 ? shallow_order(m, P.Jp, P.Ji, opt.order_trials) : minimum_degree(m, P.Jp, P.Ji);
+    P.q = opt.order_trials > 0 ? shallow_order(m, P.Jp, P.Ji, opt.order_trials, opt.level_slack)
+                               : minimum_degree(m, P.Jp, P.Ji, opt.level_slack);
     P.qinv.assign(m, 0);
     for (int k = 0; k < m; ++k) P.qinv[P.q[k]] = k;
 

@@ -138,6 +138,8 @@ struct PlanOptions {
     int order_trials = 8;             // > 0: minimum degree of this many relabellings, each followed
                                       // by its least-depth equivalent, the shallowest kept; 0:
                                       // minimum degree only
+    int level_slack = 2;              // minimum degree prefers, among the vertices of degree at most
+                                      // the minimum + level_slack, the one of lowest level; 0: off
 };
 
 // Builds a plan.  Ybus CSC (n x n, complex), V0 and Sbus (used for the first

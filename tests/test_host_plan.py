@@ -96,30 +96,31 @@ def test_fill_reducing_order_keeps_fill_low():
 
 
 def test_default_order_is_shallow():
-    """The default elimination order (minimum degree of 8 relabellings, each followed by its
-    least-depth equivalent, the shallowest kept) brings the refactorisation's dependent levels of
-    the 2848-bus Jacobian to 72 (minimum degree alone: 91) with no more fill than minimum degree
-    (48,870 LU entries)."""
+    """The default elimination order (minimum degree preferring low elimination levels, on 8
+    relabellings, each followed by its least-depth equivalent, the shallowest kept) brings the
+    refactorisation's dependent levels of the 2848-bus Jacobian to 53 (minimum degree alone: 91;
+    without the level preference: 72) with no more fill than minimum degree (48,870 LU entries)."""
     c = grid_problem("grid2848")
     m = 2 * len(c["pq"]) + len(c["pv"])
     b = np.linspace(1.0, 2.0, m)
     x, info = host_schedule_solve(c, c["V0"], b, False)
-    assert info.levels_refactor <= 74
+    assert info.levels_refactor <= 55
     assert info.nnz_lu <= 48870
     assert np.all(np.isfinite(x))
 
 
 def test_packed_programs_are_placed_for_few_bank_conflicts():
     """The packed factor program of the 2848-bus plan (FP32, LU in shared memory) makes about
-    35k shared-memory wavefronts per run under the bank model it is placed for; the longest-first
-    placement made 52k, and no placement can go below one wavefront per operand and warp-slot."""
+    37k shared-memory wavefronts per run under the bank model it is placed for (the longest-first
+    placement made 52k on the programs of the order without the level preference), and no
+    placement can go below one wavefront per operand and warp-slot."""
     c = grid_problem("grid2848")
     m = 2 * len(c["pq"]) + len(c["pv"])
     _, info = host_schedule_solve(c, c["V0"], np.ones(m), False)
     floor = 5 * (info.flops_refactor + info.nnz_lu) // 32  # operations (updates + pushes) / warp
-    assert floor < info.smem_wavefronts_factor <= 37000
-    assert 0 < info.smem_wavefronts_backward <= 8500
-    assert 0 < info.smem_wavefronts_forward <= 10000
+    assert floor < info.smem_wavefronts_factor <= 39000
+    assert 0 < info.smem_wavefronts_backward <= 8000
+    assert 0 < info.smem_wavefronts_forward <= 10500
 
 
 def test_invalid_inputs_are_rejected():
