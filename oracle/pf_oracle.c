@@ -89,6 +89,45 @@ static void iv_push(ivec *a, int x) {
     a->v[a->n++] = x;
 }
 
+/* min-heap of 64-bit keys degree << 31 | label (smaller key: smaller degree, then label) */
+typedef struct {
+    long long *v;
+    int n, cap;
+} mdheap;
+
+static long long md_key(int deg, int label) { return ((long long)deg << 31) | (long long)label; }
+
+static void mdh_push(mdheap *h, long long key) {
+    if (h->n == h->cap) {
+        h->cap = h->cap ? 2 * h->cap : 64;
+        h->v = (long long *)xrealloc(h->v, sizeof(long long) * (size_t)h->cap);
+    }
+    int i = h->n++;
+    while (i > 0) {
+        const int p = (i - 1) / 2;
+        if (h->v[p] <= key) break;
+        h->v[i] = h->v[p];
+        i = p;
+    }
+    h->v[i] = key;
+}
+
+static long long mdh_pop(mdheap *h) {
+    const long long top = h->v[0];
+    const long long last = h->v[--h->n];
+    int i = 0;
+    for (;;) {
+        int c = 2 * i + 1;
+        if (c >= h->n) break;
+        if (c + 1 < h->n && h->v[c + 1] < h->v[c]) ++c;
+        if (h->v[c] >= last) break;
+        h->v[i] = h->v[c];
+        i = c;
+    }
+    if (h->n > 0) h->v[i] = last;
+    return top;
+}
+
 static void md_order(int m, const int *Ap, const int *Ai, int *order) {
     ivec *adj = (ivec *)xcalloc((size_t)m, sizeof(ivec));
     int *mark = (int *)xmalloc(sizeof(int) * (size_t)m);
@@ -116,16 +155,21 @@ static void md_order(int m, const int *Ap, const int *Ai, int *order) {
         adj[i].n = w;
     }
     ivec nb = {0, 0, 0};
+    /* the live vertex of least degree, ties to the lowest label: a binary heap of (degree,
+       label) keys with lazy deletion (an entry whose degree is no longer current is skipped;
+       each degree change pushes a fresh entry), O(fill log m) instead of a scan per pivot */
+    mdheap H = {0, 0, 0};
+    for (int i = 0; i < m; ++i) mdh_push(&H, md_key(adj[i].n, i));
     for (int k = 0; k < m; ++k) {
-        int best = -1, bdeg = 0;
-        for (int i = 0; i < m; ++i) {
-            if (dead[i]) continue;
-            if (best < 0 || adj[i].n < bdeg) {
-                best = i;
-                bdeg = adj[i].n;
-            }
+        int v = -1;
+        while (H.n > 0) {
+            const long long top = mdh_pop(&H);
+            const int i = (int)(top & 0x7fffffff), d = (int)(top >> 31);
+            if (dead[i] || adj[i].n != d) continue;
+            v = i;
+            break;
         }
-        int v = best;
+        if (v < 0) abort();
         order[k] = v;
         dead[v] = 1;
         nb.n = 0;
@@ -151,12 +195,14 @@ static void md_order(int m, const int *Ap, const int *Ai, int *order) {
             }
             free(adj[u].v);
             adj[u] = na;
+            mdh_push(&H, md_key(adj[u].n, u));
         }
         free(adj[v].v);
         adj[v].v = NULL;
         adj[v].n = adj[v].cap = 0;
     }
     free(nb.v);
+    free(H.v);
     for (int i = 0; i < m; ++i) free(adj[i].v);
     free(adj);
     free(mark);
