@@ -56,6 +56,15 @@ typedef struct pf_options {
                                operations writing one value in their thread's first slots; 1
                                clusters spread over the phase's slots (fewer bank conflicts in
                                the host model, longer plan build).  Same results either way     */
+    int level_slack;        /* orderings 0 and 2: minimum degree takes, among the vertices of
+                               degree up to the minimum + level_slack, the one of lowest
+                               elimination level.  0: default (2); < 0: no level preference;
+                               larger values give shallower plans for some more fill          */
+    int op_prefetch;        /* Newton kernels: the operations of the phase k phases ahead are
+                               prefetched into L1 when a phase starts (k = op_prefetch), instead
+                               of the next phase's first operations being loaded into registers
+                               (which the phase's closing barrier waits for).  0: default; < 0:
+                               off.  Same results either way                                    */
 } pf_options;
 
 /* DC power flow plan (BaseDCAlgo::compute_pf, src/powerflow_algorithm/BaseDCAlgo.tpp:5-175;
@@ -203,9 +212,11 @@ int pf_batch_ts(pf_plan *plan, int nsteps, const double *Sbus_ri, const double *
                 double tol, double *V_out_ri, int *converged, int *iters, int *errs, int *status);
 
 /* Device-resident batch on `stream` (a cudaStream_t, NULL for the default stream).  No
-   host synchronisation; capturable in a CUDA graph once the plan exists.  Mixed form: a job
-   with an instance that does not converge in FP32 is solved again in FP64 inside the launch
-   (option fp64_fallback), so the outputs are the FP64 outcome for those instances. */
+   host synchronisation; capturable in a CUDA graph once the plan exists (with batch_layout 2,
+   after one call outside capture: that layout's per-CTA memory is allocated on first use).
+   Mixed form: a job with an instance that does not converge in FP32 is solved again in FP64
+   inside the launch (option fp64_fallback), so the outputs are the FP64 outcome for those
+   instances.  The current device must be the plan's (else -1, nothing launched). */
 int pf_batch_device(pf_plan *plan, const pf_device_batch *batch, void *stream);
 
 /* pf_batch_device without any allocation, for callers that cannot let the library call
@@ -214,8 +225,11 @@ int pf_batch_device(pf_plan *plan, const pf_device_batch *batch, void *stream);
    No counterpart in the reference.  The kernel's working memory comes from a 32 MiB
    file-scope device array held on every GPU that loads the library until exit; a plan whose
    per-CTA working memory does not fit is rejected with an error, otherwise the launch uses as
-   many CTAs as fit.  The first call on a device looks the array's address up
-   (cudaGetSymbolAddress) -- make it before any stream capture.  The array is shared by all
+   many CTAs as fit.  Mixed form: an instance that does not converge in FP32 is solved again in
+   FP64 inside the launch, as pf_batch_device does (the slabs then hold an FP64 LU too, so large
+   plans run on fewer CTAs: about 50 for the 2,848-bus mixed plan).  The current device must be
+   the plan's (else -1, nothing launched).  The first call on a device looks the array's address
+   up (cudaGetSymbolAddress) -- make it before any stream capture.  The array is shared by all
    calls and keeps the previous call's contents; the job counter is cleared before each launch.
    Calls whose kernels overlap on the GPU race on the array: keep them on one stream.  Calls no
    cudaMalloc, cudaFree or allocating library routine. */
@@ -344,6 +358,13 @@ int pf_server_create(const pf_server_grid *grids, int ngrids, long long hbm_budg
 int pf_server_submit(pf_server *server, long long id, int grid, int kind, const double *scale, int nbranches,
                      const int *branches, double *V_out, int *iters_out, int *errs_out);
 int pf_server_poll(pf_server *server, long long *done_ids, int cap);
+/* SM reservation of a server (no counterpart in the reference).  A request is small when its
+   instances x buses are at most 20,000; a large request is admitted only while the SMs taken by
+   the CTAs of the large requests in flight stay within (SMs - reserved_sms), so the reserved SMs
+   stay free for small requests (stream priorities alone cannot move a resident CTA); its launch
+   uses at most large_request_ctas CTAs (0: no cap), each solving several of its instances in
+   turn.  Defaults: an eighth of the SMs reserved, no cap.  Takes effect for later admissions. */
+int pf_server_configure(pf_server *server, int reserved_sms, int large_request_ctas);
 int pf_server_state(const pf_server *server, int *pending, int *inflight, long long *bytes_in_use);
 void pf_server_destroy(pf_server *server);
 
@@ -366,7 +387,8 @@ int pf_batch_device_phase_cycles(pf_plan *plan, const pf_device_batch *batch, vo
 int pf_batch_device_phase_trace(pf_plan *plan, const pf_device_batch *batch, void *stream, double *out, int cap);
 
 /* Timers of the last call (seconds): [0] total, [1] host preparation, [2] host->device,
-   [3] kernel, [4] device->host, [5] instances re-run in FP64 (count, as a double).
+   [3] kernel, [4] device->host, [5] instances re-solved in FP64 by the mixed form's fallback,
+   inside the launch or by a second launch (count, as a double).
    Replaces get_timers (src/main.cpp:236) and the batch timers (src/main.cpp:1174-1178). */
 int pf_timers(const pf_plan *plan, double *out, int nout);
 

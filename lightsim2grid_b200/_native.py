@@ -21,7 +21,8 @@ class PfOptions(ctypes.Structure):
                 ("fuse_forward", ctypes.c_int), ("pivot_threshold", ctypes.c_double),
                 ("fp64_fallback", ctypes.c_int), ("max_ctas_per_sm", ctypes.c_int), ("refine", ctypes.c_int),
                 ("refine_threshold", ctypes.c_double), ("lu_reuse_threshold", ctypes.c_double),
-                ("batch_layout", ctypes.c_int), ("ordering", ctypes.c_int), ("placement", ctypes.c_int)]
+                ("batch_layout", ctypes.c_int), ("ordering", ctypes.c_int), ("placement", ctypes.c_int),
+                ("level_slack", ctypes.c_int), ("op_prefetch", ctypes.c_int)]
 
 
 class PfPlanInfo(ctypes.Structure):
@@ -75,7 +76,8 @@ SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_g
            "pf_scratch_bytes", "pf_multi_create", "pf_multi_launch", "pf_multi_info", "pf_multi_destroy",
            "pf_flows_device", "pf_flows_host", "pf_ybus_positions", "pf_assemble_ybus_device",
            "pf_set_ybus_values_device", "pf_assemble_sbus_device", "pf_dc_plan_create", "pf_server_create",
-           "pf_server_submit", "pf_server_poll", "pf_server_state", "pf_server_destroy", "pf_fdpf_plan_create", "pf_n1_order")
+           "pf_server_submit", "pf_server_poll", "pf_server_state", "pf_server_destroy", "pf_fdpf_plan_create", "pf_n1_order",
+           "pf_server_configure")
 
 
 def load(path=None):
@@ -151,6 +153,8 @@ def load(path=None):
                                      ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     lib.pf_server_poll.restype = ctypes.c_int
     lib.pf_server_poll.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    lib.pf_server_configure.restype = ctypes.c_int
+    lib.pf_server_configure.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.pf_server_state.restype = ctypes.c_int
     lib.pf_server_state.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     lib.pf_server_destroy.restype = None

@@ -22,6 +22,9 @@ namespace {
 
 thread_local std::string g_err;
 
+// op_prefetch default: phases ahead whose operations are prefetched into L1 (0: none)
+constexpr int kDefaultOpPrefetch = 0;
+
 int fail(int code, const std::string &msg) {
     g_err = msg;
     return code;
@@ -30,6 +33,18 @@ int fail(int code, const std::string &msg) {
 int cuda_fail(cudaError_t e, const char *where) {
     g_err = std::string(where) + ": " + cudaGetErrorString(e);
     return -2;
+}
+
+// Entry points that take device pointers launch on the current device: it must be the device the
+// plan's structure and scratch live on (a plan is bound to the device current at its creation).
+int check_plan_device(int plan_device, const char *who) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, who);
+    if (dev != plan_device)
+        return fail(-1, std::string(who) + ": the plan was built on device " + std::to_string(plan_device) +
+                            " but device " + std::to_string(dev) + " is current");
+    return 0;
 }
 
 double now() {
@@ -528,6 +543,14 @@ void release(pf_plan *pl) {
 // Whether a launch runs the batch-interleaved kernel: Newton plans, independent instances (no
 // chain), no per-launch diagnostics (J output, phase cycles or trace, LU reuse), and option
 // batch_layout 2 (auto keeps one CTA per instance, measured faster on every grid so far).
+// Phases ahead whose operations the Newton kernel prefetches into L1 (option op_prefetch:
+// 0 default, < 0 off).
+int op_prefetch_of(const pf_plan *pl) {
+    const int o = pl->opt.op_prefetch;
+    if (o < 0) return 0;
+    return o > 0 ? std::min(o, 8) : kDefaultOpPrefetch;
+}
+
 bool use_tile(const pf_plan *pl, const l2g::BatchArgs &a) {
     if (pl->P.dc || pl->P.fdpf || a.chain || a.Jout || a.phase_cycles || a.trace || a.reuse_below > 0) return false;
     return pl->opt.batch_layout == 2;
@@ -552,7 +575,7 @@ int launch_tile(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, i
 }
 
 int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, unsigned char *scratch,
-                size_t scratch_bytes, int *counter, bool allow_tile = false) {
+                size_t scratch_bytes, int *counter, bool allow_tile = false, bool allow_inline = false) {
     a.scratch = scratch;
     a.slab_bytes = (long long)pl->slab;
     a.job_counter = counter;
@@ -560,14 +583,17 @@ int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, u
     a.refine = (precision == 1 && pl->refine) ? 1 : 0;
     a.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
     a.reuse_below = lu_reuse_below(pl, a.refine_below);
+    a.op_prefetch = op_prefetch_of(pl);
     pl->last_inline = false;
     if (a.njobs <= 0) return 0;
     if (allow_tile && use_tile(pl, a)) return launch_tile(pl, a, precision, st, counter);
-    if (allow_tile && pl->inline_fb && precision == pl->precision && a.refine && !pl->P.dc && !pl->P.fdpf) {
+    if ((allow_tile || allow_inline) && pl->inline_fb && precision == pl->precision && a.refine && !pl->P.dc &&
+        !pl->P.fdpf) {
         // the plan's own scratch: FP64 fallback inside the launch
         a.fp64_inline = 1;
         a.slab_bytes = (long long)pl->slab_fb;
-        cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+        // the job counter and, after it, the count of instances re-solved in FP64
+        cudaError_t e = cudaMemsetAsync(counter, 0, 2 * sizeof(int), st);
         if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
         int grid = std::min(pl->grid, a.njobs);
         grid = std::min<long long>(grid, (long long)(scratch_bytes / pl->slab_fb));
@@ -619,7 +645,7 @@ int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, u
 
 int launch(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st) {
     return launch_into(pl, a, precision, st, static_cast<unsigned char *>(pl->scratch.p),
-                       pl->slab_fb * (size_t)pl->grid, static_cast<int *>(pl->counter.p), true);
+                       pl->slab_fb * (size_t)pl->grid, static_cast<int *>(pl->counter.p), true, true);
 }
 
 template <typename T>
@@ -705,6 +731,11 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
     if ((e = cudaMemcpyAsync(errs, pl->errs.p, (size_t)n_inst * sizeof(int), cudaMemcpyDeviceToHost, st)) !=
         cudaSuccess)
         return cuda_fail(e, "batch: download");
+    int inline_reruns = 0;  // instances the launch re-solved in FP64 itself
+    if (pl->last_inline &&
+        (e = cudaMemcpyAsync(&inline_reruns, static_cast<int *>(pl->counter.p) + 1, sizeof(int),
+                             cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "batch: download");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "batch: kernel execution");
     float kms = 0.f;
     cudaEventElapsedTime(&kms, pl->ev0, pl->ev1);
@@ -712,7 +743,7 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
     // mixed form: re-run in FP64 the jobs that contain a failure.  `settled` (if given) is called
     // once the re-run is queued, with the instances it recomputes: every other instance's row is
     // final, so the caller can copy those rows out while the re-run runs.
-    int rerun = 0;
+    int rerun = inline_reruns;
     std::vector<char> again;
     if (settled) again.assign((size_t)n_inst, 0);
     if (pl->precision == 1 && pl->opt.fp64_fallback != 2 && !pl->last_inline) {
@@ -803,19 +834,26 @@ BatchArgs device_args(const pf_device_batch *b) {
 }
 
 int batch_device_with_scratch(pf_plan *pl, const pf_device_batch *b, void *stream, void *scratch,
-                              size_t scratch_bytes) {
+                              size_t scratch_bytes, bool fp64_fallback) {
     if (!pl || !b || !scratch) return fail(-1, "batch with scratch: null argument");
+    if (int rc = check_plan_device(pl->device, "batch with scratch")) return rc;
     if (reinterpret_cast<uintptr_t>(scratch) % 256 != 0)
         return fail(-1, "batch with scratch: scratch not 256-byte aligned");
     const size_t head = 256;  // job counter
     if (scratch_bytes < head + pl->slab) return fail(-1, "batch with scratch: scratch holds no CTA slab");
     unsigned char *base = static_cast<unsigned char *>(scratch);
     l2g::BatchArgs a = l2g::device_args(b);
+    if (fp64_fallback && pl->inline_fb && scratch_bytes < head + pl->slab_fb)
+        return fail(-1, "batch with scratch: scratch holds no CTA slab with room for the FP64 fallback");
     return launch_into(pl, a, pl->precision, static_cast<cudaStream_t>(stream), base + head, scratch_bytes - head,
-                       reinterpret_cast<int *>(base));
+                       reinterpret_cast<int *>(base), false, fp64_fallback);
 }
 
 size_t plan_slab_bytes(const pf_plan *pl) { return pl ? pl->slab : 0; }
+
+size_t plan_fallback_slab_bytes(const pf_plan *pl) { return pl ? (pl->inline_fb ? pl->slab_fb : pl->slab) : 0; }
+
+int plan_device(const pf_plan *pl) { return pl ? pl->device : -1; }
 
 void set_last_error(const std::string &msg) { g_err = msg; }
 
@@ -848,6 +886,13 @@ int finish_plan(pf_plan *pl, pf_plan **out) {
 
 extern "C" {
 
+// Level preference of minimum degree for options `o`: none for orderings 1 and 3, else
+// o.level_slack when positive, 2 by default (a negative value also turns it off).
+static int level_slack_of(const pf_options &o) {
+    if (o.ordering == 1 || o.ordering == 3 || o.level_slack < 0) return 0;
+    return o.level_slack > 0 ? std::min(o.level_slack, 64) : 2;
+}
+
 const char *pf_last_error(void) { return g_err.c_str(); }
 
 int pf_plan_create(int n, const int *colptr, const int *rowind, const double *ybus_ri, const double *V0_ri,
@@ -863,7 +908,7 @@ int pf_plan_create(int n, const int *colptr, const int *rowind, const double *yb
     l2g::PlanOptions po;
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
-    po.level_slack = pl->opt.ordering == 1 || pl->opt.ordering == 3 ? 0 : 2;
+    po.level_slack = level_slack_of(pl->opt);
     po.elem_bytes = pl->opt.precision ? 4 : 8;
     po.spread_clusters = pl->opt.placement == 1;
     {
@@ -904,7 +949,7 @@ int pf_dc_plan_create(int n, const int *colptr, const int *rowind, const double 
     l2g::PlanOptions po;
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
-    po.level_slack = pl->opt.ordering == 1 || pl->opt.ordering == 3 ? 0 : 2;
+    po.level_slack = level_slack_of(pl->opt);
     po.elem_bytes = pl->opt.precision ? 4 : 8;
     po.spread_clusters = pl->opt.placement == 1;
     int thr = pl->opt.threads;
@@ -942,7 +987,7 @@ int pf_fdpf_plan_create(int n, const int *colptr, const int *rowind, const doubl
     l2g::PlanOptions po;
     if (pl->opt.pivot_threshold > 0) po.pivot_threshold = pl->opt.pivot_threshold;
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
-    po.level_slack = pl->opt.ordering == 1 || pl->opt.ordering == 3 ? 0 : 2;
+    po.level_slack = level_slack_of(pl->opt);
     po.elem_bytes = pl->opt.precision ? 4 : 8;
     po.spread_clusters = pl->opt.placement == 1;
     int thr = pl->opt.threads;
@@ -1377,7 +1422,7 @@ static int batch_device_impl(pf_plan *pl, const pf_device_batch *b, void *stream
 int pf_batch_device_scratch(pf_plan *plan, const pf_device_batch *batch, void *scratch, long long scratch_bytes,
                             void *stream) {
     if (scratch_bytes <= 0) return fail(-1, "pf_batch_device_scratch: scratch too small");
-    return l2g::batch_device_with_scratch(plan, batch, stream, scratch, (size_t)scratch_bytes);
+    return l2g::batch_device_with_scratch(plan, batch, stream, scratch, (size_t)scratch_bytes, false);
 }
 
 long long pf_scratch_bytes(const pf_plan *plan, int ctas) {
@@ -1388,6 +1433,7 @@ long long pf_scratch_bytes(const pf_plan *plan, int ctas) {
 
 int pf_batch_device(pf_plan *pl, const pf_device_batch *b, void *stream) {
     if (!pl || !b) return fail(-1, "pf_batch_device: null argument");
+    if (int rc = check_plan_device(pl->device, "pf_batch_device")) return rc;
     return batch_device_impl(pl, b, stream, nullptr);
 }
 
@@ -1738,6 +1784,7 @@ int pf_multi_create(pf_plan *const *plans, const pf_device_batch *batches, int n
         sg.A.refine = mp->refine ? 1 : 0;
         sg.A.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
         sg.A.reuse_below = lu_reuse_below(pl, sg.A.refine_below);
+        sg.A.op_prefetch = op_prefetch_of(pl);
     }
     e = cudaMemcpy(mp->segs.p, host.data(), sizeof(l2g::Segment) * (size_t)nseg, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
@@ -1758,6 +1805,7 @@ int pf_multi_create(pf_plan *const *plans, const pf_device_batch *batches, int n
 
 int pf_multi_launch(pf_multi *mp, void *stream) {
     if (!mp) return fail(-1, "pf_multi_launch: null argument");
+    if (int rc = check_plan_device(mp->device, "pf_multi_launch")) return rc;
     if (mp->M.njobs <= 0) return 0;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemsetAsync(mp->counter.p, 0, sizeof(int), st);

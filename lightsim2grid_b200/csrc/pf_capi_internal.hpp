@@ -14,11 +14,21 @@ BatchArgs device_args(const pf_device_batch *b);
 
 // pf_batch_device with caller-provided scratch: the first 256 bytes hold the job counter,
 // the rest the per-CTA slabs (the grid shrinks to the slabs that fit).  Allocates nothing.
+// fp64_fallback: a mixed plan that runs its FP64 fallback inside launches does so here too, with
+// slabs of plan_fallback_slab_bytes (else the FP32 result of a failing instance is reported as is).
+// Fails without launching when the current device is not the plan's.
 int batch_device_with_scratch(pf_plan *pl, const pf_device_batch *b, void *stream, void *scratch,
-                              size_t scratch_bytes);
+                              size_t scratch_bytes, bool fp64_fallback);
 
 // Bytes of one CTA slab of the plan's kernel.
 size_t plan_slab_bytes(const pf_plan *pl);
+
+// Bytes of one CTA slab when the launch runs the FP64 fallback inside (plan_slab_bytes when the plan
+// has no such fallback).
+size_t plan_fallback_slab_bytes(const pf_plan *pl);
+
+// Device the plan was created on (-1 for a null plan).
+int plan_device(const pf_plan *pl);
 
 // Sets the message returned by pf_last_error on this thread.
 void set_last_error(const std::string &msg);

@@ -80,6 +80,9 @@ struct BatchArgs {
     int fp64_inline;                   // mixed form: a job that failed in FP32 is solved again in FP64
                                        // by the same CTA (slab_bytes then holds an FP64 LU, and the
                                        // dynamic shared memory an FP64 solve vector)
+    int op_prefetch;                   // Newton phase programs: phases ahead whose operations are
+                                       // prefetched into L1 (0: operations loaded into registers
+                                       // one phase ahead)
 };
 
 // The output row of an instance (Vout may be mapped host memory: rows stream out as instances

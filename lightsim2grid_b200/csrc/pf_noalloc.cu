@@ -12,14 +12,18 @@
 // For them this entry point runs the same Newton-Raphson kernel as pf_batch_device, but
 // takes its per-CTA working memory (the slabs holding voltages, currents, mismatches and,
 // when the factor does not fit in shared memory, the LU values) and its job counter from a
-// file-scope device array instead of the plan's buffers.
+// file-scope device array instead of the plan's buffers.  A mixed-precision plan re-solves an
+// instance that fails in FP32 in FP64 inside the launch, as pf_batch_device does, so the two
+// entry points give the same results; its slabs then also hold an FP64 LU.
 //
 // Limits and rules.
 //   * The array is kNoAllocScratchBytes (32 MiB) and exists on every GPU that loads this
 //     library, until the process exits.  A plan whose CTA slab does not fit is rejected
 //     with an error; otherwise the launch uses as many CTAs as there are slabs in the array
 //     (at most the plan's own grid), so large grids may run on fewer CTAs than
-//     pf_batch_device would use.
+//     pf_batch_device would use (the 2,848-bus mixed plan, whose slab carries room for the
+//     FP64 fallback's LU, runs on about 50 CTAs).
+//   * The current device must be the plan's device (checked before anything else).
 //   * The first call on a device looks the array's device address up (cudaGetSymbolAddress
 //     with that device current) and caches it; make that first call before any stream
 //     capture begins.  Later calls do no set-up.
@@ -61,6 +65,14 @@ extern "C" int pf_batch_device_noalloc(pf_plan *plan, const pf_device_batch *bat
                             cudaGetErrorString(e));
         return -2;
     }
+    if (dev != l2g::plan_device(plan)) {
+        // the array's address is per device: a launch with another device's address would mix
+        // two GPUs' memory
+        l2g::set_last_error("pf_batch_device_noalloc: the plan was built on device " +
+                            std::to_string(l2g::plan_device(plan)) + " but device " + std::to_string(dev) +
+                            " is current");
+        return -1;
+    }
     void *scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -77,12 +89,12 @@ extern "C" int pf_batch_device_noalloc(pf_plan *plan, const pf_device_batch *bat
             g_scratch_addr[dev] = scratch;
         }
     }
-    const size_t need = l2g::plan_slab_bytes(plan) + 256;
+    const size_t need = l2g::plan_fallback_slab_bytes(plan) + 256;
     if (need > kNoAllocScratchBytes) {
         l2g::set_last_error("pf_batch_device_noalloc: one CTA of this plan needs " + std::to_string(need) +
                             " bytes of working memory, more than the " + std::to_string(kNoAllocScratchBytes) +
                             "-byte static scratch array; use pf_batch_device");
         return -1;
     }
-    return l2g::batch_device_with_scratch(plan, batch, stream, scratch, kNoAllocScratchBytes);
+    return l2g::batch_device_with_scratch(plan, batch, stream, scratch, kNoAllocScratchBytes, true);
 }

@@ -77,7 +77,7 @@ struct Arena {
 
 struct Grid {
     pf_plan *plan = nullptr;
-    int n = 0, nbr = 0, ctas = 0;
+    int n = 0, nbr = 0, ctas = 0, ctas_per_sm = 1;
     std::vector<cplx> S;            // base injections (host)
     void *dV0 = nullptr, *dS = nullptr;
     std::vector<int> cptr, rows, cols;
@@ -98,6 +98,11 @@ struct Slot {
 // earlier, so a small request does not wait behind them.
 constexpr long long kSmallWork = 20000;
 
+// Priorities reorder pending CTAs only: a CTA of a large batch that is already resident keeps its
+// SM until its instance is solved (milliseconds on the largest grids).  So large requests are
+// also admitted only while the SMs their CTAs occupy, summed over the large requests in flight,
+// stay within num_sms - reserved_sms: the reserved SMs are left to small requests.
+
 struct Req {
     long long id = 0;
     int grid = 0, kind = 0, ncases = 0, ninst = 0;
@@ -109,6 +114,9 @@ struct Req {
     int *iters = nullptr, *errs = nullptr;
     size_t scratch = 0, outs = 0, ins = 0, bytes = 0, off = 0;
     int slot = -1;
+    bool small = true;   // instance-buses <= kSmallWork
+    int ctas = 0;        // CTAs of its launch
+    int sms = 0;         // SMs those CTAs occupy (large requests)
 };
 
 }  // namespace
@@ -124,6 +132,8 @@ struct pf_server {
     int *djf = nullptr, *djc = nullptr;
     std::deque<Req *> pending;
     std::vector<Req *> inflight;
+    // SM reservation for small requests (see kSmallWork)
+    int num_sms = 1, reserved_sms = 0, large_ctas = 1 << 30, large_sms_inflight = 0;
 };
 
 namespace {
@@ -190,7 +200,11 @@ int prepare(pf_server *s, Req *r) {
     }
     if (r->ninst > s->max_k) return fail("pf_server_submit: request has more instances than the server's maximum");
     if (r->ins > s->in_cap) return fail("pf_server_submit: request inputs exceed the staging buffers");
-    const int ctas = std::max(1, std::min(r->ninst, g.ctas));
+    r->small = (long long)r->ninst * g.n <= kSmallWork;
+    int ctas = std::max(1, std::min(r->ninst, g.ctas));
+    if (!r->small) ctas = std::max(1, std::min(ctas, s->large_ctas));
+    r->ctas = ctas;
+    r->sms = (ctas + g.ctas_per_sm - 1) / g.ctas_per_sm;
     r->scratch = r->ninst ? align256((size_t)pf_scratch_bytes(g.plan, ctas)) : 0;
     r->outs = align256((size_t)r->ninst * g.n * 16 + 8 * (size_t)r->ninst);
     r->bytes = r->scratch + r->outs + r->ins;
@@ -295,6 +309,7 @@ int pf_server_create(const pf_server_grid *grids, int ngrids, long long hbm_budg
         g.plan = gi.plan;
         g.n = info.n;
         g.ctas = info.grid;
+        g.ctas_per_sm = std::max(1, info.ctas_per_sm);
         g.nbr = gi.nbr;
         g.max_iter = gi.max_iter > 0 ? gi.max_iter : 10;
         g.tol = gi.tol > 0 ? gi.tol : 1e-8;
@@ -348,6 +363,11 @@ int pf_server_create(const pf_server_grid *grids, int ngrids, long long hbm_budg
     }
     for (int i = slots - 1; i >= 0; --i) (s->slots[i].high ? s->free_high : s->free_low).push_back(i);
     s->nslots = slots;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    s->num_sms = std::max(1, s->num_sms);
+    s->reserved_sms = s->num_sms / 8;
     *out = s;
     return 0;
 }
@@ -396,6 +416,7 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
         }
         if (q != cudaSuccess) return fail(std::string("pf_server_poll: ") + cudaGetErrorString(q));
         deliver(s, r);
+        if (!r->small) s->large_sms_inflight -= r->sms;
         s->arena.release(r->off, r->bytes);
         s->in_use -= align256(r->bytes);
         (s->slots[r->slot].high ? s->free_high : s->free_low).push_back(r->slot);
@@ -404,12 +425,26 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
         s->inflight[i] = s->inflight.back();
         s->inflight.pop_back();
     }
-    // admissions, oldest first
-    while (!s->pending.empty() && (!s->free_high.empty() || !s->free_low.empty())) {
-        Req *r = s->pending.front();
+    // admissions, oldest first; a large request that would take SMs from the reserve waits, and
+    // the large ones behind it wait too (their order is kept), while small ones go past it
+    const int large_budget = std::max(1, s->num_sms - s->reserved_sms);
+    bool large_blocked = false;
+    for (auto it = s->pending.begin();
+         it != s->pending.end() && (!s->free_high.empty() || !s->free_low.empty());) {
+        Req *r = *it;
+        if (!r->small) {
+            // a request needing more than the whole budget runs alone
+            const bool fits = s->large_sms_inflight + r->sms <= large_budget || s->large_sms_inflight == 0;
+            if (large_blocked || !fits) {
+                large_blocked = true;
+                ++it;
+                continue;
+            }
+        }
         size_t off = 0;
         if (!s->arena.alloc(r->bytes, off)) break;
-        s->pending.pop_front();
+        it = s->pending.erase(it);
+        if (!r->small) s->large_sms_inflight += r->sms;
         r->off = off;
         s->in_use += align256(r->bytes);
         // small requests prefer high-priority streams, large ones low-priority ones
@@ -424,6 +459,13 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
         if (rc != 0) return rc;
     }
     return nd;
+}
+
+int pf_server_configure(pf_server *s, int reserved_sms, int large_request_ctas) {
+    if (!s || reserved_sms < 0 || large_request_ctas < 0) return fail("pf_server_configure: invalid argument");
+    s->reserved_sms = std::min(reserved_sms, s->num_sms - 1);
+    s->large_ctas = large_request_ctas > 0 ? large_request_ctas : (1 << 30);
+    return 0;
 }
 
 int pf_server_state(const pf_server *s, int *pending, int *inflight, long long *bytes_in_use) {

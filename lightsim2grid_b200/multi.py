@@ -84,17 +84,21 @@ class GridCases:
     N-1 instances for the drawn branches (islanded outages are skipped, as the reference's
     check_invertible does, ContingencyAnalysis.cpp:14-45)."""
 
-    def __init__(self, name, grid, branches, device, precision=1, max_iter=10, tol=1e-8, **plan_options):
+    def __init__(self, name, grid, branches, device, precision=1, max_iter=10, tol=1e-8, base_state=None,
+                 **plan_options):
         import torch
 
         self.name, self.grid, self.branches = name, grid, np.asarray(branches, np.int64)
         Y, S = grid.get_Ybus(), grid.get_Sbus()
         sl, w, pv, pq = grid.get_slack_ids(), grid.get_slack_weights(), grid.get_pv(), grid.get_pq()
-        base = Plan(Y, grid.flat_start(), S, sl, w, pv, pq, precision=0)
-        V, conv, _, _ = base.solve(grid.flat_start(), S, max_iter, tol)
-        if not conv:
-            raise RuntimeError("base case of {} did not converge".format(name))
-        del base
+        if base_state is None:
+            base = Plan(Y, grid.flat_start(), S, sl, w, pv, pq, precision=0)
+            V, conv, _, _ = base.solve(grid.flat_start(), S, max_iter, tol)
+            if not conv:
+                raise RuntimeError("base case of {} did not converge".format(name))
+            del base
+        else:  # (base-case voltages, injections) of an earlier GridCases of the same grid
+            V, S = base_state
         self.Vbase, self.Sbase = nat.as_c128(V).ravel().copy(), nat.as_c128(S).ravel().copy()
         self.plan = Plan(Y, V, S, sl, w, pv, pq, precision=precision, **plan_options)
         self.n = int(Y.shape[0])
@@ -158,13 +162,16 @@ class GridCases:
         return V, conv, it, er
 
 
-def build_uneven(parts, device, precision=1, max_iter=10, tol=1e-8, **plan_options):
+def build_uneven(parts, device, precision=1, max_iter=10, tol=1e-8, per_grid=None, **plan_options):
     """``parts``: list of (name, GridModel, drawn branches).  Returns (MultiBatch, [GridCases]).
     Jobs: one per solvable instance, grids ordered by decreasing size (costliest first), each
-    grid's instances hardest first (pf_n1_order)."""
+    grid's instances hardest first (pf_n1_order).  ``per_grid``: name -> plan options of that
+    grid (its schedule: elimination order, level slack, placement), over ``plan_options``."""
     import torch
 
-    cases = [GridCases(nm, g, br, device, precision, max_iter, tol, **plan_options) for nm, g, br in parts]
+    per_grid = per_grid or {}
+    cases = [GridCases(nm, g, br, device, precision, max_iter, tol, **dict(plan_options, **per_grid.get(nm, {})))
+             for nm, g, br in parts]
     order = sorted(range(len(cases)), key=lambda i: -cases[i].plan.info()["nnz_lu"])
     seg, first = [], []
     for i in order:
@@ -194,7 +201,8 @@ def main(argv=None):
     ap.add_argument("--total", type=int, default=4096)
     ap.add_argument("--repeat", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--threads", type=int, default=0, help="0: autotuned on a sample of the mix")
+    ap.add_argument("--threads", type=int, default=0,
+                    help="0: thread count and per-grid schedules autotuned on a sample of the mix")
     ap.add_argument("--seed", type=int, default=4096)
     args = ap.parse_args(argv)
     import torch
@@ -207,14 +215,13 @@ def main(argv=None):
     counts[-1] += args.total - sum(counts)
     grids = [(nm, synthetic.make_named_grid(nm)[0], k) for nm, k in zip(names, counts)]
     tuning = None
-    threads = args.threads
-    if threads <= 0:
+    best = {"threads": args.threads}
+    if args.threads <= 0:
         from .autotune import tune_uneven
 
         sample = draw_outages([(nm, g, max(8, k // 8)) for nm, g, k in grids], args.seed + 1)
         best, tuning = tune_uneven(sample, precision=1)
-        threads = best["threads"]
-    mb, cases = build_uneven(draw_outages(grids, args.seed), dev, precision=1, threads=threads)
+    mb, cases = build_uneven(draw_outages(grids, args.seed), dev, precision=1, **best)
     st = torch.cuda.current_stream()
     for _ in range(args.warmup):
         mb.launch(st.cuda_stream)

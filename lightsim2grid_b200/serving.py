@@ -160,7 +160,7 @@ class GridService:
 class NativeServer:
     """The library's serving core (``pf_server_*``) over ``GridService`` objects."""
 
-    def __init__(self, services, hbm_budget, slots, max_instances=64):
+    def __init__(self, services, hbm_budget, slots, max_instances=64, reserved_sms=None, large_request_ctas=0):
         self._lib = nat.load()
         self.names = list(services)
         self.index = {nm: i for i, nm in enumerate(self.names)}
@@ -179,8 +179,21 @@ class NativeServer:
         nat.check(self._lib.pf_server_create(grids, len(self.names), int(hbm_budget), int(slots), int(max_instances),
                                              nat.ctypes.byref(h)), "pf_server_create", self._lib)
         self._h = h
+        if reserved_sms is not None or large_request_ctas:
+            self.configure(reserved_sms, large_request_ctas)
         self._done = np.zeros(1024, np.int64)
         self.live = {}
+
+    def configure(self, reserved_sms=None, large_request_ctas=0):
+        """SM reservation for small requests (pf_server_configure): large requests are admitted
+        only while their CTAs leave ``reserved_sms`` SMs free (None: an eighth of the SMs), each
+        launched on at most ``large_request_ctas`` CTAs (0: no cap)."""
+        if reserved_sms is None:
+            import torch
+
+            reserved_sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count // 8
+        nat.check(self._lib.pf_server_configure(self._h, int(reserved_sms), int(large_request_ctas)),
+                  "pf_server_configure", self._lib)
 
     def submit(self, req):
         """Queues a request; its result arrays are allocated here (case order)."""
@@ -247,10 +260,10 @@ class PowerFlowServer:
     """Grids served from one GPU.  ``grids``: name -> GridModel."""
 
     def __init__(self, grids, device=None, hbm_budget=2 << 30, slots=32, precision=1, max_iter=10, tol=1e-8,
-                 max_instances=64, **plan_options):
+                 max_instances=64, reserved_sms=None, large_request_ctas=0, **plan_options):
         self.services = {name: GridService(name, g, precision=precision, max_iter=max_iter, tol=tol, **plan_options)
                          for name, g in grids.items()}
-        self.native = NativeServer(self.services, hbm_budget, slots, max_instances)
+        self.native = NativeServer(self.services, hbm_budget, slots, max_instances, reserved_sms, large_request_ctas)
 
     def serve(self, requests, realtime=True, clock=time.perf_counter):
         """Serves ``requests`` (sorted by arrival).  ``realtime``: a request is submitted when

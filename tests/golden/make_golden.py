@@ -65,7 +65,10 @@ def convert(src_dir, dst_dir):
 
 
 if __name__ == "__main__":
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/lightsim2grid/tests"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <reference checkout>/lightsim2grid/tests  (the folder holding "
+                 "case14.zip ... case1888.zip)")
+    src = sys.argv[1]
     dst = os.path.dirname(os.path.abspath(__file__))
     for path in convert(src, dst):
         print(path, os.path.getsize(path))

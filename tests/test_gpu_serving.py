@@ -17,8 +17,11 @@ def server():
     from lightsim2grid_b200 import synthetic
     from lightsim2grid_b200.serving import PowerFlowServer
 
-    grids = {name: synthetic.make_named_grid(name)[0] for name in ("grid14", "grid118", "grid300")}
-    srv = PowerFlowServer(grids, hbm_budget=1 << 30, slots=8, precision=1)
+    # the six grids of the serving workload (14 to 6,515 buses): the large grids' CTAs are the
+    # ones that stay resident longest beside other requests
+    grids = {name: synthetic.make_named_grid(name)[0]
+             for name in ("grid14", "grid118", "grid300", "grid1354", "grid2848", "grid6515")}
+    srv = PowerFlowServer(grids, hbm_budget=2 << 30, slots=16, precision=1, large_request_ctas=16)
     srv.grids = grids
     return srv
 
@@ -38,7 +41,11 @@ def test_mix_equals_alone(server):
     assert len(done) == len(reqs)
     assert server.last.peak_inflight >= 2  # work did overlap
     by_id = {r.rid: r for r in done}
-    for rid in sorted(by_id)[::5]:
+    # every fifth request, and every request on the three largest grids
+    picked = set(sorted(by_id)[::5]) | {rid for rid, r in by_id.items() if r.grid in ("grid1354", "grid2848",
+                                                                                     "grid6515")}
+    assert {by_id[rid].grid for rid in picked} >= {"grid1354", "grid2848", "grid6515"}
+    for rid in sorted(picked):
         mix = by_id[rid]
         alone = server.solve_alone(mix)
         assert np.array_equal(alone.errs, mix.errs) and np.array_equal(alone.iters, mix.iters)

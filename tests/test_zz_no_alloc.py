@@ -3,7 +3,8 @@ allocate device memory (work issued during CUDA-graph capture, hosts that own th
 budget, plugin hosts that forbid allocation on work calls).
 
 It must give the same answer as pf_batch_device on the same device-resident inputs, call
-after call, although its working memory is a static array shared by every call.  This file
+after call, although its working memory is a static array shared by every call -- including
+for instances that fail in FP32 and are solved again in FP64 inside the launch.  This file
 is collected last so that a failure here cannot hide any other test.
 """
 import numpy as np
@@ -14,12 +15,18 @@ from conftest import grid_problem
 pytestmark = pytest.mark.gpu
 
 
-def _device_batch(plan, c, ncases, dev):
+# outages of the 2,848-bus synthetic grid that keep it connected but that Newton-Raphson does not
+# solve within 10 iterations (found with the CPU oracle): a mixed-precision batch meets them in FP32
+# first, then re-solves them in FP64 inside the launch
+FAILING_2848 = (179, 1335, 1665, 1942, 2072, 2113, 2236, 2517, 3139, 3227, 3746)
+
+
+def _device_batch(plan, c, branches, dev):
     import torch
     from lightsim2grid_b200 import _native as nat
 
     g = c["grid"]
-    coeffs = [g.branch_coeffs([b]) for b in range(min(ncases, g.nb_powerline()))]
+    coeffs = [g.branch_coeffs([b]) for b in branches]
     cp = np.zeros(len(coeffs) + 1, np.int32)
     rows, cols, vals = [], [], []
     for k, lst in enumerate(coeffs):
@@ -60,17 +67,28 @@ def _device_batch(plan, c, ncases, dev):
     return ns, keep, outputs, desc
 
 
-@pytest.mark.parametrize("name,ncases,precision", [("grid118", 186, 0), ("grid118", 186, 1), ("grid2848", 400, 1)])
-def test_noalloc_matches_allocating_entry_point_twice(name, ncases, precision):
+@pytest.mark.parametrize("name,branches,precision", [
+    ("grid118", tuple(range(186)), 0),
+    ("grid118", tuple(range(186)), 1),
+    ("grid2848", tuple(range(400)), 1),
+    ("grid2848", tuple(range(120)) + FAILING_2848, 1),
+])
+def test_noalloc_matches_allocating_entry_point_twice(name, branches, precision):
     import torch
     from lightsim2grid_b200 import Plan, _native as nat
 
     dev = torch.device("cuda:0")
     torch.cuda.set_device(dev)
     c = grid_problem(name)
+    if set(FAILING_2848) <= set(branches):
+        # those outages fail from the base-case solution, the start point of a security analysis
+        base = Plan(c["Ybus"], c["V0"], c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=0)
+        Vn, conv, _, _ = base.solve(c["V0"], c["Sbus"], 10, 1e-8)
+        assert conv
+        c = dict(c, V0=Vn)
     plan = Plan(c["Ybus"], c["V0"], c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=precision)
     lib = plan._lib
-    ns, keep, outputs, desc = _device_batch(plan, c, ncases, dev)
+    ns, keep, outputs, desc = _device_batch(plan, c, branches, dev)
     stream = torch.cuda.current_stream().cuda_stream
 
     ref = outputs()
@@ -93,3 +111,31 @@ def test_noalloc_matches_allocating_entry_point_twice(name, ncases, precision):
         assert np.array_equal(it, it_ref), call
         ok = np.repeat(er_ref == 0, V.size // ns)
         assert np.abs(V[ok] - V_ref[ok]).max() <= 1e-10, call
+        if not np.all(er_ref == 0):
+            # failed instances: both entry points report the FP64 re-solve's final state
+            assert np.array_equal(V[~ok], V_ref[~ok]), call
+    if set(FAILING_2848) <= set(branches):
+        assert int((er_ref != 0).sum()) >= len(FAILING_2848)
+
+
+def test_noalloc_rejects_another_current_device():
+    """A plan is bound to the device it was built on: with another device current, the entry
+    point returns an error before it looks anything up or launches (host-side check)."""
+    import torch
+    from lightsim2grid_b200 import Plan, _native as nat
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    c = grid_problem("grid118")
+    torch.cuda.set_device(0)
+    plan = Plan(c["Ybus"], c["V0"], c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=1)
+    ns, keep, outputs, desc = _device_batch(plan, c, tuple(range(20)), torch.device("cuda:0"))
+    b = desc(outputs())
+    lib = plan._lib
+    torch.cuda.set_device(1)
+    try:
+        assert lib.pf_batch_device_noalloc(plan.handle, nat.ctypes.byref(b), None) == -1
+        assert "device" in nat.last_error(lib)
+        assert lib.pf_batch_device(plan.handle, nat.ctypes.byref(b), None) == -1
+    finally:
+        torch.cuda.set_device(0)
