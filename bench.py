@@ -463,17 +463,18 @@ def _config3(dev, stream, flush, K, W, threads, total=4096, seed=4096):
 SERVE_GRIDS = ("grid14", "grid118", "grid300", "grid1354", "grid2848", "grid6515")
 
 
-def _serve(seconds, rate, device):
+def _serve(seconds, rate, device, reserved_sms=None, large_request_ctas=0):
     """Serving leg: Poisson arrivals at `rate` requests/s for `seconds` over the six synthetic
     grids (14 to 6,515 buses); half the requests are one power flow with injections scaled by
-    U[0.9, 1.1] per bus, half an N-1 batch of 8 to 64 outages; mixed precision, tol 1e-8."""
+    U[0.9, 1.1] per bus, half an N-1 batch of 8 to 64 outages; mixed precision, tol 1e-8.
+    reserved_sms / large_request_ctas: the serving core's SM reservation (pf_server_configure)."""
     from lightsim2grid_b200 import synthetic
     from lightsim2grid_b200.serving import PowerFlowServer, latency_stats, make_requests
 
     grids = {g: synthetic.make_named_grid(g)[0] for g in SERVE_GRIDS}
     budget, slots = 4 << 30, 32
     srv = PowerFlowServer(grids, device=device, hbm_budget=budget, slots=slots, precision=1, max_iter=MAX_ITER,
-                          tol=TOL)
+                          tol=TOL, reserved_sms=reserved_sms, large_request_ctas=large_request_ctas)
     nb = {k: v.n_bus for k, v in grids.items()}
     nbr = {k: v.nb_powerline() for k, v in grids.items()}
     srv.serve(make_requests(nb, rate=rate, duration=min(1.0, seconds), seed=12345, branches_of=nbr))  # warm-up
@@ -488,10 +489,11 @@ def _serve(seconds, rate, device):
                 per["{}/{}".format(g, kind)] = {"p50_ms": float(np.percentile(lat, 50) * 1e3),
                                                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "count": int(lat.size)}
     st.update({"duration_s": seconds, "arrival_rate": rate, "grids": list(SERVE_GRIDS), "per_class": per,
+               "reserved_sms": reserved_sms, "large_request_ctas": large_request_ctas,
                "slots": slots, "hbm_budget_bytes": budget, "peak_inflight": srv.last.peak_inflight,
                "peak_bytes": srv.last.peak_bytes, "rejected": len(srv.last.rejected),
-               "latency": "arrival to result in pinned host memory (host clock)",
-               "kernel_launches": srv.last.launches if hasattr(srv.last, "launches") else None})
+               "latency": "arrival to result in the caller's host arrays (host clock)",
+               "host_loop": srv.last.host_stats()})
     return st
 
 
@@ -757,7 +759,8 @@ def run_case(argv):
     """One N-1 batch of a grid through pf_batch_device, for profilers (ncu) and quick timing."""
     ap = argparse.ArgumentParser(prog="bench.py case")
     ap.add_argument("--grid", default="grid2848")
-    ap.add_argument("--cases", type=int, default=0, help="first N branches (0: all)")
+    ap.add_argument("--cases", type=int, default=0, help="N branches from --first (0: all)")
+    ap.add_argument("--first", type=int, default=0, help="first branch")
     ap.add_argument("--precision", type=int, default=1)
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
@@ -775,7 +778,6 @@ def run_case(argv):
     ap.add_argument("--ordering", type=int, default=0)
     ap.add_argument("--placement", type=int, default=0)
     ap.add_argument("--level-slack", type=int, default=0)
-    ap.add_argument("--op-prefetch", type=int, default=0)
     ap.add_argument("--no-trace", action="store_true", help="skip the phase-cycle and trace launches")
     args = ap.parse_args(argv)
 
@@ -788,19 +790,20 @@ def run_case(argv):
                            g.get_pv(), g.get_pq(), 10, 1e-8):
         raise SystemExit("base case did not converge")
     Vn = base.get_V()
-    nb = g.nb_powerline() if args.cases <= 0 else min(args.cases, g.nb_powerline())
+    first = max(0, min(args.first, g.nb_powerline()))
+    nb = g.nb_powerline() - first if args.cases <= 0 else min(args.cases, g.nb_powerline() - first)
+    branches = range(first, first + nb)
     dev = torch.device("cuda:0")
     opts = dict(threads=args.threads, lu_placement=args.lu_placement, max_ctas_per_sm=args.ctas_per_sm,
                 refine=args.refine, lu_reuse_threshold=args.lu_reuse, batch_layout=args.batch_layout,
-                ordering=args.ordering, placement=args.placement, level_slack=args.level_slack,
-                op_prefetch=args.op_prefetch)
+                ordering=args.ordering, placement=args.placement, level_slack=args.level_slack)
     if args.dc or args.fdpf >= 0:
         # DC / FDPF: the grid's DC Ybus and outage coefficients, or its B' / B''
         gd = _DCView(g) if args.dc else g
         opts.update(dc=args.dc, fdpf=g.get_Bp_Bpp(args.fdpf) if args.fdpf >= 0 else None)
-        d = N1Device(gd, Vn, dev, 0, branches=range(nb), case_order=True, **opts)
+        d = N1Device(gd, Vn, dev, 0, branches=branches, case_order=True, **opts)
     else:
-        d = N1Device(g, Vn, dev, args.precision, branches=range(nb), case_order=args.case_order, **opts)
+        d = N1Device(g, Vn, dev, args.precision, branches=branches, case_order=args.case_order, **opts)
     d.batch.max_iter = args.max_iter
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
@@ -833,7 +836,7 @@ def run_case(argv):
         trace = np.diff(tr[:ntr]).astype(int).tolist()
     check = None
     if args.check:
-        ref = N1Device(g, Vn, dev, 0, branches=range(nb), case_order=args.case_order)
+        ref = N1Device(g, Vn, dev, 0, branches=branches, case_order=args.case_order)
         ref.launch(stream.cuda_stream)
         torch.cuda.synchronize()
         Vf, itf, ef = ref.results()
@@ -867,9 +870,28 @@ class _DCView:
         return getattr(self.g, k)
 
 
+def run_serve(argv):
+    """The serving leg alone: ``python bench.py serve [--seconds S --rate R --reserve K --large-ctas C]``."""
+    ap = argparse.ArgumentParser(prog="bench.py serve")
+    ap.add_argument("--seconds", type=float, default=10.0)
+    ap.add_argument("--rate", type=float, default=2000.0)
+    ap.add_argument("--reserve", type=int, default=-1, help="SMs reserved for small requests (-1: default)")
+    ap.add_argument("--large-ctas", type=int, default=0, help="CTAs per large request (0: no cap)")
+    args = ap.parse_args(argv)
+    import torch
+
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    out = _serve(args.seconds, args.rate, dev, None if args.reserve < 0 else args.reserve, args.large_ctas)
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     if len(sys.argv) > 1 and sys.argv[1] == "case":
         return run_case(sys.argv[2:])
+    if len(sys.argv) > 1 and sys.argv[1] == "serve":
+        return run_serve(sys.argv[2:])
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)

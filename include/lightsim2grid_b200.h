@@ -40,11 +40,15 @@ typedef struct pf_options {
                                1e-5: 5-9 % faster, same iterations and flags, but results up
                                to 5e-8 pu from the FP64 ones instead of 3e-10               */
     int batch_layout;       /* Newton batches of independent instances (no time-series chain):
-                               0 auto (one CTA per instance), 1 one CTA per instance, 2 batch-
-                               interleaved: 32 instances per CTA, one per lane, every value
-                               stored as 32 consecutive per-instance values (coalesced, the
-                               batch dimension amortises each phase); its per-CTA memory is
-                               allocated on first use                                         */
+                               0 auto: batch-interleaved for plans whose LU stays in global
+                               memory with at least 80,000 entries (6,515 buses) and 4 jobs per
+                               SM or more, else one CTA per instance; 1 one CTA per instance; 2
+                               batch-interleaved: 32 instances per CTA, one per lane, every value
+                               stored as 32 consecutive per-instance values (coalesced, the batch
+                               dimension amortises each phase), the last running instances of a
+                               CTA and, mixed form, the FP32 failures handed to the one-CTA
+                               kernel in the same stream; its per-CTA memory is allocated on
+                               first use                                                     */
     int ordering;           /* elimination order of the first factorisation.  0: default, minimum
                                degree preferring low elimination levels (among the vertices of
                                degree up to the minimum + 2, the lowest level) on 8 relabellings
@@ -52,19 +56,15 @@ typedef struct pf_options {
                                depth (no added fill, fewer dependent phases), the shallowest kept;
                                1: plain minimum degree only; 2: as 0 with one labelling; 3: as 0
                                without the level preference                                    */
-    int placement;          /* packed programs (LU in shared memory): 0 default, clusters of
-                               operations writing one value in their thread's first slots; 1
-                               clusters spread over the phase's slots (fewer bank conflicts in
-                               the host model, longer plan build).  Same results either way     */
+    int placement;          /* packed programs (LU in shared memory): 0 default = 1; 1 clusters
+                               of operations writing one value spread over the phase's slots
+                               (fewer bank conflicts: 2848-bus factor 36.7k -> 30.6k shared-memory
+                               wavefronts, N-1 batch 11.37 -> 11.23 ms); 2 clusters in their
+                               thread's first slots (shorter plan build).  Same results          */
     int level_slack;        /* orderings 0 and 2: minimum degree takes, among the vertices of
                                degree up to the minimum + level_slack, the one of lowest
                                elimination level.  0: default (2); < 0: no level preference;
                                larger values give shallower plans for some more fill          */
-    int op_prefetch;        /* Newton kernels: the operations of the phase k phases ahead are
-                               prefetched into L1 when a phase starts (k = op_prefetch), instead
-                               of the next phase's first operations being loaded into registers
-                               (which the phase's closing barrier waits for).  0: default; < 0:
-                               off.  Same results either way                                    */
 } pf_options;
 
 /* DC power flow plan (BaseDCAlgo::compute_pf, src/powerflow_algorithm/BaseDCAlgo.tpp:5-175;
@@ -212,8 +212,9 @@ int pf_batch_ts(pf_plan *plan, int nsteps, const double *Sbus_ri, const double *
                 double tol, double *V_out_ri, int *converged, int *iters, int *errs, int *status);
 
 /* Device-resident batch on `stream` (a cudaStream_t, NULL for the default stream).  No
-   host synchronisation; capturable in a CUDA graph once the plan exists (with batch_layout 2,
-   after one call outside capture: that layout's per-CTA memory is allocated on first use).
+   host synchronisation; capturable in a CUDA graph once the plan exists (when the batch-
+   interleaved layout runs -- batch_layout 2, or auto on large global-LU plans -- after one call
+   of the same size outside capture: that layout's per-CTA memory is allocated on first use).
    Mixed form: a job with an instance that does not converge in FP32 is solved again in FP64
    inside the launch (option fp64_fallback), so the outputs are the FP64 outcome for those
    instances.  The current device must be the plan's (else -1, nothing launched). */

@@ -7,8 +7,9 @@ depends on the grid and on the batch, so they are measured on the device:
   preference for low elimination levels among the vertices of degree up to the minimum +
   ``level_slack`` (``ordering`` 0; slack 2 by default, larger slacks give fewer, wider phases
   for a little more fill), or without that preference (``ordering`` 3);
-* ``placement`` places the packed programs' clusters of operations in the first slots of
-  their threads (0) or spread over the phase (1), trading shared-memory bank conflicts;
+* ``placement`` spreads the packed programs' clusters of operations over the phase (1, the
+  default) or puts them in the first slots of their threads (2), trading shared-memory bank
+  conflicts;
 * ``threads`` is the width every phase is packed for and, with the shared-memory layout, sets
   the CTAs resident per SM;
 * ``batch_layout`` picks one CTA per instance (1) or the batch-interleaved tile kernel (2: 32
@@ -82,7 +83,7 @@ def schedule_candidates(m):
     """Elimination-order and placement candidates (threads left to the plan's default)."""
     out = []
     for order in ({"ordering": 0}, {"ordering": 0, "level_slack": 4}, {"ordering": 3}):
-        for placement in (0, 1):
+        for placement in (1, 2):
             out.append(dict(order, placement=placement))
     return out
 

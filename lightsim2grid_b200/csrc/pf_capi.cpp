@@ -22,9 +22,6 @@ namespace {
 
 thread_local std::string g_err;
 
-// op_prefetch default: phases ahead whose operations are prefetched into L1 (0: none)
-constexpr int kDefaultOpPrefetch = 0;
-
 int fail(int code, const std::string &msg) {
     g_err = msg;
     return code;
@@ -96,8 +93,11 @@ struct pf_plan {
     // fast-decoupled plans: the B' and B'' systems
     l2g::DevPlan dsub[2]{};
     void *d_sub_int[2] = {nullptr, nullptr}, *d_sub_dbl[2] = {nullptr, nullptr};
-    // batch-interleaved kernel: per-CTA slabs (allocated on first use) and their size
-    DevBuf tile_scratch;
+    // batch-interleaved kernel: per-CTA slabs, hand-off lists and a row of ones (allocated on
+    // first use)
+    DevBuf tile_scratch, tile_aux;
+    int tile_ones = 0;       // instances for which tile_aux holds the row of ones
+    bool last_tile = false;  // the last launch ran the batch-interleaved kernel
     // device work buffers
     DevBuf scratch, counter, V0, Sbus, optr, opos, oval, jfirst, jcount, Vout, iters, errs, Jout, cycles, Vcase,
         casemap;
@@ -516,7 +516,7 @@ int configure(pf_plan *pl) {
 }
 
 void release(pf_plan *pl) {
-    for (DevBuf *b : {&pl->tile_scratch, &pl->scratch, &pl->counter, &pl->V0, &pl->Sbus, &pl->optr, &pl->opos, &pl->oval,
+    for (DevBuf *b : {&pl->tile_scratch, &pl->tile_aux, &pl->scratch, &pl->counter, &pl->V0, &pl->Sbus, &pl->optr, &pl->opos, &pl->oval,
                       &pl->jfirst, &pl->jcount, &pl->Vout, &pl->iters, &pl->errs, &pl->Jout, &pl->cycles,
                       &pl->Vcase, &pl->casemap})
         b->release();
@@ -542,40 +542,89 @@ void release(pf_plan *pl) {
 // The number of CTAs is bounded by the slabs that fit in the scratch.
 // Whether a launch runs the batch-interleaved kernel: Newton plans, independent instances (no
 // chain), no per-launch diagnostics (J output, phase cycles or trace, LU reuse), and option
-// batch_layout 2 (auto keeps one CTA per instance, measured faster on every grid so far).
-// Phases ahead whose operations the Newton kernel prefetches into L1 (option op_prefetch:
-// 0 default, < 0 off).
-int op_prefetch_of(const pf_plan *pl) {
-    const int o = pl->opt.op_prefetch;
-    if (o < 0) return 0;
-    return o > 0 ? std::min(o, 8) : kDefaultOpPrefetch;
-}
+// batch_layout 2, or auto (0) for plans whose LU stays in global memory and is large (at least
+// kAutoTileLU entries) with several jobs per SM: measured on the 6,515-bus N-1 batch, 87.7 against
+// 105 ms (mixed) and 88.7 against 140 ms (FP64); where the LU sits in shared memory (up to 2,848
+// buses mixed) one CTA per instance is faster.
+constexpr int kAutoTileLU = 80000;
 
 bool use_tile(const pf_plan *pl, const l2g::BatchArgs &a) {
     if (pl->P.dc || pl->P.fdpf || a.chain || a.Jout || a.phase_cycles || a.trace || a.reuse_below > 0) return false;
-    return pl->opt.batch_layout == 2;
+    if (pl->opt.batch_layout == 2) return true;
+    return pl->opt.batch_layout == 0 && !pl->lu_in_smem && pl->P.nnzLU >= kAutoTileLU && a.njobs >= 4 * pl->num_sms;
 }
 
+int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, unsigned char *scratch,
+                size_t scratch_bytes, int *counter, bool allow_tile, bool allow_inline);
+
+// The batch-interleaved kernel, then the one-CTA kernel over what it handed off: its stragglers
+// (continued from their state) and, in the mixed form, its FP32 failures (re-solved in FP64 from
+// their start voltages).  The lists and their counts stay in device memory: no host
+// synchronisation.  Counter words: [0] jobs, [2] stragglers, [3] FP32 failures, [8..9] and [12..13]
+// the two follow-up launches.
 int launch_tile(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, int *counter) {
     const int lub = precision ? 4 : 8;
     const size_t slab = l2g::tile_slab_bytes(pl->dp, lub);
     const int grid = std::max(1, std::min(pl->num_sms, a.njobs));
     cudaError_t e = pl->tile_scratch.ensure(slab * (size_t)grid);
     if (e != cudaSuccess) return cuda_fail(e, "launch: batch-interleaved scratch allocation");
+    const int ni = std::max(a.n_inst, 1);
+    e = pl->tile_aux.ensure((size_t)3 * ni * sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e, "launch: batch-interleaved hand-off lists");
+    int *hand = static_cast<int *>(pl->tile_aux.p), *fbl = hand + ni, *ones = hand + 2 * (size_t)ni;
+    if (pl->tile_ones < ni) {
+        std::vector<int> one((size_t)ni, 1);
+        e = cudaMemcpyAsync(ones, one.data(), (size_t)ni * sizeof(int), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "launch: batch-interleaved job counts");
+        pl->tile_ones = ni;
+    }
+    const l2g::BatchArgs orig = a;
     a.scratch = static_cast<unsigned char *>(pl->tile_scratch.p);
     a.slab_bytes = (long long)slab;
     a.job_counter = counter;
     // spread the jobs over all CTAs: lanes per CTA
     a.tile_lanes = std::max(1, std::min(32, (a.njobs + grid - 1) / grid));
-    e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    a.hand_list = hand;
+    a.hand_count = counter + 2;
+    a.hand_lanes = std::max(1, a.tile_lanes / 2);
+    const bool fallback = precision == 1 && pl->precision == 1 && pl->opt.fp64_fallback != 2 && a.refine;
+    a.fb_list = fallback ? fbl : nullptr;
+    a.fb_count = counter + 3;
+    e = cudaMemsetAsync(counter, 0, 16 * sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "launch: counter reset");
     e = l2g::launch_nr_tile(pl->dp, a, precision, grid, st);
     if (e != cudaSuccess) return cuda_fail(e, "launch: batch-interleaved kernel");
+    // the stragglers, from their output rows and iteration counts (the mixed form's in-launch FP64
+    // fallback covers their failures)
+    l2g::BatchArgs c = orig;
+    c.job_first = hand;
+    c.job_count = ones;
+    c.njobs = a.n_inst;
+    c.njobs_dev = counter + 2;
+    c.it_start = a.iters;
+    c.v0_from_out = 1;
+    int rc = launch_into(pl, c, precision, st, static_cast<unsigned char *>(pl->scratch.p),
+                         pl->slab_fb * (size_t)pl->grid, counter + 8, false, true);
+    if (rc) return rc;
+    if (fallback) {
+        l2g::BatchArgs f = orig;
+        f.job_first = fbl;
+        f.job_count = ones;
+        f.njobs = a.n_inst;
+        f.njobs_dev = counter + 3;
+        rc = launch_into(pl, f, 0, st, static_cast<unsigned char *>(pl->scratch.p), pl->slab_fb * (size_t)pl->grid,
+                         counter + 12, false, false);
+        if (rc) return rc;
+    }
+    pl->last_inline = fallback;
+    pl->last_tile = true;
     return 0;
 }
 
 int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, unsigned char *scratch,
                 size_t scratch_bytes, int *counter, bool allow_tile = false, bool allow_inline = false) {
+    pl->last_tile = false;
     a.scratch = scratch;
     a.slab_bytes = (long long)pl->slab;
     a.job_counter = counter;
@@ -583,7 +632,6 @@ int launch_into(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, u
     a.refine = (precision == 1 && pl->refine) ? 1 : 0;
     a.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
     a.reuse_below = lu_reuse_below(pl, a.refine_below);
-    a.op_prefetch = op_prefetch_of(pl);
     pl->last_inline = false;
     if (a.njobs <= 0) return 0;
     if (allow_tile && use_tile(pl, a)) return launch_tile(pl, a, precision, st, counter);
@@ -731,10 +779,9 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
     if ((e = cudaMemcpyAsync(errs, pl->errs.p, (size_t)n_inst * sizeof(int), cudaMemcpyDeviceToHost, st)) !=
         cudaSuccess)
         return cuda_fail(e, "batch: download");
-    int inline_reruns = 0;  // instances the launch re-solved in FP64 itself
+    int words[16] = {0};  // the launch's counters: re-solves in FP64 done on the device
     if (pl->last_inline &&
-        (e = cudaMemcpyAsync(&inline_reruns, static_cast<int *>(pl->counter.p) + 1, sizeof(int),
-                             cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        (e = cudaMemcpyAsync(words, pl->counter.p, sizeof(words), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_fail(e, "batch: download");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "batch: kernel execution");
     float kms = 0.f;
@@ -743,7 +790,7 @@ int run_batch(pf_plan *pl, int n_inst, const cplx *V0, long long v0_stride, cons
     // mixed form: re-run in FP64 the jobs that contain a failure.  `settled` (if given) is called
     // once the re-run is queued, with the instances it recomputes: every other instance's row is
     // final, so the caller can copy those rows out while the re-run runs.
-    int rerun = inline_reruns;
+    int rerun = pl->last_tile ? words[3] + words[9] : words[1];
     std::vector<char> again;
     if (settled) again.assign((size_t)n_inst, 0);
     if (pl->precision == 1 && pl->opt.fp64_fallback != 2 && !pl->last_inline) {
@@ -910,7 +957,7 @@ int pf_plan_create(int n, const int *colptr, const int *rowind, const double *yb
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
     po.level_slack = level_slack_of(pl->opt);
     po.elem_bytes = pl->opt.precision ? 4 : 8;
-    po.spread_clusters = pl->opt.placement == 1;
+    po.spread_clusters = pl->opt.placement != 2;
     {
         const int m_est = npv + (distributed && nslack > 1 ? nslack - 1 : 0) + 2 * npq + (distributed ? 1 : 0);
         int thr = pl->opt.threads;
@@ -951,7 +998,7 @@ int pf_dc_plan_create(int n, const int *colptr, const int *rowind, const double 
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
     po.level_slack = level_slack_of(pl->opt);
     po.elem_bytes = pl->opt.precision ? 4 : 8;
-    po.spread_clusters = pl->opt.placement == 1;
+    po.spread_clusters = pl->opt.placement != 2;
     int thr = pl->opt.threads;
     if (thr <= 0) thr = n > 2000 ? 512 : (n > 300 ? 256 : 128);
     thr = std::max(32, std::min(512, (thr / 32) * 32));
@@ -989,7 +1036,7 @@ int pf_fdpf_plan_create(int n, const int *colptr, const int *rowind, const doubl
     po.order_trials = pl->opt.ordering == 1 ? 0 : (pl->opt.ordering == 2 ? 1 : 8);
     po.level_slack = level_slack_of(pl->opt);
     po.elem_bytes = pl->opt.precision ? 4 : 8;
-    po.spread_clusters = pl->opt.placement == 1;
+    po.spread_clusters = pl->opt.placement != 2;
     int thr = pl->opt.threads;
     if (thr <= 0) {
         // factors in global memory, read through L1 by every CTA of an SM, and several small
@@ -1784,7 +1831,6 @@ int pf_multi_create(pf_plan *const *plans, const pf_device_batch *batches, int n
         sg.A.refine = mp->refine ? 1 : 0;
         sg.A.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
         sg.A.reuse_below = lu_reuse_below(pl, sg.A.refine_below);
-        sg.A.op_prefetch = op_prefetch_of(pl);
     }
     e = cudaMemcpy(mp->segs.p, host.data(), sizeof(l2g::Segment) * (size_t)nseg, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {

@@ -245,54 +245,6 @@ __device__ __forceinline__ void load_first2(const OP *__restrict__ ops, const in
     }
 }
 
-// Hint that the thread's first four operations of phase p will be read soon: a prefetch into L1
-// has no destination register, so the barrier that ends the current phase does not wait for it
-// (it waits for loads in flight), and the loads of phase p then hit L1.
-template <typename OP>
-__device__ __forceinline__ void prefetch_phase(const OP *__restrict__ ops, const int *sb, const int *sw, int nph,
-                                               int p) {
-    if (p < nph) {
-        const int w = sw[p];
-        if ((int)threadIdx.x < w) {
-            const int e = sb[p + 1];
-#pragma unroll
-            for (int j = 0, k = sb[p] + (int)threadIdx.x; j < 4; ++j, k += w)
-                if (k < e) asm volatile("prefetch.L1 [%0];" ::"l"(ops + k));
-        }
-    }
-}
-
-template <typename OP, typename F>
-__device__ __forceinline__ void run_phase_body(const OP *__restrict__ ops, const int *sb, const int *sw, int p,
-                                               OpPair<OP> &cur, OP none, F &&apply) {
-    const int w = sw[p];
-    if ((int)threadIdx.x < w) {
-        const int e = sb[p + 1];
-        int k = sb[p] + threadIdx.x;
-        OP c = none, d = none;
-        if (k + 2 * w < e) c = ops[k + 2 * w];
-        if (k + 3 * w < e) d = ops[k + 3 * w];
-        for (;;) {
-            if (k >= e) break;
-            apply(cur.a);
-            if (k + 4 * w < e) cur.a = ops[k + 4 * w];
-            k += w;
-            if (k >= e) break;
-            apply(cur.b);
-            if (k + 4 * w < e) cur.b = ops[k + 4 * w];
-            k += w;
-            if (k >= e) break;
-            apply(c);
-            if (k + 4 * w < e) c = ops[k + 4 * w];
-            k += w;
-            if (k >= e) break;
-            apply(d);
-            if (k + 4 * w < e) d = ops[k + 4 * w];
-            k += w;
-        }
-    }
-}
-
 template <typename OP, typename F>
 __device__ __forceinline__ void run_phase(const OP *__restrict__ ops, const int *sb, const int *sw, int nph, int p,
                                           OpPair<OP> &cur, OpPair<OP> &nxt, OP none, F &&apply, Trace &tr) {
@@ -327,25 +279,10 @@ __device__ __forceinline__ void run_phase(const OP *__restrict__ ops, const int 
     tr.mark();
 }
 
-// pf > 0: the operations of phase p + pf are prefetched into L1 when phase p starts, and each
-// phase loads its own first operations (from L1) instead of the previous phase loading them into
-// registers.
 template <typename OP, typename F>
 __device__ void run_program(const OP *__restrict__ ops, const int *sb, const int *sw, int nph, OP none, F &&apply,
-                            Trace &tr, int pf = 0) {
+                            Trace &tr) {
     if (nph <= 0) return;
-    if (pf > 0) {
-        for (int q = 0; q < pf; ++q) prefetch_phase<OP>(ops, sb, sw, nph, q);
-        for (int p = 0; p < nph; ++p) {
-            prefetch_phase<OP>(ops, sb, sw, nph, p + pf);
-            OpPair<OP> cur;
-            load_first2<OP>(ops, sb, sw, nph, p, cur, none);
-            run_phase_body<OP>(ops, sb, sw, p, cur, none, apply);
-            __syncthreads();
-            tr.mark();
-        }
-        return;
-    }
     OpPair<OP> A, B;
     load_first2<OP>(ops, sb, sw, nph, 0, A, none);
     for (int p = 0; p < nph; p += 2) {
@@ -359,14 +296,14 @@ __device__ void run_program(const OP *__restrict__ ops, const int *sb, const int
 // index space, or int4 operations over the global LU and the shared solve vector.
 template <typename LT, typename XT, bool LU_SMEM>
 __device__ __forceinline__ void run_lu_program(const uint2 *cops, const int4 *ops, const int *sb, const int *sw,
-                                               int nph, int m, LT *lu, XT *x, Trace &tr, int pf = 0) {
+                                               int nph, int m, LT *lu, XT *x, Trace &tr) {
     if constexpr (LU_SMEM) {
         static_assert(sizeof(LT) == sizeof(XT), "the packed layout needs one element type");
         const uint2 none = make_uint2((unsigned)m | ((unsigned)m << 16), (unsigned)m | ((unsigned)m << 16));
-        run_program<uint2>(cops, sb, sw, nph, none, [x](const uint2 o) { run_op_packed<XT>(o, x); }, tr, pf);
+        run_program<uint2>(cops, sb, sw, nph, none, [x](const uint2 o) { run_op_packed<XT>(o, x); }, tr);
     } else {
         run_program<int4>(ops, sb, sw, nph, empty_op<int4>(), [lu, x](const int4 o) { run_op<LT, XT>(o, lu, x); },
-                          tr, pf);
+                          tr);
     }
 }
 
@@ -491,7 +428,6 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                                           int first, int count, Prof &pr) {
     const int tid = threadIdx.x;
     const int n = P.n, m = P.m;
-    const int pf = A.op_prefetch;
     XT *x = L.x;
     LT *lu = L.lu;
     double2 *V = L.V, *Ibus = L.Ibus, *Fbus = L.Fbus;
@@ -508,7 +444,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
         const int inst = first + step;
         const double2 *Sb = A.Sbus + (long long)inst * A.sbus_stride;
         if (step == 0 || !A.chain) {
-            const double2 *v0 = A.V0 + (long long)inst * A.v0_stride;
+            const double2 *v0 = A.v0_from_out ? out_row(A, inst, n) : A.V0 + (long long)inst * A.v0_stride;
             for (int b = tid; b < n; b += blockDim.x) {
                 const double2 v = v0[b];
                 V[b] = v;
@@ -571,7 +507,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
         mismatch<XT>(P, S, Vs ? Vs : V, Ibus, Fbus, Sb, x, norm, bad);
         pr.mark(0);
         bool conv = !bad && norm < A.tol;
-        int it = 0, err = 0;
+        int it = A.it_start ? A.it_start[inst] : 0, err = 0;
         double *Jout = (A.Jout && inst == A.j_inst) ? A.Jout : nullptr;
         Trace tr{(A.trace != nullptr && blockIdx.x == 0 && pr.traced == 0) ? A.trace : nullptr, A.trace_cap, 0};
         pr.traced = 1;
@@ -589,7 +525,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 __syncthreads();
                 pr.mark(1);
                 // refactorisation with the forward substitution of the right-hand side fused in
-                run_lu_program<LT, XT, LU_SMEM>(P.fac_cops, P.fac_ops, L.sb_fac, L.sw_fac, P.fac_nph, m, lu, x, tr, pf);
+                run_lu_program<LT, XT, LU_SMEM>(P.fac_cops, P.fac_ops, L.sb_fac, L.sw_fac, P.fac_nph, m, lu, x, tr);
                 check_pivots<LT>(P, S, lu);
                 pr.mark(2);
                 if (S.piv_err) {
@@ -598,10 +534,10 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 }
                 have_lu = true;
             } else {
-                run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr, pf);
+                run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr);
                 pr.mark(3);
             }
-            run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr, pf);
+            run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr);
             scale_by_pivots<LT, XT>(P, lu, x);
             pr.mark(4);
             if (refine_now) {
@@ -609,8 +545,8 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 __syncthreads();
                 newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, x);
                 __syncthreads();
-                run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr, pf);
-                run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr, pf);
+                run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr);
+                run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr);
                 scale_by_pivots<LT, XT>(P, lu, x);
                 pr.mark(5);
             }
@@ -710,7 +646,7 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, cons
     const int tid = threadIdx.x;
     const bool multi = M.segs != nullptr;
     int *const counter = multi ? M.job_counter : A0.job_counter;
-    const int njobs = multi ? M.njobs : A0.njobs;
+    const int njobs = multi ? M.njobs : (A0.njobs_dev ? min(A0.njobs, *A0.njobs_dev) : A0.njobs);
     Prof pr;
     pr.start(A0.phase_cycles != nullptr && tid == 0);
     int cur = -1;
@@ -751,10 +687,22 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, cons
                 }
                 __syncthreads();
                 if (S.job_failed) {
-                    // the word after the job counter counts the instances re-solved in FP64
-                    if (tid == 0 && seg.A.job_counter != nullptr) atomicAdd(seg.A.job_counter + 1, count);
+                    // the word after the job counter counts the instances re-solved in FP64; the
+                    // re-solve starts afresh from the instance's start voltages
+                    const int *its = seg.A.it_start;
+                    const int vfo = seg.A.v0_from_out;
+                    if (tid == 0) {
+                        if (seg.A.job_counter != nullptr) atomicAdd(seg.A.job_counter + 1, count);
+                        seg.A.it_start = nullptr;
+                        seg.A.v0_from_out = 0;
+                    }
+                    __syncthreads();
                     fp64_rerun(seg.P, seg.A, S, dyn, first, count);
                     __syncthreads();
+                    if (tid == 0) {
+                        seg.A.it_start = its;
+                        seg.A.v0_from_out = vfo;
+                    }
                     stage_tables<LT, XT>(seg.P, L);  // the FP64 solve vector covered them
                     __syncthreads();
                 }

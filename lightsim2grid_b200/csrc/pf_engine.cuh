@@ -75,14 +75,19 @@ struct BatchArgs {
                                        // instance: clock after every phase of every program
     int trace_cap;
     int tile_lanes;                    // batch-interleaved kernel: lanes (instances) per CTA
+    // hand-off from the batch-interleaved kernel to the one-CTA kernel (no host synchronisation):
+    int *hand_list, *hand_count;       // instances continued from their current state (stragglers)
+    int hand_lanes;                    // ... once the jobs are exhausted and at most this many of a
+                                       // CTA's lanes are still running
+    int *fb_list, *fb_count;           // mixed form: instances that failed in FP32, re-solved in FP64
+    const int *njobs_dev;              // one-CTA kernel: job count in device memory (min with njobs)
+    const int *it_start;               // ... iterations an instance has already taken (null: 0)
+    int v0_from_out;                   // ... an instance starts from its output row (its state)
     const int *vout_row;               // optional: output row of each instance (default: the instance)
     int zero_failed;                   // 1: an instance that did not converge writes a zero row
     int fp64_inline;                   // mixed form: a job that failed in FP32 is solved again in FP64
                                        // by the same CTA (slab_bytes then holds an FP64 LU, and the
                                        // dynamic shared memory an FP64 solve vector)
-    int op_prefetch;                   // Newton phase programs: phases ahead whose operations are
-                                       // prefetched into L1 (0: operations loaded into registers
-                                       // one phase ahead)
 };
 
 // The output row of an instance (Vout may be mapped host memory: rows stream out as instances

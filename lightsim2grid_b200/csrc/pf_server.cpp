@@ -14,10 +14,13 @@
 
 #include <algorithm>
 #include <complex>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <list>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pf_capi_internal.hpp"
@@ -134,11 +137,34 @@ struct pf_server {
     std::vector<Req *> inflight;
     // SM reservation for small requests (see kSmallWork)
     int num_sms = 1, reserved_sms = 0, large_ctas = 1 << 30, large_sms_inflight = 0;
+    // delivery: copying a finished request's rows from pinned staging into the caller's arrays
+    // (megabytes for N-1 batches of the large grids) runs on worker threads, so the polling thread
+    // keeps admitting and completing other requests meanwhile
+    std::vector<std::thread> workers;
+    mutable std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Req *> to_deliver;   // device work done, rows not yet copied
+    std::vector<Req *> delivered;   // rows copied: slot and id returned by the next poll
+    bool stop = false;
 };
 
 namespace {
 
+void stop_workers(pf_server *s) {
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    for (std::thread &t : s->workers)
+        if (t.joinable()) t.join();
+    s->workers.clear();
+}
+
 void destroy(pf_server *s) {
+    stop_workers(s);
+    for (Req *r : s->to_deliver) delete r;
+    for (Req *r : s->delivered) delete r;
     for (Grid &g : s->grids) {
         if (g.dV0) cudaFree(g.dV0);
         if (g.dS) cudaFree(g.dS);
@@ -283,6 +309,22 @@ void deliver(pf_server *s, Req *r) {
     }
 }
 
+void delivery_worker(pf_server *s) {
+    for (;;) {
+        Req *r = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv.wait(lk, [s] { return s->stop || !s->to_deliver.empty(); });
+            if (s->to_deliver.empty()) return;  // stopping
+            r = s->to_deliver.front();
+            s->to_deliver.pop_front();
+        }
+        deliver(s, r);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->delivered.push_back(r);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -368,6 +410,14 @@ int pf_server_create(const pf_server_grid *grids, int ngrids, long long hbm_budg
     cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, dev);
     s->num_sms = std::max(1, s->num_sms);
     s->reserved_sms = s->num_sms / 8;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nworkers = (int)std::max(1u, std::min(4u, hw > 2 ? hw / 2 : 1u));
+    try {
+        for (int i = 0; i < nworkers; ++i) s->workers.emplace_back(delivery_worker, s);
+    } catch (const std::exception &ex) {
+        destroy(s);
+        return fail(std::string("pf_server_create: delivery threads: ") + ex.what());
+    }
     *out = s;
     return 0;
 }
@@ -406,8 +456,22 @@ int pf_server_submit(pf_server *s, long long id, int grid, int kind, const doubl
 int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
     if (!s || (cap > 0 && !done_ids)) return fail("pf_server_poll: invalid argument");
     int nd = 0;
-    // completions
-    for (size_t i = 0; i < s->inflight.size() && nd < cap;) {
+    // requests whose rows the workers copied: their slot is free again
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        size_t k = 0;
+        for (; k < s->delivered.size() && nd < cap; ++k) {
+            Req *r = s->delivered[k];
+            (s->slots[r->slot].high ? s->free_high : s->free_low).push_back(r->slot);
+            done_ids[nd++] = r->id;
+            delete r;
+        }
+        s->delivered.erase(s->delivered.begin(), s->delivered.begin() + (long)k);
+    }
+    // device completions: the device region is free; the rows go to a delivery worker (the slot's
+    // pinned staging stays with the request until they are copied)
+    bool queued = false;
+    for (size_t i = 0; i < s->inflight.size();) {
         Req *r = s->inflight[i];
         const cudaError_t q = cudaEventQuery(s->slots[r->slot].ev);
         if (q == cudaErrorNotReady) {
@@ -415,16 +479,18 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
             continue;
         }
         if (q != cudaSuccess) return fail(std::string("pf_server_poll: ") + cudaGetErrorString(q));
-        deliver(s, r);
         if (!r->small) s->large_sms_inflight -= r->sms;
         s->arena.release(r->off, r->bytes);
         s->in_use -= align256(r->bytes);
-        (s->slots[r->slot].high ? s->free_high : s->free_low).push_back(r->slot);
-        done_ids[nd++] = r->id;
-        delete r;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->to_deliver.push_back(r);
+        }
+        queued = true;
         s->inflight[i] = s->inflight.back();
         s->inflight.pop_back();
     }
+    if (queued) s->cv.notify_all();
     // admissions, oldest first; a large request that would take SMs from the reserve waits, and
     // the large ones behind it wait too (their order is kept), while small ones go past it
     const int large_budget = std::max(1, s->num_sms - s->reserved_sms);
@@ -471,7 +537,11 @@ int pf_server_configure(pf_server *s, int reserved_sms, int large_request_ctas) 
 int pf_server_state(const pf_server *s, int *pending, int *inflight, long long *bytes_in_use) {
     if (!s) return fail("pf_server_state: null argument");
     if (pending) *pending = (int)s->pending.size();
-    if (inflight) *inflight = (int)s->inflight.size();
+    if (inflight) {
+        // on the device, or finished and not yet returned by pf_server_poll
+        std::lock_guard<std::mutex> lk(s->mu);
+        *inflight = (int)(s->inflight.size() + s->to_deliver.size() + s->delivered.size());
+    }
     if (bytes_in_use) *bytes_in_use = (long long)s->in_use;
     return 0;
 }
@@ -479,6 +549,7 @@ int pf_server_state(const pf_server *s, int *pending, int *inflight, long long *
 void pf_server_destroy(pf_server *s) {
     if (!s) return;
     for (Req *r : s->inflight) cudaEventSynchronize(s->slots[r->slot].ev);
+    stop_workers(s);  // lets the workers finish the queued deliveries first
     destroy(s);
 }
 

@@ -38,6 +38,8 @@ struct TileLanes {
     double red[kW][kLanes];
     int ired[kW][kLanes];
     int nactive, nstep, nrefine;
+    int exhausted;  // a lane found the job list empty
+    int handoff;    // the CTA hands its running instances to the one-CTA kernel and stops
 };
 
 // 32-bit offsets: every slab array has fewer than 2^27 rows
@@ -128,6 +130,10 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
     double *Vm = reinterpret_cast<double *>(q);
     q += al256((size_t)n * kLanes * 8);
     double *Va = reinterpret_cast<double *>(q);
+    if (tid == 0) {
+        S.exhausted = 0;
+        S.handoff = 0;
+    }
     if (tid < kLanes) {
         S.state[tid] = tid < A.tile_lanes ? kFree : kIdle;
         S.next[tid] = S.end[tid] = 0;
@@ -140,11 +146,15 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
         // ---- refill: finished lanes take the next instance of their job, or a new job
         if (warp == 0) {
             int st = S.state[lane];
+            int lane_exh = 0;
             if (st == kFree || st == kDone) {
                 st = kIdle;
                 while (S.next[lane] >= S.end[lane]) {
                     const int j = atomicAdd(A.job_counter, 1);
-                    if (j >= A.njobs) break;
+                    if (j >= A.njobs) {
+                        lane_exh = 1;
+                        break;
+                    }
                     S.next[lane] = A.job_first[j];
                     S.end[lane] = A.job_first[j] + A.job_count[j];
                 }
@@ -173,10 +183,37 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
             }
             S.state[lane] = st;
             const unsigned act = __ballot_sync(0xffffffffu, st == kNew || st == kStep);
-            if (lane == 0) S.nactive = __popc(act);
+            const bool exh = __any_sync(0xffffffffu, lane_exh != 0);
+            if (lane == 0) {
+                S.nactive = __popc(act);
+                if (exh) S.exhausted = 1;
+                // stragglers: with the jobs exhausted, a round costs about as much for a few lanes
+                // as for all of them, so the last few instances continue on the one-CTA kernel
+                // (single slack only: there the Newton state is V alone)
+                S.handoff = A.hand_list != nullptr && !P.distributed && S.exhausted && S.nactive > 0 &&
+                            S.nactive <= A.hand_lanes;
+            }
         }
         __syncthreads();
         if (S.nactive == 0) break;
+        if (S.handoff) {
+            // the state of every running lane into its output row: V (the start voltages for a lane
+            // that has not started), the iterations taken so far; the instance joins the list
+            const int st = S.state[lane];
+            const bool run = st == kNew || st == kStep;
+            const int inst = S.inst[lane];
+            if (run) {
+                double2 *vo = out_row(A, inst, n);
+                const double2 *v0 = A.V0 + (long long)inst * A.v0_stride;
+                for (int r = warp; r < n; r += kW) vo[r] = st == kNew ? v0[r] : V[ix(r, lane)];
+            }
+            if (warp == 0 && run) {
+                A.iters[inst] = S.it[lane];
+                A.errs[inst] = 0;
+                A.hand_list[atomicAdd(A.hand_count, 1)] = inst;
+            }
+            break;
+        }
         const bool fresh = S.state[lane] == kNew;
         const int inst = S.inst[lane];
         const double2 *Sb = A.Sbus + (long long)inst * A.sbus_stride;
@@ -420,6 +457,8 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
             if (warp == 0) {
                 A.iters[inst] = S.it[lane];
                 A.errs[inst] = S.err[lane];
+                // mixed form: an instance that failed in FP32 is solved again in FP64 afterwards
+                if (A.fb_list != nullptr && S.err[lane] != 0) A.fb_list[atomicAdd(A.fb_count, 1)] = inst;
             }
         }
         __syncthreads();

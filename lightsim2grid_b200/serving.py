@@ -254,6 +254,20 @@ class ServeRun:
         self.done, self.rejected = [], []
         self.peak_inflight = 0
         self.peak_bytes = 0
+        self.poll_s = []     # duration of each pf_server_poll call (admissions, launches, deliveries)
+        self.submit_s = []   # duration of each batch of submissions
+
+    def host_stats(self):
+        """p50/p99/max of the host loop's poll and submit calls (ms), and the time spent in
+        calls longer than 1 ms."""
+        out = {}
+        for k, v in (("poll_ms", self.poll_s), ("submit_ms", self.submit_s)):
+            a = np.asarray(v) * 1e3
+            if a.size:
+                out[k] = {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)),
+                          "max": float(a.max()), "calls": int(a.size), "over_1ms": int((a > 1.0).sum()),
+                          "ms_in_calls_over_1ms": float(a[a > 1.0].sum())}
+        return out
 
 
 class PowerFlowServer:
@@ -276,6 +290,7 @@ class PowerFlowServer:
         i, total = 0, len(reqs)
         while len(run.done) + len(run.rejected) < total:
             t = now()
+            i0 = i
             while i < total and (not realtime or reqs[i].arrival <= t):
                 r = reqs[i]
                 if not realtime:
@@ -284,7 +299,11 @@ class PowerFlowServer:
                     r.t_done = now()
                     run.rejected.append(r)
                 i += 1
+            t1 = now()
+            if i > i0:
+                run.submit_s.append(t1 - t)
             fin = self.native.poll()
+            run.poll_s.append(now() - t1)
             if fin:
                 td = now()
                 for r in fin:

@@ -91,7 +91,7 @@ def test_autotuner_picks_a_schedule_with_unchanged_results():
 
     g = synthetic.make_named_grid("grid1354")[0]
     branches = np.arange(0, 1991, 31)
-    cands = [{"ordering": 0, "threads": 256}, {"ordering": 0, "level_slack": 4, "placement": 1, "threads": 256},
+    cands = [{"ordering": 0, "threads": 256}, {"ordering": 0, "level_slack": 4, "placement": 2, "threads": 256},
              {"ordering": 3, "threads": 512}]
     best, table = autotune.tune_n1(g, branches, precision=1, candidates=cands, repeat=2)
     assert best in cands

@@ -139,3 +139,70 @@ def test_tile_device_batch_with_multi_instance_jobs():
     assert np.array_equal(e1, e2) and np.array_equal(i1, i2)
     ok = e1 == 0
     assert max(_vdiff(V1[k], V2[k]) for k in np.nonzero(ok)[0]) <= TOL_FP64
+
+
+def _threads():
+    import os
+
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except Exception:
+        return 1
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_tile_headline_batch_with_hand_off_matches_oracle(precision):
+    """Every outage of the 2,848-bus grid through the batch-interleaved layout: the CTAs hand their
+    last running instances to the one-CTA kernel (continued from their state) and, in the mixed
+    form, the 11 instances that fail in FP32 are solved again in FP64 -- all in one stream, and
+    the results are the oracle's (FP64: flags, error codes and iteration counts)."""
+    from lightsim2grid_b200 import Plan
+    from oracle.oracle import ContingencyBatch
+
+    c = grid_problem("grid2848")
+    g = c["grid"]
+    Vn = _base(c)
+    coeffs = [g.branch_coeffs([b]) for b in range(g.nb_powerline())]
+    ob = ContingencyBatch(c["Ybus"], c["Sbus"], Vn, c["ref"], c["weights"], c["pv"], c["pq"], coeffs)
+    ok, Vo, conv_o, it_o, err_o, _ = ob.run(_threads())
+    plan = Plan(c["Ybus"], Vn, c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=precision,
+                batch_layout=2)
+    V, conv, iters, errs = plan.batch_n1(coeffs, Vn, c["Sbus"], 10, 1e-8)
+    isl = err_o == 8
+    assert np.array_equal(errs == 1, isl)
+    assert np.array_equal(conv, conv_o)
+    assert np.array_equal(errs[~isl], err_o[~isl])
+    failed = ~isl & ~conv_o
+    if precision == 0:
+        assert np.array_equal(iters[~isl], it_o[~isl])
+    else:
+        assert plan.timers()[5] >= failed.sum()
+        assert np.array_equal(iters[failed], it_o[failed])
+    tol = TOL_FP64 if precision == 0 else TOL_MIXED
+    assert max(_vdiff(V[k], Vo[k]) for k in np.nonzero(conv)[0]) <= tol
+    assert np.all(V[~conv] == 0)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_auto_layout_on_the_largest_grid_matches_oracle(precision):
+    """The 6,515-bus plans keep their LU in global memory; with enough jobs per SM the default
+    layout is the batch-interleaved one.  1,200 outages against the oracle."""
+    from lightsim2grid_b200 import Plan
+    from oracle.oracle import ContingencyBatch
+
+    c = grid_problem("grid6515")
+    g = c["grid"]
+    Vn = _base(c)
+    coeffs = [g.branch_coeffs([b]) for b in range(1200)]
+    ob = ContingencyBatch(c["Ybus"], c["Sbus"], Vn, c["ref"], c["weights"], c["pv"], c["pq"], coeffs)
+    ok, Vo, conv_o, it_o, err_o, _ = ob.run(_threads())
+    plan = Plan(c["Ybus"], Vn, c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=precision)
+    assert plan.info()["lu_in_shared"] == 0 and plan.info()["nnz_lu"] >= 80000
+    V, conv, iters, errs = plan.batch_n1(coeffs, Vn, c["Sbus"], 10, 1e-8)
+    isl = err_o == 8
+    assert np.array_equal(errs == 1, isl)
+    assert np.array_equal(conv, conv_o)
+    if precision == 0:
+        assert np.array_equal(iters[~isl], it_o[~isl])
+    tol = TOL_FP64 if precision == 0 else TOL_MIXED
+    assert max(_vdiff(V[k], Vo[k]) for k in np.nonzero(conv)[0]) <= tol

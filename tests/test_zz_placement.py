@@ -1,4 +1,4 @@
-"""The two placements of the packed phase programs (pf_options.placement 0 and 1) on the device:
+"""The two placements of the packed phase programs (pf_options.placement 1, the default, and 2):
 within a phase every written value has one thread and its operations keep their order, so an N-1
 batch gives the same bits with either (voltages, iterations, error codes).  Mixed form on the
 1354-bus grid and FP64 on the 118-bus grid, whose LUs sit in shared memory."""
@@ -23,7 +23,7 @@ def test_placements_give_the_same_bits(name, precision, ncases):
     nb = g.nb_powerline() if ncases is None else ncases
     coeffs = [g.branch_coeffs([b]) for b in range(nb)]
     out = []
-    for placement in (0, 1):
+    for placement in (1, 2):
         plan = Plan(c["Ybus"], Vn, c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], precision=precision,
                     placement=placement)
         assert plan.info()["lu_in_shared"] == 1
