@@ -484,10 +484,15 @@ def _serve(seconds, rate, device, reserved_sms=None, large_request_ctas=0):
     per = {}
     for g in SERVE_GRIDS:
         for kind in ("pf", "n1"):
-            lat = np.array([r.latency for r in done if r.grid == g and r.kind == kind])
+            rs = [r for r in done if r.grid == g and r.kind == kind]
+            lat = np.array([r.latency for r in rs])
             if lat.size:
+                # host lag: arrival to the submission by the serving loop
+                lag = np.array([r.t_admit - r.arrival for r in rs if r.t_admit is not None])
                 per["{}/{}".format(g, kind)] = {"p50_ms": float(np.percentile(lat, 50) * 1e3),
-                                                "p99_ms": float(np.percentile(lat, 99) * 1e3), "count": int(lat.size)}
+                                                "p99_ms": float(np.percentile(lat, 99) * 1e3), "count": int(lat.size),
+                                                "submit_lag_p99_ms": float(np.percentile(lag, 99) * 1e3) if lag.size
+                                                else None}
     st.update({"duration_s": seconds, "arrival_rate": rate, "grids": list(SERVE_GRIDS), "per_class": per,
                "reserved_sms": reserved_sms, "large_request_ctas": large_request_ctas,
                "slots": slots, "hbm_budget_bytes": budget, "peak_inflight": srv.last.peak_inflight,
@@ -778,6 +783,7 @@ def run_case(argv):
     ap.add_argument("--ordering", type=int, default=0)
     ap.add_argument("--placement", type=int, default=0)
     ap.add_argument("--level-slack", type=int, default=0)
+    ap.add_argument("--handoff-lanes", type=int, default=0)
     ap.add_argument("--no-trace", action="store_true", help="skip the phase-cycle and trace launches")
     args = ap.parse_args(argv)
 
@@ -796,7 +802,8 @@ def run_case(argv):
     dev = torch.device("cuda:0")
     opts = dict(threads=args.threads, lu_placement=args.lu_placement, max_ctas_per_sm=args.ctas_per_sm,
                 refine=args.refine, lu_reuse_threshold=args.lu_reuse, batch_layout=args.batch_layout,
-                ordering=args.ordering, placement=args.placement, level_slack=args.level_slack)
+                ordering=args.ordering, placement=args.placement, level_slack=args.level_slack,
+                handoff_lanes=args.handoff_lanes)
     if args.dc or args.fdpf >= 0:
         # DC / FDPF: the grid's DC Ybus and outage coefficients, or its B' / B''
         gd = _DCView(g) if args.dc else g

@@ -41,8 +41,9 @@ typedef struct pf_options {
                                to 5e-8 pu from the FP64 ones instead of 3e-10               */
     int batch_layout;       /* Newton batches of independent instances (no time-series chain):
                                0 auto: batch-interleaved for plans whose LU stays in global
-                               memory with at least 80,000 entries (6,515 buses) and 4 jobs per
-                               SM or more, else one CTA per instance; 1 one CTA per instance; 2
+                               memory with at least 40,000 entries (2,848 buses FP64, 6,515 buses)
+                               and 4 jobs per SM or more, else one CTA per instance; 1 one CTA
+                               per instance; 2
                                batch-interleaved: 32 instances per CTA, one per lane, every value
                                stored as 32 consecutive per-instance values (coalesced, the batch
                                dimension amortises each phase), the last running instances of a
@@ -65,6 +66,10 @@ typedef struct pf_options {
                                degree up to the minimum + level_slack, the one of lowest
                                elimination level.  0: default (2); < 0: no level preference;
                                larger values give shallower plans for some more fill          */
+    int handoff_lanes;      /* batch-interleaved layout: once the jobs are exhausted, a CTA hands
+                               its running instances to the one-CTA kernel when at most this many
+                               of its lanes still run.  0: default (all its lanes when no lane
+                               takes a second job, else half); < 0: never                      */
 } pf_options;
 
 /* DC power flow plan (BaseDCAlgo::compute_pf, src/powerflow_algorithm/BaseDCAlgo.tpp:5-175;
@@ -360,7 +365,8 @@ int pf_server_submit(pf_server *server, long long id, int grid, int kind, const 
                      const int *branches, double *V_out, int *iters_out, int *errs_out);
 int pf_server_poll(pf_server *server, long long *done_ids, int cap);
 /* SM reservation of a server (no counterpart in the reference).  A request is small when its
-   instances x buses are at most 20,000; a large request is admitted only while the SMs taken by
+   instances x buses are at most 20,000 on a grid of at most 2,000 buses (an instance of a larger
+   grid holds its SM for a millisecond or more); a large request is admitted only while the SMs taken by
    the CTAs of the large requests in flight stay within (SMs - reserved_sms), so the reserved SMs
    stay free for small requests (stream priorities alone cannot move a resident CTA); its launch
    uses at most large_request_ctas CTAs (0: no cap), each solving several of its instances in

@@ -22,7 +22,7 @@ class PfOptions(ctypes.Structure):
                 ("fp64_fallback", ctypes.c_int), ("max_ctas_per_sm", ctypes.c_int), ("refine", ctypes.c_int),
                 ("refine_threshold", ctypes.c_double), ("lu_reuse_threshold", ctypes.c_double),
                 ("batch_layout", ctypes.c_int), ("ordering", ctypes.c_int), ("placement", ctypes.c_int),
-                ("level_slack", ctypes.c_int)]
+                ("level_slack", ctypes.c_int), ("handoff_lanes", ctypes.c_int)]
 
 
 class PfPlanInfo(ctypes.Structure):

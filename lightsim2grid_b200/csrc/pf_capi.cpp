@@ -542,11 +542,12 @@ void release(pf_plan *pl) {
 // The number of CTAs is bounded by the slabs that fit in the scratch.
 // Whether a launch runs the batch-interleaved kernel: Newton plans, independent instances (no
 // chain), no per-launch diagnostics (J output, phase cycles or trace, LU reuse), and option
-// batch_layout 2, or auto (0) for plans whose LU stays in global memory and is large (at least
-// kAutoTileLU entries) with several jobs per SM: measured on the 6,515-bus N-1 batch, 87.7 against
-// 105 ms (mixed) and 88.7 against 140 ms (FP64); where the LU sits in shared memory (up to 2,848
-// buses mixed) one CTA per instance is faster.
-constexpr int kAutoTileLU = 80000;
+// batch_layout 2, or auto (0) for plans whose LU stays in global memory and has at least
+// kAutoTileLU entries, with several jobs per SM.  Measured on all N-1 outages: 6,515 buses mixed
+// 77.1 against 105.6 ms, FP64 70.4 against 139.8 ms; 2,848 buses FP64 18.4 against 20.7 ms.  Where
+// the LU sits in shared memory (up to 2,848 buses mixed, 1,354 buses FP64) one CTA per instance
+// is faster (2,848 mixed: 11.2 against 20.8 ms).
+constexpr int kAutoTileLU = 40000;
 
 bool use_tile(const pf_plan *pl, const l2g::BatchArgs &a) {
     if (pl->P.dc || pl->P.fdpf || a.chain || a.Jout || a.phase_cycles || a.trace || a.reuse_below > 0) return false;
@@ -585,9 +586,15 @@ int launch_tile(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, i
     a.job_counter = counter;
     // spread the jobs over all CTAs: lanes per CTA
     a.tile_lanes = std::max(1, std::min(32, (a.njobs + grid - 1) / grid));
-    a.hand_list = hand;
+    // hand-off point: with at most one job per lane (no refill) as soon as the jobs are exhausted,
+    // i.e. after the first instance of the CTA finishes (2,848 buses, 21 lanes: FP64 20.8 -> 18.4
+    // ms); with refills once half the lanes are idle (6,515 buses, 32 lanes: 77.1 ms mixed against
+    // 78.6 when handing off at 24 lanes and 89.9 at 4)
+    const int ho = pl->opt.handoff_lanes;
+    a.hand_list = ho < 0 ? nullptr : hand;
     a.hand_count = counter + 2;
-    a.hand_lanes = std::max(1, a.tile_lanes / 2);
+    const bool refills = (long long)a.njobs > (long long)grid * a.tile_lanes;
+    a.hand_lanes = ho > 0 ? ho : (refills ? std::max(1, a.tile_lanes / 2) : a.tile_lanes);
     const bool fallback = precision == 1 && pl->precision == 1 && pl->opt.fp64_fallback != 2 && a.refine;
     a.fb_list = fallback ? fbl : nullptr;
     a.fb_count = counter + 3;

@@ -100,6 +100,10 @@ struct Slot {
 // scheduler then dispatches their CTAs before the pending CTAs of large batches launched
 // earlier, so a small request does not wait behind them.
 constexpr long long kSmallWork = 20000;
+// ... and whose grid has at most this many buses: one instance of a larger grid keeps its SM for a
+// millisecond or more (the whole shared memory of the 2,848-bus mixed plan), so it counts as large
+// for the SM reservation below even alone
+constexpr int kHeavyBuses = 2000;
 
 // Priorities reorder pending CTAs only: a CTA of a large batch that is already resident keeps its
 // SM until its instance is solved (milliseconds on the largest grids).  So large requests are
@@ -117,7 +121,7 @@ struct Req {
     int *iters = nullptr, *errs = nullptr;
     size_t scratch = 0, outs = 0, ins = 0, bytes = 0, off = 0;
     int slot = -1;
-    bool small = true;   // instance-buses <= kSmallWork
+    bool small = true;   // instance-buses <= kSmallWork on a grid of at most kHeavyBuses buses
     int ctas = 0;        // CTAs of its launch
     int sms = 0;         // SMs those CTAs occupy (large requests)
 };
@@ -226,7 +230,7 @@ int prepare(pf_server *s, Req *r) {
     }
     if (r->ninst > s->max_k) return fail("pf_server_submit: request has more instances than the server's maximum");
     if (r->ins > s->in_cap) return fail("pf_server_submit: request inputs exceed the staging buffers");
-    r->small = (long long)r->ninst * g.n <= kSmallWork;
+    r->small = (long long)r->ninst * g.n <= kSmallWork && g.n <= kHeavyBuses;
     int ctas = std::max(1, std::min(r->ninst, g.ctas));
     if (!r->small) ctas = std::max(1, std::min(ctas, s->large_ctas));
     r->ctas = ctas;
@@ -514,7 +518,7 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
         r->off = off;
         s->in_use += align256(r->bytes);
         // small requests prefer high-priority streams, large ones low-priority ones
-        const bool small = (long long)r->ninst * s->grids[r->grid].n <= kSmallWork;
+        const bool small = r->small;
         std::vector<int> &pref = small ? s->free_high : s->free_low;
         std::vector<int> &other = small ? s->free_low : s->free_high;
         std::vector<int> &pool = pref.empty() ? other : pref;

@@ -295,6 +295,7 @@ class PowerFlowServer:
                 r = reqs[i]
                 if not realtime:
                     r.arrival = t
+                r.t_admit = t  # handed to the serving core (queued there until admitted)
                 if not self.native.submit(r):
                     r.t_done = now()
                     run.rejected.append(r)

@@ -113,7 +113,7 @@ class Plan:
     def __init__(self, Ybus, V0, Sbus, slack_ids, slack_weights, pv, pq, distributed=False, precision=0,
                  threads=0, lu_placement=0, fuse_forward=0, fp64_fallback=0, max_ctas_per_sm=0, refine=0,
                  refine_threshold=0.0, lu_reuse_threshold=0.0, dc=False, fdpf=None, batch_layout=0, ordering=0,
-                 placement=0, level_slack=0):
+                 placement=0, level_slack=0, handoff_lanes=0):
         self._lib = nat.load()
         Y = canonical_csc(Ybus)
         n = Y.shape[0]
@@ -139,7 +139,8 @@ class Plan:
                             fp64_fallback=int(fp64_fallback), max_ctas_per_sm=int(max_ctas_per_sm),
                             refine=int(refine), refine_threshold=float(refine_threshold),
                             lu_reuse_threshold=float(lu_reuse_threshold), batch_layout=int(batch_layout),
-                            ordering=int(ordering), placement=int(placement), level_slack=int(level_slack))
+                            ordering=int(ordering), placement=int(placement), level_slack=int(level_slack),
+                            handoff_lanes=int(handoff_lanes))
         h = nat.ctypes.c_void_p()
         self.dc = bool(dc)
         self.fdpf = fdpf is not None
