@@ -629,6 +629,9 @@ def run_ours(args):
         e2e_times.append(time.perf_counter() - t0)
         e2e_conv = int(conv.sum())
     e2e_t = float(np.mean(e2e_times))
+    tm = plan_e2e.timers()  # the last call: total, host preparation, uploads, kernel, downloads, FP64 re-solves
+    e2e_breakdown = {"total_ms": 1e3 * tm[0], "host_prep_ms": 1e3 * tm[1], "h2d_ms": 1e3 * tm[2],
+                     "kernel_ms": 1e3 * tm[3], "d2h_ms": 1e3 * tm[4], "fp64_resolves": int(tm[5])}
     if ws > 1:
         tt = torch.tensor([e2e_t], dtype=torch.float64, device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -722,7 +725,8 @@ def run_ours(args):
             "e2e": {"value": ws * e2e_conv / e2e_t, "unit": "PF/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_t,
                     "path": "Plan.batch_n1_arrays -> pf_batch_n1 (host buffers; islanding check, uploads, kernel, "
-                            "download of all voltages into pinned host arrays)"},
+                            "download of all voltages into pinned host arrays)",
+                    "breakdown": e2e_breakdown},
             "error_vs_oracle": err_vs_oracle,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,

@@ -338,7 +338,8 @@ int pf_assemble_sbus_device(const pf_sbus_layout *lay, int nsteps, const double 
    base-case voltages and injections (host arrays, copied to the device once), its branch-removal
    coefficients as CSR over branches (as for pf_batch_n1) and its Newton settings.  Device memory
    is one arena of hbm_budget bytes allocated at creation; each admitted request gets one region
-   of it (inputs, outputs, kernel working memory) and one of `slots` streams with pinned staging.
+   of it (inputs, kernel working memory) and one of `slots` streams with pinned staging, mapped
+   into the device address space: the kernel writes the results there directly.
    pf_server_submit queues a request: kind 0 = one power flow with the base injections scaled
    bus by bus by scale[n]; kind 1 = the outages of `nbranches` branches from the base-case state.
    V_out (rows x n complex, rows = 1 or nbranches), iters_out and errs_out (rows) receive the

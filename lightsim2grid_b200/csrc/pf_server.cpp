@@ -93,6 +93,7 @@ struct Slot {
     cudaStream_t st = nullptr;
     cudaEvent_t ev = nullptr;
     unsigned char *pin_in = nullptr, *pin_out = nullptr;
+    unsigned char *pin_out_dev = nullptr;  // device address of pin_out
     bool high = false;  // on a high-priority stream
 };
 
@@ -236,7 +237,7 @@ int prepare(pf_server *s, Req *r) {
     r->ctas = ctas;
     r->sms = (ctas + g.ctas_per_sm - 1) / g.ctas_per_sm;
     r->scratch = r->ninst ? align256((size_t)pf_scratch_bytes(g.plan, ctas)) : 0;
-    r->outs = align256((size_t)r->ninst * g.n * 16 + 8 * (size_t)r->ninst);
+    r->outs = 0;  // the kernel writes the results straight into the slot's mapped pinned staging
     r->bytes = r->scratch + r->outs + r->ins;
     return 0;
 }
@@ -245,7 +246,10 @@ int launch(pf_server *s, Req *r) {
     Grid &g = s->grids[r->grid];
     Slot &sl = s->slots[r->slot];
     unsigned char *base = s->arena_ptr + r->off;
-    unsigned char *scr = base, *out = base + r->scratch, *in = out + r->outs;
+    unsigned char *scr = base, *in = base + r->scratch + r->outs;
+    // outputs: the slot's pinned staging, mapped into the device address space (the kernel writes
+    // each instance's row there as it finishes: no copy engine in the way of other requests)
+    unsigned char *out = sl.pin_out_dev;
     cudaError_t e = cudaSuccess;
     if (r->ninst > 0) {
         pf_device_batch b{};
@@ -278,9 +282,6 @@ int launch(pf_server *s, Req *r) {
         if (e != cudaSuccess) return fail(std::string("pf_server: upload: ") + cudaGetErrorString(e));
         const int rc = pf_batch_device_scratch(g.plan, &b, scr, (long long)r->scratch, sl.st);
         if (rc != 0) return rc;
-        e = cudaMemcpyAsync(sl.pin_out, out, (size_t)r->ninst * g.n * 16 + 8 * (size_t)r->ninst,
-                            cudaMemcpyDeviceToHost, sl.st);
-        if (e != cudaSuccess) return fail(std::string("pf_server: download: ") + cudaGetErrorString(e));
     }
     e = cudaEventRecord(sl.ev, sl.st);
     if (e != cudaSuccess) return fail(std::string("pf_server: event: ") + cudaGetErrorString(e));
@@ -401,7 +402,9 @@ int pf_server_create(const pf_server_grid *grids, int ngrids, long long hbm_budg
                 cudaSuccess ||
             (e = cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaHostAlloc(reinterpret_cast<void **>(&sl.pin_in), s->in_cap, cudaHostAllocDefault)) != cudaSuccess ||
-            (e = cudaHostAlloc(reinterpret_cast<void **>(&sl.pin_out), s->out_cap, cudaHostAllocDefault)) !=
+            (e = cudaHostAlloc(reinterpret_cast<void **>(&sl.pin_out), s->out_cap, cudaHostAllocMapped)) !=
+                cudaSuccess ||
+            (e = cudaHostGetDevicePointer(reinterpret_cast<void **>(&sl.pin_out_dev), sl.pin_out, 0)) !=
                 cudaSuccess) {
             destroy(s);
             return fail(std::string("pf_server_create: slots: ") + cudaGetErrorString(e));
