@@ -463,7 +463,7 @@ def _config3(dev, stream, flush, K, W, threads, total=4096, seed=4096):
 SERVE_GRIDS = ("grid14", "grid118", "grid300", "grid1354", "grid2848", "grid6515")
 
 
-def _serve(seconds, rate, device, reserved_sms=None, large_request_ctas=0):
+def _serve(seconds, rate, device, reserved_sms=None, large_request_ctas=0, device_loop=False, loop_ctas=(0, 0)):
     """Serving leg: Poisson arrivals at `rate` requests/s for `seconds` over the six synthetic
     grids (14 to 6,515 buses); half the requests are one power flow with injections scaled by
     U[0.9, 1.1] per bus, half an N-1 batch of 8 to 64 outages; mixed precision, tol 1e-8.
@@ -475,6 +475,8 @@ def _serve(seconds, rate, device, reserved_sms=None, large_request_ctas=0):
     budget, slots = 4 << 30, 32
     srv = PowerFlowServer(grids, device=device, hbm_budget=budget, slots=slots, precision=1, max_iter=MAX_ITER,
                           tol=TOL, reserved_sms=reserved_sms, large_request_ctas=large_request_ctas)
+    if device_loop:
+        srv.native.set_device_loop(True, *loop_ctas)
     nb = {k: v.n_bus for k, v in grids.items()}
     nbr = {k: v.nb_powerline() for k, v in grids.items()}
     srv.serve(make_requests(nb, rate=rate, duration=min(1.0, seconds), seed=12345, branches_of=nbr))  # warm-up
@@ -495,6 +497,8 @@ def _serve(seconds, rate, device, reserved_sms=None, large_request_ctas=0):
                                                 else None}
     st.update({"duration_s": seconds, "arrival_rate": rate, "grids": list(SERVE_GRIDS), "per_class": per,
                "reserved_sms": reserved_sms, "large_request_ctas": large_request_ctas,
+               "mode": "device-resident request loop" if device_loop else "one launch per request",
+               "loop_ctas": list(loop_ctas) if device_loop else None,
                "slots": slots, "hbm_budget_bytes": budget, "peak_inflight": srv.last.peak_inflight,
                "peak_bytes": srv.last.peak_bytes, "rejected": len(srv.last.rejected),
                "latency": "arrival to result in the caller's host arrays (host clock)",
@@ -654,7 +658,7 @@ def run_ours(args):
 
     serve = None
     if ws == 1 and args.serve_seconds > 0:
-        serve = _serve(args.serve_seconds, args.serve_rate, dev)
+        serve = _serve(args.serve_seconds, args.serve_rate, dev, device_loop=not args.serve_launches)
 
     cpu, err_vs_oracle = None, None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -888,12 +892,15 @@ def run_serve(argv):
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--reserve", type=int, default=-1, help="SMs reserved for small requests (-1: default)")
     ap.add_argument("--large-ctas", type=int, default=0, help="CTAs per large request (0: no cap)")
+    ap.add_argument("--loop", action="store_true", help="device-resident request loop")
+    ap.add_argument("--loop-ctas", default="0,0", help="CTAs of the shared-memory and global-LU loops (0: default)")
     args = ap.parse_args(argv)
     import torch
 
     dev = torch.device("cuda:0")
     torch.cuda.set_device(dev)
-    out = _serve(args.seconds, args.rate, dev, None if args.reserve < 0 else args.reserve, args.large_ctas)
+    out = _serve(args.seconds, args.rate, dev, None if args.reserve < 0 else args.reserve, args.large_ctas,
+                 args.loop, tuple(int(x) for x in args.loop_ctas.split(",")))
     print(json.dumps(out))
     return 0
 
@@ -912,6 +919,9 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the config 1-3 legs")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving leg duration (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving leg arrival rate (requests/s)")
+    ap.add_argument("--serve-launches", action="store_true",
+                    help="serving leg with one launch per request (default: the device-resident loop for the small "
+                         "requests)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -373,6 +373,20 @@ int pf_server_poll(pf_server *server, long long *done_ids, int cap);
    uses at most large_request_ctas CTAs (0: no cap), each solving several of its instances in
    turn.  Defaults: an eighth of the SMs reserved, no cap.  Takes effect for later admissions. */
 int pf_server_configure(pf_server *server, int reserved_sms, int large_request_ctas);
+/* Device-resident request loop (no counterpart in the reference).  enable = 1: instead of one
+   launch per request, the small requests (see pf_server_configure) of each class of grids of at
+   most 2,000 buses (plans with the LU in shared memory; the others) are served by a persistent
+   launch of the Newton kernel that takes jobs from a ring in device memory (the large requests keep
+   their own launches, which spread over the SMs the loops leave free):
+   an admitted request's inputs, segment (plan and batch) and jobs are copied to the device on a
+   feeder stream, then the ring's tail; the loop's CTAs claim the jobs as they appear, write the
+   results into the slot's mapped pinned staging and count the finished instances per slot in
+   mapped host memory, which pf_server_poll reads.  A CTA leaves after a few milliseconds without
+   work (every wait in the kernel is bounded); the loop is launched again when work is published
+   while it is not running.  ctas_shared / ctas_global: CTAs of each class's loop (0: a quarter of
+   the SMs' worth, an eighth each when both classes exist).  Switch modes only while no request is
+   queued or running.  Results are those of the launch-per-request mode, bit for bit. */
+int pf_server_device_loop(pf_server *server, int enable, int ctas_shared, int ctas_global);
 int pf_server_state(const pf_server *server, int *pending, int *inflight, long long *bytes_in_use);
 void pf_server_destroy(pf_server *server);
 

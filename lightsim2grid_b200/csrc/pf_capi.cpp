@@ -907,6 +907,66 @@ size_t plan_slab_bytes(const pf_plan *pl) { return pl ? pl->slab : 0; }
 
 size_t plan_fallback_slab_bytes(const pf_plan *pl) { return pl ? (pl->inline_fb ? pl->slab_fb : pl->slab) : 0; }
 
+int loop_shape(pf_plan *const *plans, int n, LoopShape *sh) {
+    if (!plans || n <= 0 || !sh) return fail(-1, "request loop: invalid argument");
+    LoopShape r;
+    r.inline_fb = true;
+    for (int i = 0; i < n; ++i) {
+        const pf_plan *pl = plans[i];
+        if (!pl) return fail(-1, "request loop: null plan");
+        if (pl->P.dc || pl->P.fdpf) return fail(-1, "request loop: Newton plans only");
+        if (i == 0) {
+            r.device = pl->device;
+            r.precision = pl->precision;
+            r.refine = pl->refine;
+            r.lu_in_smem = pl->lu_in_smem;
+            r.num_sms = pl->num_sms;
+        } else if (pl->device != r.device || pl->precision != r.precision || pl->refine != r.refine ||
+                   pl->lu_in_smem != r.lu_in_smem) {
+            return fail(-1, "request loop: plans differ in device, precision, refinement or LU placement");
+        }
+        r.inline_fb = r.inline_fb && pl->inline_fb;
+        r.threads = std::max(r.threads, pl->threads);
+    }
+    for (int i = 0; i < n; ++i) {
+        const pf_plan *pl = plans[i];
+        r.smem = std::max(r.smem, r.inline_fb ? pl->smem_fb : pl->smem);
+        r.slab = std::max(r.slab, r.inline_fb ? pl->slab_fb : pl->slab);
+    }
+    r.ctas_per_sm = l2g::nr_occupancy(r.precision, r.lu_in_smem, r.refine, r.threads, r.smem);
+    if (r.ctas_per_sm <= 0) return fail(-1, "request loop: the plans' largest layout cannot be launched");
+    *sh = r;
+    return 0;
+}
+
+int loop_segment(pf_plan *pl, const pf_device_batch *b, const LoopShape &sh, unsigned char *scratch, Segment *seg) {
+    if (!pl || !b || !seg || !scratch) return fail(-1, "request loop: invalid argument");
+    Segment &sg = *seg;
+    sg.P = pl->dp;
+    sg.A = device_args(b);
+    sg.A.scratch = scratch;
+    sg.A.slab_bytes = (long long)sh.slab;
+    sg.A.job_counter = nullptr;  // jobs come from the queue
+    sg.A.lu_in_smem = sh.lu_in_smem ? 1 : 0;
+    sg.A.refine = sh.refine ? 1 : 0;
+    sg.A.refine_below = pl->opt.refine_threshold > 0 ? pl->opt.refine_threshold : 1e-3;
+    sg.A.reuse_below = lu_reuse_below(pl, sg.A.refine_below);
+    sg.A.fp64_inline = (sh.inline_fb && sh.refine && sh.precision == 1) ? 1 : 0;
+    return 0;
+}
+
+int loop_launch(const LoopShape &sh, const Segment &seg0, const DevQueue &q, int grid, void *stream) {
+    MultiArgs M{};
+    M.q = q;
+    l2g::BatchArgs a0 = seg0.A;
+    a0.phase_cycles = nullptr;
+    a0.trace = nullptr;
+    cudaError_t e = l2g::launch_nr_batch(seg0.P, a0, sh.precision, sh.threads, grid, sh.smem,
+                                         static_cast<cudaStream_t>(stream), M);
+    if (e != cudaSuccess) return cuda_fail(e, "request loop: kernel");
+    return 0;
+}
+
 int plan_device(const pf_plan *pl) { return pl ? pl->device : -1; }
 
 void set_last_error(const std::string &msg) { g_err = msg; }

@@ -30,6 +30,22 @@ size_t plan_fallback_slab_bytes(const pf_plan *pl);
 // Device the plan was created on (-1 for a null plan).
 int plan_device(const pf_plan *pl);
 
+// Device-resident request loop over several plans (the serving core's device loop): the shape of
+// one persistent launch of the Newton kernel in queue mode.  The plans must share device,
+// precision, refinement and LU placement; the shape takes the largest thread count, shared memory
+// and slab, with room for the in-launch FP64 fallback when every plan has it.
+struct LoopShape {
+    int device = 0, precision = 0, threads = 0, num_sms = 0, ctas_per_sm = 0;
+    bool lu_in_smem = false, refine = false, inline_fb = false;
+    size_t smem = 0, slab = 0;
+};
+int loop_shape(pf_plan *const *plans, int n, LoopShape *sh);
+// The segment of one request (its plan and device batch) for a loop whose per-CTA slabs start at
+// `scratch`.
+int loop_segment(pf_plan *pl, const pf_device_batch *b, const LoopShape &sh, unsigned char *scratch, Segment *seg);
+// One persistent launch of `grid` CTAs taking jobs from q (asynchronous on `stream`).
+int loop_launch(const LoopShape &sh, const Segment &seg0, const DevQueue &q, int grid, void *stream);
+
 // Sets the message returned by pf_last_error on this thread.
 void set_last_error(const std::string &msg);
 

@@ -40,6 +40,48 @@ struct Shared {
     double slack_absorbed;
 };
 
+// load with acquire semantics at GPU scope: the job ring entries and segments written before the
+// tail (by the host's copies, in stream order) are seen after it
+__device__ __forceinline__ int ld_acquire_gpu(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Request loop: claims the next published job of the ring (compare-and-swap on the head, so a
+// CTA never holds a job that is not there yet) into *job and returns its index, or -1 when the
+// launch is closing and the ring is empty.  After idle_polls polls of an empty ring the CTA closes
+// the launch (every CTA then leaves at its next empty poll), so the wait is bounded.  A function of
+// its own: its registers do not add to the solver's.
+__device__ __noinline__ int claim_queue_job(const QueueJob *jobs, int cap, int *head, const int *tail, int *closing,
+                                            int idle_polls, QueueJob *job) {
+    for (int polls = 0;;) {
+        const int t = ld_acquire_gpu(tail);
+        const int h = *reinterpret_cast<volatile int *>(head);
+        if (h < t) {
+            if (atomicCAS(head, h, h + 1) == h) {
+                const QueueJob *e = jobs + (h % cap);
+                *job = QueueJob{__ldcg(&e->slot), __ldcg(&e->first), __ldcg(&e->count), __ldcg(&e->req)};
+                return h;
+            }
+            continue;  // another CTA took it: look again
+        }
+        if (*reinterpret_cast<volatile int *>(closing)) return -1;
+        if (++polls > idle_polls) {
+            atomicExch(closing, 1);
+            return -1;
+        }
+        __nanosleep(500);
+    }
+}
+
+// Request loop: the job's rows, iterations and errors (mapped host memory) are made visible before
+// its instances are added to the slot's completion count.
+__device__ __noinline__ void signal_queue_job(int *done, int slot, int count) {
+    __threadfence_system();
+    atomicAdd_system(done + slot, count);
+}
+
 // block-wide max of |F| and "any non-finite" flag; every thread receives the result
 __device__ __forceinline__ void block_norm(Shared &S, double lmax, int lbad, double &norm, int &bad) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -131,7 +173,7 @@ __device__ void mismatch(const DevPlan &P, Shared &S, const double2 *__restrict_
         const double2 s = ybus_row_product(P, S, V, r);
         Ibus[r] = s;
         const double2 vr = V[r];
-        const double2 sb = Sbus[r];
+        const double2 sb = __ldcg(Sbus + r);
         double mr = vr.x * s.x + vr.y * s.y - sb.x;  // V * conj(I) - S
         const double mi = vr.y * s.x - vr.x * s.y - sb.y;
         if (P.distributed) mr += sa * P.w[r];
@@ -422,7 +464,10 @@ struct Prof {
     }
 };
 
-// One job: instances [first, first + count) of a batch, chained for a time series.
+// One job: instances [first, first + count) of a batch, chained for a time series.  The batch's
+// inputs (start voltages, injections, overrides) are read through L2 only (ld.global.cg): in the
+// device-resident request loop one launch serves many requests whose inputs reuse device
+// addresses, and an SM's L1 could still hold an earlier request's lines.
 template <typename LT, typename XT, bool LU_SMEM, bool REFINE>
 __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, Shared &S, const Layout<LT, XT> &L,
                                           int first, int count, Prof &pr) {
@@ -446,7 +491,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
         if (step == 0 || !A.chain) {
             const double2 *v0 = A.v0_from_out ? out_row(A, inst, n) : A.V0 + (long long)inst * A.v0_stride;
             for (int b = tid; b < n; b += blockDim.x) {
-                const double2 v = v0[b];
+                const double2 v = __ldcg(v0 + b);
                 V[b] = v;
                 if (Vs) Vs[b] = v;
                 Vm[b] = cabs2(v);
@@ -463,8 +508,8 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
         if (tid == 0) {
             int k0 = 0, k1 = 0;
             if (A.ovr_ptr) {
-                k0 = A.ovr_ptr[inst];
-                k1 = A.ovr_ptr[inst + 1];
+                k0 = __ldcg(A.ovr_ptr + inst);
+                k1 = __ldcg(A.ovr_ptr + inst + 1);
             }
             S.novr = k1 - k0 > kMaxOverrides ? -1 : k1 - k0;  // -1: too many to stage
             S.piv_err = 0;
@@ -472,13 +517,13 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
         }
         __syncthreads();
         if (tid < S.novr) {
-            const int k0 = A.ovr_ptr[inst];
-            S.opos[tid] = A.ovr_pos[k0 + tid];
-            S.oval[tid] = A.ovr_val[k0 + tid];
+            const int k0 = __ldcg(A.ovr_ptr + inst);
+            S.opos[tid] = __ldcg(A.ovr_pos + k0 + tid);
+            S.oval[tid] = __ldcg(A.ovr_val + k0 + tid);
         }
         if (P.distributed) {
             double ls = 0.0;
-            for (int b = tid; b < n; b += blockDim.x) ls += Sb[b].x;
+            for (int b = tid; b < n; b += blockDim.x) ls += __ldcg(Sb + b).x;
             const double tot = block_sum(S, ls);
             if (tid == 0) S.slack_absorbed = tot;
         }
@@ -634,7 +679,9 @@ __device__ __noinline__ void fp64_rerun(const DevPlan &P, const BatchArgs &A, Sh
     solve_job<double, double, false, false>(P, A, S, L, first, count, pr);
 }
 
-template <typename LT, typename XT, bool LU_SMEM, bool REFINE>
+// QUEUE: the device-resident request loop (jobs from M.q); a variant of its own so that the
+// other launches keep their registers.
+template <typename LT, typename XT, bool LU_SMEM, bool REFINE, bool QUEUE>
 __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, const BatchArgs A0, const MultiArgs M) {
     extern __shared__ __align__(16) unsigned char dyn[];
     __shared__ Shared S;
@@ -644,26 +691,42 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, cons
     // kinds run the same code, so an instance gives the same bits in either.
     __shared__ __align__(16) Segment seg;
     const int tid = threadIdx.x;
-    const bool multi = M.segs != nullptr;
+    constexpr bool queue = QUEUE;
+    const bool multi = M.segs != nullptr || queue;
     int *const counter = multi ? M.job_counter : A0.job_counter;
     const int njobs = multi ? M.njobs : (A0.njobs_dev ? min(A0.njobs, *A0.njobs_dev) : A0.njobs);
     Prof pr;
     pr.start(A0.phase_cycles != nullptr && tid == 0);
     int cur = -1;
     Layout<LT, XT> L{};
+    __shared__ QueueJob qjob;
     for (;;) {
-        if (tid == 0) S.job = atomicAdd(counter, 1);
-        __syncthreads();
+        if constexpr (QUEUE) {
+            // request loop: claim the next published job (compare-and-swap on the head, so a CTA
+            // never holds a job that is not there yet); after idle_polls empty polls, leave
+            if (tid == 0)
+                S.job = claim_queue_job(M.q.jobs, M.q.cap, M.q.head, M.q.tail, M.q.closing, M.q.idle_polls, &qjob);
+            __syncthreads();
+            const int got = S.job;
+            __syncthreads();
+            if (got < 0) break;
+        } else {
+            if (tid == 0) S.job = atomicAdd(counter, 1);
+            __syncthreads();
+            const int job = S.job;
+            __syncthreads();
+            if (job >= njobs) break;
+        }
         const int job = S.job;
-        __syncthreads();
-        if (job >= njobs) break;
-        const int sj = multi ? M.job_seg[job] : 0;
+        // a request loop keys the segment a CTA holds by the request's sequence number (slots
+        // are reused by later requests)
+        const int sj = queue ? qjob.req : (multi ? M.job_seg[job] : 0);
         if (sj != cur) {
             if (multi) {
                 static_assert(sizeof(Segment) % sizeof(int4) == 0, "segment records are copied as int4");
-                const int4 *src = reinterpret_cast<const int4 *>(M.segs + sj);
+                const int4 *src = reinterpret_cast<const int4 *>(queue ? M.q.segs + qjob.slot : M.segs + sj);
                 int4 *dst = reinterpret_cast<int4 *>(&seg);
-                for (int i = tid; i < (int)(sizeof(Segment) / sizeof(int4)); i += blockDim.x) dst[i] = src[i];
+                for (int i = tid; i < (int)(sizeof(Segment) / sizeof(int4)); i += blockDim.x) dst[i] = __ldcg(src + i);
             } else if (tid == 0) {
                 seg.P = P0;
                 seg.A = A0;
@@ -674,8 +737,8 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, cons
             stage_tables<LT, XT>(seg.P, L);
             __syncthreads();
         }
-        const int first = multi ? M.job_first[job] : A0.job_first[job];
-        const int count = multi ? M.job_count[job] : A0.job_count[job];
+        const int first = queue ? qjob.first : (multi ? M.job_first[job] : A0.job_first[job]);
+        const int count = queue ? qjob.count : (multi ? M.job_count[job] : A0.job_count[job]);
         solve_job<LT, XT, LU_SMEM, REFINE>(seg.P, seg.A, S, L, first, count, pr);
         __syncthreads();
         if constexpr (REFINE) {
@@ -707,6 +770,9 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, cons
                     __syncthreads();
                 }
             }
+        }
+        if constexpr (QUEUE) {
+            if (tid == 0) signal_queue_job(M.q.done, qjob.slot, count);
         }
     }
     if (pr.on)
@@ -1121,20 +1187,28 @@ __global__ void __launch_bounds__(MAXT, MINB) fdpf_batch_kernel(const DevPlan P0
     }
 }
 
+template <typename LT, typename XT, bool SM, bool RF, bool Q>
+cudaError_t launch_variant_q(const DevPlan &P, const BatchArgs &A, const MultiArgs &M, int threads, int grid,
+                             size_t smem, cudaStream_t st) {
+    cudaError_t e = allow_max_smem(reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, Q>));
+    if (e != cudaSuccess) return e;
+    nr_batch_kernel<LT, XT, SM, RF, Q><<<grid, threads, smem, st>>>(P, A, M);
+    return cudaGetLastError();
+}
+
 template <typename LT, typename XT, bool SM, bool RF>
 cudaError_t launch_variant(const DevPlan &P, const BatchArgs &A, const MultiArgs &M, int threads, int grid,
                            size_t smem, cudaStream_t st) {
-    cudaError_t e = allow_max_smem(reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF>));
-    if (e != cudaSuccess) return e;
-    nr_batch_kernel<LT, XT, SM, RF><<<grid, threads, smem, st>>>(P, A, M);
-    return cudaGetLastError();
+    if (M.q.jobs != nullptr) return launch_variant_q<LT, XT, SM, RF, true>(P, A, M, threads, grid, smem, st);
+    return launch_variant_q<LT, XT, SM, RF, false>(P, A, M, threads, grid, smem, st);
 }
 
 template <typename LT, typename XT, bool SM, bool RF>
 int occupancy_variant(int threads, size_t smem) {
     int nb = 0;
-    if (allow_max_smem(reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF>)) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, nr_batch_kernel<LT, XT, SM, RF>, threads, smem) !=
+    if (allow_max_smem(reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, false>)) != cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, nr_batch_kernel<LT, XT, SM, RF, false>, threads, smem) !=
         cudaSuccess)
         return 0;
     return nb;

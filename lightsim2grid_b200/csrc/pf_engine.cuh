@@ -104,6 +104,27 @@ struct alignas(16) Segment {
 
 // Launch over several plans (segments): job j runs instances [job_first[j], job_first[j] +
 // job_count[j]) of segment job_seg[j].  segs == nullptr: a launch of one plan.
+// Device-resident request loop: a persistent launch takes its jobs from a ring in device memory
+// that the host appends to (through copies on a stream of its own), one segment per request slot.
+struct QueueJob {
+    int slot;   // the request's segment (and completion counter)
+    int first;  // its instances [first, first + count)
+    int count;
+    int req;    // the request's sequence number: identifies the segment a CTA holds
+};
+struct DevQueue {
+    const QueueJob *jobs;   // ring of `cap` jobs
+    int cap;
+    const Segment *segs;    // one per slot
+    int *head;              // jobs claimed (device memory, advanced with atomicCAS)
+    const int *tail;        // jobs published (device memory, written by the host's copies)
+    int *done;              // per slot, instances finished (mapped host memory, system-scope adds)
+    int *closing;           // device memory: set, the CTAs leave once the ring is empty
+    int idle_polls;         // a CTA that polled an empty ring this many times sets `closing` and
+                            // leaves (bounded wait): the launch ends as a whole, so the host never
+                            // sees a launch that kept only some of its CTAs
+};
+
 struct MultiArgs {
     const Segment *segs;
     const int *job_seg;
@@ -111,6 +132,7 @@ struct MultiArgs {
     const int *job_count;
     int njobs;
     int *job_counter;
+    DevQueue q;             // q.jobs non-null: the request loop (segs, job lists unused)
 };
 
 // phase_cycles slots: mismatch, J fill, refactorisation, forward, backward, refinement,

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <complex>
 #include <condition_variable>
 #include <cstring>
@@ -81,6 +82,7 @@ struct Arena {
 struct Grid {
     pf_plan *plan = nullptr;
     int n = 0, nbr = 0, ctas = 0, ctas_per_sm = 1;
+    int cls = -1;  // device loop: its class
     std::vector<cplx> S;            // base injections (host)
     void *dV0 = nullptr, *dS = nullptr;
     std::vector<int> cptr, rows, cols;
@@ -125,6 +127,38 @@ struct Req {
     bool small = true;   // instance-buses <= kSmallWork on a grid of at most kHeavyBuses buses
     int ctas = 0;        // CTAs of its launch
     int sms = 0;         // SMs those CTAs occupy (large requests)
+    int cls = -1;        // device loop: the loop class that runs it
+};
+
+// Device-resident request loop: the grids whose plans share an LU placement form a class, served by
+// one persistent launch of the Newton kernel in queue mode.  The host appends each admitted
+// request's segment and jobs to the class's rings in device memory through copies on a feeder
+// stream, then advances the ring's tail the same way (stream order: the entries land before the
+// tail); the kernel's CTAs claim jobs as they are published, write the results into the slot's
+// mapped pinned staging and count the finished instances per slot in mapped host memory.  After
+// kIdlePolls empty polls a CTA closes the loop (all its CTAs leave once the ring is empty); the host
+// closes it the same way when it switches modes or is destroyed, and launches it again whenever
+// work is published while it is not running.
+constexpr int kIdlePolls = 2000000;  // ~1-2 s of empty polls (500 ns naps) before a loop closes
+
+struct LoopClass {
+    std::vector<int> grids;
+    l2g::LoopShape sh;
+    int ctas = 0;
+    unsigned char *scratch = nullptr;   // device: per-CTA slabs
+    l2g::QueueJob *jobs = nullptr;      // device: job ring
+    int cap = 0;
+    l2g::Segment *segs = nullptr;       // device: one segment per slot
+    int *head = nullptr, *tail = nullptr, *closing = nullptr;  // device
+    l2g::QueueJob *job_stage = nullptr; // pinned: the ring's host image
+    l2g::Segment *seg_stage = nullptr;  // pinned: one segment per slot
+    int *tail_stage = nullptr;          // pinned: a ring of published tail values
+    int ntail = 0, tail_next = 0;
+    int published = 0;                  // jobs published
+    cudaStream_t kst = nullptr, fst = nullptr;
+    cudaEvent_t kev = nullptr;
+    bool launched = false;
+    int inflight = 0;                   // its requests not yet complete
 };
 
 }  // namespace
@@ -151,6 +185,11 @@ struct pf_server {
     std::deque<Req *> to_deliver;   // device work done, rows not yet copied
     std::vector<Req *> delivered;   // rows copied: slot and id returned by the next poll
     bool stop = false;
+    // device-resident request loop (pf_server_device_loop)
+    bool loop = false;
+    std::vector<LoopClass> classes;
+    int *done_host = nullptr, *done_dev = nullptr;  // mapped: instances finished per slot
+    int req_seq = 0;
 };
 
 namespace {
@@ -166,8 +205,32 @@ void stop_workers(pf_server *s) {
     s->workers.clear();
 }
 
+void free_loop(pf_server *s) {
+    for (LoopClass &c : s->classes) {
+        // close the loop (its CTAs leave once the ring is empty) and wait for it
+        if (c.closing && c.fst) {
+            cudaMemsetAsync(c.closing, 0xff, sizeof(int), c.fst);
+            cudaStreamSynchronize(c.fst);
+        }
+        if (c.kst) cudaStreamSynchronize(c.kst);
+        if (c.fst) cudaStreamSynchronize(c.fst);
+        for (void *p : {(void *)c.scratch, (void *)c.jobs, (void *)c.segs, (void *)c.head})
+            if (p) cudaFree(p);
+        for (void *p : {(void *)c.job_stage, (void *)c.seg_stage, (void *)c.tail_stage})
+            if (p) cudaFreeHost(p);
+        if (c.kev) cudaEventDestroy(c.kev);
+        if (c.kst) cudaStreamDestroy(c.kst);
+        if (c.fst) cudaStreamDestroy(c.fst);
+    }
+    s->classes.clear();
+    if (s->done_host) cudaFreeHost(s->done_host);
+    s->done_host = s->done_dev = nullptr;
+    s->loop = false;
+}
+
 void destroy(pf_server *s) {
     stop_workers(s);
+    free_loop(s);
     for (Req *r : s->to_deliver) delete r;
     for (Req *r : s->delivered) delete r;
     for (Grid &g : s->grids) {
@@ -236,7 +299,10 @@ int prepare(pf_server *s, Req *r) {
     if (!r->small) ctas = std::max(1, std::min(ctas, s->large_ctas));
     r->ctas = ctas;
     r->sms = (ctas + g.ctas_per_sm - 1) / g.ctas_per_sm;
-    r->scratch = r->ninst ? align256((size_t)pf_scratch_bytes(g.plan, ctas)) : 0;
+    // device loop: the small requests of grids that a loop serves go through it (their CTAs are
+    // resident); the others are launched as usual
+    r->cls = (s->loop && r->small) ? g.cls : -1;
+    r->scratch = (r->ninst && r->cls < 0) ? align256((size_t)pf_scratch_bytes(g.plan, ctas)) : 0;
     r->outs = 0;  // the kernel writes the results straight into the slot's mapped pinned staging
     r->bytes = r->scratch + r->outs + r->ins;
     return 0;
@@ -285,6 +351,79 @@ int launch(pf_server *s, Req *r) {
     }
     e = cudaEventRecord(sl.ev, sl.st);
     if (e != cudaSuccess) return fail(std::string("pf_server: event: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+// Device loop: the request's inputs, segment and jobs go to the class's rings on the feeder stream,
+// then the new tail; the loop is launched when it is not running.
+int publish(pf_server *s, Req *r) {
+    Grid &g = s->grids[r->grid];
+    Slot &sl = s->slots[r->slot];
+    LoopClass &c = s->classes[r->cls];
+    unsigned char *in = s->arena_ptr + r->off;
+    unsigned char *out = sl.pin_out_dev;
+    cudaError_t e = cudaSuccess;
+    pf_device_batch b{};
+    b.n_inst = r->ninst;
+    b.V0 = g.dV0;
+    b.max_iter = g.max_iter;
+    b.tol = g.tol;
+    b.Vout = out;
+    b.iters = reinterpret_cast<int *>(out + (size_t)r->ninst * g.n * 16);
+    b.errs = b.iters + r->ninst;
+    if (r->kind == 0) {
+        cplx *S = reinterpret_cast<cplx *>(sl.pin_in);
+        for (int i = 0; i < g.n; ++i) S[i] = g.S[i] * r->scale[i];
+        e = cudaMemcpyAsync(in, sl.pin_in, (size_t)g.n * 16, cudaMemcpyHostToDevice, c.fst);
+        b.Sbus = in;
+    } else {
+        const size_t a1 = align256((size_t)(r->ninst + 1) * 4), a2 = align256(r->opos.size() * 4);
+        std::memcpy(sl.pin_in, r->optr.data(), (size_t)(r->ninst + 1) * 4);
+        std::memcpy(sl.pin_in + a1, r->opos.data(), r->opos.size() * 4);
+        std::memcpy(sl.pin_in + a1 + a2, r->oval.data(), r->oval.size() * 16);
+        e = cudaMemcpyAsync(in, sl.pin_in, a1 + a2 + r->oval.size() * 16, cudaMemcpyHostToDevice, c.fst);
+        b.Sbus = g.dS;
+        b.ovr_ptr = reinterpret_cast<const int *>(in);
+        b.ovr_pos = reinterpret_cast<const int *>(in + a1);
+        b.ovr_val = in + a1 + a2;
+    }
+    if (e != cudaSuccess) return fail(std::string("pf_server: upload: ") + cudaGetErrorString(e));
+    l2g::Segment &sg = c.seg_stage[r->slot];
+    int rc = l2g::loop_segment(g.plan, &b, c.sh, c.scratch, &sg);
+    if (rc != 0) return rc;
+    e = cudaMemcpyAsync(c.segs + r->slot, &sg, sizeof(l2g::Segment), cudaMemcpyHostToDevice, c.fst);
+    if (e != cudaSuccess) return fail(std::string("pf_server: segment: ") + cudaGetErrorString(e));
+    // the jobs: one per instance, in the ring (two copies when it wraps)
+    const int seq = s->req_seq++;
+    s->done_host[r->slot] = 0;  // read by the host only; the loop adds once it runs the jobs
+    const int start = c.published % c.cap;
+    for (int i = 0; i < r->ninst; ++i) c.job_stage[(start + i) % c.cap] = l2g::QueueJob{r->slot, i, 1, seq};
+    const int first_len = std::min(r->ninst, c.cap - start);
+    e = cudaMemcpyAsync(c.jobs + start, c.job_stage + start, (size_t)first_len * sizeof(l2g::QueueJob),
+                        cudaMemcpyHostToDevice, c.fst);
+    if (e == cudaSuccess && r->ninst > first_len)
+        e = cudaMemcpyAsync(c.jobs, c.job_stage, (size_t)(r->ninst - first_len) * sizeof(l2g::QueueJob),
+                            cudaMemcpyHostToDevice, c.fst);
+    c.published += r->ninst;
+    // the new tail, from a ring of pinned values (each stays untouched until its copy has run:
+    // the ring is longer than the requests that can be in flight)
+    int *tv = c.tail_stage + c.tail_next;
+    c.tail_next = (c.tail_next + 1) % c.ntail;
+    *tv = c.published;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c.tail, tv, sizeof(int), cudaMemcpyHostToDevice, c.fst);
+    if (e != cudaSuccess) return fail(std::string("pf_server: queue: ") + cudaGetErrorString(e));
+    c.inflight += 1;
+    if (!c.launched) {
+        if ((e = cudaMemsetAsync(c.closing, 0, sizeof(int), c.kst)) != cudaSuccess)
+            return fail(std::string("pf_server: loop reset: ") + cudaGetErrorString(e));
+        rc = l2g::loop_launch(c.sh, sg,
+                              l2g::DevQueue{c.jobs, c.cap, c.segs, c.head, c.tail, s->done_dev, c.closing, kIdlePolls},
+                              c.ctas, c.kst);
+        if (rc != 0) return rc;
+        if ((e = cudaEventRecord(c.kev, c.kst)) != cudaSuccess)
+            return fail(std::string("pf_server: loop event: ") + cudaGetErrorString(e));
+        c.launched = true;
+    }
     return 0;
 }
 
@@ -478,14 +617,26 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
     // device completions: the device region is free; the rows go to a delivery worker (the slot's
     // pinned staging stays with the request until they are copied)
     bool queued = false;
+    if (s->loop) std::atomic_thread_fence(std::memory_order_acquire);
     for (size_t i = 0; i < s->inflight.size();) {
         Req *r = s->inflight[i];
-        const cudaError_t q = cudaEventQuery(s->slots[r->slot].ev);
-        if (q == cudaErrorNotReady) {
-            ++i;
-            continue;
+        if (r->cls >= 0) {
+            // the loop counts the finished instances of the slot in mapped host memory
+            const int d = *reinterpret_cast<volatile int *>(s->done_host + r->slot);
+            if (d < r->ninst) {
+                ++i;
+                continue;
+            }
+            std::atomic_thread_fence(std::memory_order_acquire);
+            if (r->ninst > 0) s->classes[r->cls].inflight -= 1;
+        } else {
+            const cudaError_t q = cudaEventQuery(s->slots[r->slot].ev);
+            if (q == cudaErrorNotReady) {
+                ++i;
+                continue;
+            }
+            if (q != cudaSuccess) return fail(std::string("pf_server_poll: ") + cudaGetErrorString(q));
         }
-        if (q != cudaSuccess) return fail(std::string("pf_server_poll: ") + cudaGetErrorString(q));
         if (!r->small) s->large_sms_inflight -= r->sms;
         s->arena.release(r->off, r->bytes);
         s->in_use -= align256(r->bytes);
@@ -498,6 +649,27 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
         s->inflight.pop_back();
     }
     if (queued) s->cv.notify_all();
+    // the loops: one that left (its CTAs ran out of published jobs) while requests of its class are
+    // still open is launched again (their jobs are published and not yet claimed)
+    for (LoopClass &c : s->classes) {
+        if (!c.launched) continue;
+        const cudaError_t q = cudaEventQuery(c.kev);
+        if (q == cudaErrorNotReady) continue;
+        if (q != cudaSuccess) return fail(std::string("pf_server_poll: request loop: ") + cudaGetErrorString(q));
+        c.launched = false;
+        if (c.inflight > 0) {
+            cudaError_t e0 = cudaMemsetAsync(c.closing, 0, sizeof(int), c.kst);
+            if (e0 != cudaSuccess) return fail(std::string("pf_server_poll: loop reset: ") + cudaGetErrorString(e0));
+            const int rc = l2g::loop_launch(
+                c.sh, c.seg_stage[0],
+                l2g::DevQueue{c.jobs, c.cap, c.segs, c.head, c.tail, s->done_dev, c.closing, kIdlePolls}, c.ctas,
+                c.kst);
+            if (rc != 0) return rc;
+            const cudaError_t e = cudaEventRecord(c.kev, c.kst);
+            if (e != cudaSuccess) return fail(std::string("pf_server_poll: loop event: ") + cudaGetErrorString(e));
+            c.launched = true;
+        }
+    }
     // admissions, oldest first; a large request that would take SMs from the reserve waits, and
     // the large ones behind it wait too (their order is kept), while small ones go past it
     const int large_budget = std::max(1, s->num_sms - s->reserved_sms);
@@ -527,11 +699,97 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
         std::vector<int> &pool = pref.empty() ? other : pref;
         r->slot = pool.back();
         pool.pop_back();
-        const int rc = launch(s, r);
+        int rc = 0;
+        if (r->cls >= 0) {
+            if (r->ninst > 0) rc = publish(s, r);
+            else s->done_host[r->slot] = 0;  // every outage islanded: nothing to run
+        } else {
+            rc = launch(s, r);
+        }
         s->inflight.push_back(r);
         if (rc != 0) return rc;
     }
     return nd;
+}
+
+int pf_server_device_loop(pf_server *s, int enable, int ctas_shared, int ctas_global) {
+    if (!s || ctas_shared < 0 || ctas_global < 0) return fail("pf_server_device_loop: invalid argument");
+    if (!s->pending.empty() || !s->inflight.empty())
+        return fail("pf_server_device_loop: requests are queued or running; switch modes when idle");
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (!s->to_deliver.empty() || !s->delivered.empty())
+            return fail("pf_server_device_loop: results are being delivered; switch modes when idle");
+    }
+    free_loop(s);
+    if (!enable) return 0;
+    // classes: the grids that have small requests (at most kHeavyBuses buses), split by LU
+    // placement; the requests of larger grids keep their own launches, which spread over the SMs
+    // the loops leave free
+    std::vector<int> by[2];
+    for (int i = 0; i < (int)s->grids.size(); ++i) {
+        s->grids[i].cls = -1;
+        pf_plan_info info;
+        if (pf_plan_info_get(s->grids[i].plan, &info) != 0) return fail("pf_server_device_loop: plan info");
+        if (s->grids[i].n <= kHeavyBuses) by[info.lu_in_shared ? 0 : 1].push_back(i);
+    }
+    if (by[0].empty() && by[1].empty()) return 0;  // nothing small to serve: launches only
+    const int ncls = (!by[0].empty()) + (!by[1].empty());
+    cudaError_t e = cudaSuccess;
+    if ((e = cudaHostAlloc(reinterpret_cast<void **>(&s->done_host), sizeof(int) * (size_t)s->nslots,
+                           cudaHostAllocMapped)) != cudaSuccess ||
+        (e = cudaHostGetDevicePointer(reinterpret_cast<void **>(&s->done_dev), s->done_host, 0)) != cudaSuccess) {
+        free_loop(s);
+        return fail(std::string("pf_server_device_loop: completion counters: ") + cudaGetErrorString(e));
+    }
+    std::memset(s->done_host, 0, sizeof(int) * (size_t)s->nslots);
+    s->classes.resize(ncls);
+    int k = 0;
+    for (int which = 0; which < 2; ++which) {
+        if (by[which].empty()) continue;
+        LoopClass &c = s->classes[k];
+        c.grids = by[which];
+        std::vector<pf_plan *> plans;
+        for (int gi : c.grids) {
+            plans.push_back(s->grids[gi].plan);
+            s->grids[gi].cls = k;
+        }
+        int rc = l2g::loop_shape(plans.data(), (int)plans.size(), &c.sh);
+        if (rc != 0) {
+            free_loop(s);
+            return rc;
+        }
+        // CTAs: a quarter of the SMs' worth for one class (the small requests' load; the rest of the
+        // GPU stays with the launches of the large ones), an eighth each with two
+        int want = which == 0 ? ctas_shared : ctas_global;
+        if (want <= 0) want = std::max(1, (ncls == 1 ? s->num_sms / 4 : s->num_sms / 8) * c.sh.ctas_per_sm);
+        c.ctas = std::min(want, s->num_sms * c.sh.ctas_per_sm);
+        c.cap = 2 * s->nslots * s->max_k;
+        c.ntail = 2 * s->nslots + 2;
+        if ((e = cudaMalloc(&c.scratch, c.sh.slab * (size_t)c.ctas)) != cudaSuccess ||
+            (e = cudaMalloc(&c.jobs, sizeof(l2g::QueueJob) * (size_t)c.cap)) != cudaSuccess ||
+            (e = cudaMalloc(&c.segs, sizeof(l2g::Segment) * (size_t)s->nslots)) != cudaSuccess ||
+            (e = cudaMalloc(&c.head, 3 * sizeof(int))) != cudaSuccess ||
+            (e = cudaMemset(c.head, 0, 3 * sizeof(int))) != cudaSuccess ||
+            (e = cudaHostAlloc(reinterpret_cast<void **>(&c.job_stage), sizeof(l2g::QueueJob) * (size_t)c.cap,
+                               cudaHostAllocDefault)) != cudaSuccess ||
+            (e = cudaHostAlloc(reinterpret_cast<void **>(&c.seg_stage), sizeof(l2g::Segment) * (size_t)s->nslots,
+                               cudaHostAllocDefault)) != cudaSuccess ||
+            (e = cudaHostAlloc(reinterpret_cast<void **>(&c.tail_stage), sizeof(int) * (size_t)c.ntail,
+                               cudaHostAllocDefault)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&c.kst, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&c.fst, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&c.kev, cudaEventDisableTiming)) != cudaSuccess) {
+            free_loop(s);
+            return fail(std::string("pf_server_device_loop: allocation: ") + cudaGetErrorString(e));
+        }
+        c.tail = c.head + 1;
+        c.closing = c.head + 2;
+        std::memset(c.seg_stage, 0, sizeof(l2g::Segment) * (size_t)s->nslots);
+        ++k;
+    }
+    s->loop = true;
+    return 0;
 }
 
 int pf_server_configure(pf_server *s, int reserved_sms, int large_request_ctas) {

@@ -160,7 +160,8 @@ class GridService:
 class NativeServer:
     """The library's serving core (``pf_server_*``) over ``GridService`` objects."""
 
-    def __init__(self, services, hbm_budget, slots, max_instances=64, reserved_sms=None, large_request_ctas=0):
+    def __init__(self, services, hbm_budget, slots, max_instances=64, reserved_sms=None, large_request_ctas=0,
+                 device_loop=False):
         self._lib = nat.load()
         self.names = list(services)
         self.index = {nm: i for i, nm in enumerate(self.names)}
@@ -181,6 +182,8 @@ class NativeServer:
         self._h = h
         if reserved_sms is not None or large_request_ctas:
             self.configure(reserved_sms, large_request_ctas)
+        if device_loop:
+            self.set_device_loop(True)
         self._done = np.zeros(1024, np.int64)
         self.live = {}
 
@@ -194,6 +197,15 @@ class NativeServer:
             reserved_sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count // 8
         nat.check(self._lib.pf_server_configure(self._h, int(reserved_sms), int(large_request_ctas)),
                   "pf_server_configure", self._lib)
+
+    device_loop = False
+
+    def set_device_loop(self, enable=True, ctas_shared=0, ctas_global=0):
+        """Serve through persistent device loops (pf_server_device_loop) instead of one launch per
+        request; only while nothing is queued or running."""
+        nat.check(self._lib.pf_server_device_loop(self._h, 1 if enable else 0, int(ctas_shared), int(ctas_global)),
+                  "pf_server_device_loop", self._lib)
+        self.device_loop = bool(enable)
 
     def submit(self, req):
         """Queues a request; its result arrays are allocated here (case order)."""
@@ -274,10 +286,11 @@ class PowerFlowServer:
     """Grids served from one GPU.  ``grids``: name -> GridModel."""
 
     def __init__(self, grids, device=None, hbm_budget=2 << 30, slots=32, precision=1, max_iter=10, tol=1e-8,
-                 max_instances=64, reserved_sms=None, large_request_ctas=0, **plan_options):
+                 max_instances=64, reserved_sms=None, large_request_ctas=0, device_loop=False, **plan_options):
         self.services = {name: GridService(name, g, precision=precision, max_iter=max_iter, tol=tol, **plan_options)
                          for name, g in grids.items()}
-        self.native = NativeServer(self.services, hbm_budget, slots, max_instances, reserved_sms, large_request_ctas)
+        self.native = NativeServer(self.services, hbm_budget, slots, max_instances, reserved_sms, large_request_ctas,
+                                   device_loop)
 
     def serve(self, requests, realtime=True, clock=time.perf_counter):
         """Serves ``requests`` (sorted by arrival).  ``realtime``: a request is submitted when

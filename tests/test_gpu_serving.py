@@ -12,8 +12,8 @@ pytestmark = pytest.mark.gpu
 TOL_ORACLE = 1e-8  # |V - V_oracle| (pu) for the mixed form converged at 1e-8 pu
 
 
-@pytest.fixture(scope="module")
-def server():
+@pytest.fixture(scope="module", params=["launch per request", "device loop"])
+def server(request):
     from lightsim2grid_b200 import synthetic
     from lightsim2grid_b200.serving import PowerFlowServer
 
@@ -21,7 +21,8 @@ def server():
     # ones that stay resident longest beside other requests
     grids = {name: synthetic.make_named_grid(name)[0]
              for name in ("grid14", "grid118", "grid300", "grid1354", "grid2848", "grid6515")}
-    srv = PowerFlowServer(grids, hbm_budget=2 << 30, slots=16, precision=1, large_request_ctas=16)
+    srv = PowerFlowServer(grids, hbm_budget=2 << 30, slots=16, precision=1, large_request_ctas=16,
+                          device_loop=request.param == "device loop")
     srv.grids = grids
     return srv
 
@@ -80,3 +81,21 @@ def test_results_match_oracle(server):
                 assert np.abs(r.V[ok] - Vo[ok]).max() <= TOL_ORACLE
             checked["n1"] += 1
     assert checked["pf"] >= 3 and checked["n1"] >= 2
+
+
+def test_device_loop_equals_launch_per_request(server):
+    """The same requests through the persistent device loop and through one launch per request:
+    the same bits (the same solver code per instance, inputs read through L2 in both)."""
+    reqs = _requests(server, seed=23, duration=0.03)
+    done = {r.rid: r for r in server.serve(reqs, realtime=True)}
+    other = not server.native.device_loop
+    server.native.set_device_loop(other)
+    try:
+        again = {r.rid: r for r in server.serve(_requests(server, seed=23, duration=0.03), realtime=True)}
+    finally:
+        server.native.set_device_loop(not other)
+    assert set(done) == set(again) and len(done) >= 20
+    for rid, r in done.items():
+        a = again[rid]
+        assert np.array_equal(r.errs, a.errs) and np.array_equal(r.iters, a.iters), rid
+        assert np.array_equal(r.V, a.V), rid
