@@ -398,7 +398,9 @@ long long pf_scratch_bytes(const pf_plan *plan, int ctas);
    over CTAs spent in mismatch, J fill, refactorisation, forward substitution, backward
    substitution, refinement (mixed form), voltage update / start-up, and the number of
    instances.  The device counterpart of the reference's per-phase NR timers
-   (get_timers_jacobian, src/powerflow_algorithm/BaseNRAlgo.hpp:48-62). */
+   (get_timers_jacobian, src/powerflow_algorithm/BaseNRAlgo.hpp:48-62).  With the batch-interleaved
+   layout the counters are that kernel's (its follow-up launches are not counted), the
+   substitution slots cover its backward programs and out[7] counts its rounds. */
 int pf_batch_device_phase_cycles(pf_plan *plan, const pf_device_batch *batch, void *stream, double *out);
 
 /* pf_batch_device, synchronously, recording the SM clock after every phase of the first

@@ -550,7 +550,7 @@ void release(pf_plan *pl) {
 constexpr int kAutoTileLU = 40000;
 
 bool use_tile(const pf_plan *pl, const l2g::BatchArgs &a) {
-    if (pl->P.dc || pl->P.fdpf || a.chain || a.Jout || a.phase_cycles || a.trace || a.reuse_below > 0) return false;
+    if (pl->P.dc || pl->P.fdpf || a.chain || a.Jout || a.trace || a.reuse_below > 0) return false;
     if (pl->opt.batch_layout == 2) return true;
     return pl->opt.batch_layout == 0 && !pl->lu_in_smem && pl->P.nnzLU >= kAutoTileLU && a.njobs >= 4 * pl->num_sms;
 }
@@ -605,6 +605,7 @@ int launch_tile(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, i
     // the stragglers, from their output rows and iteration counts (the mixed form's in-launch FP64
     // fallback covers their failures)
     l2g::BatchArgs c = orig;
+    c.phase_cycles = nullptr;  // the per-section cycles are the interleaved kernel's
     c.job_first = hand;
     c.job_count = ones;
     c.njobs = a.n_inst;
@@ -616,6 +617,7 @@ int launch_tile(pf_plan *pl, l2g::BatchArgs a, int precision, cudaStream_t st, i
     if (rc) return rc;
     if (fallback) {
         l2g::BatchArgs f = orig;
+        f.phase_cycles = nullptr;
         f.job_first = fbl;
         f.job_count = ones;
         f.njobs = a.n_inst;

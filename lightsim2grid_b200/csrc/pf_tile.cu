@@ -40,7 +40,20 @@ struct TileLanes {
     int nactive, nstep, nrefine;
     int exhausted;  // a lane found the job list empty
     int handoff;    // the CTA hands its running instances to the one-CTA kernel and stops
+    // optional SM cycles per section (A.phase_cycles): mismatch, J fill, refactorisation, forward,
+    // backward, refinement residual, update / refill / results, rounds
+    unsigned long long pc[kPhaseSlots];
+    unsigned long long tmark;
 };
+
+// adds the cycles since the last mark to section k (thread 0, when requested)
+__device__ __forceinline__ void tile_mark(TileLanes &S, bool on, int k) {
+    if (on && threadIdx.x == 0) {
+        const unsigned long long t = clock64();
+        S.pc[k] += t - S.tmark;
+        S.tmark = t;
+    }
+}
 
 // 32-bit offsets: every slab array has fewer than 2^27 rows
 __device__ __forceinline__ unsigned ix(int i, int lane) { return ((unsigned)i << 5) | (unsigned)lane; }
@@ -130,9 +143,12 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
     double *Vm = reinterpret_cast<double *>(q);
     q += al256((size_t)n * kLanes * 8);
     double *Va = reinterpret_cast<double *>(q);
+    const bool prof = A.phase_cycles != nullptr;
     if (tid == 0) {
         S.exhausted = 0;
         S.handoff = 0;
+        for (int k = 0; k < kPhaseSlots; ++k) S.pc[k] = 0;
+        S.tmark = clock64();
     }
     if (tid < kLanes) {
         S.state[tid] = tid < A.tile_lanes ? kFree : kIdle;
@@ -144,6 +160,8 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
     __syncthreads();
     for (;;) {
         // ---- refill: finished lanes take the next instance of their job, or a new job
+        tile_mark(S, prof, 6);
+        if (prof && tid == 0) S.pc[7] += 1;
         if (warp == 0) {
             int st = S.state[lane];
             int lane_exh = 0;
@@ -281,6 +299,7 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
             S.ired[warp][lane] = lbad;
         }
         __syncthreads();
+        tile_mark(S, prof, 0);
         // ---- per-instance decisions
         if (warp == 0) {
             int st = S.state[lane];
@@ -342,8 +361,10 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
                 for (int i = warp; i < P.nconst; i += kW) lu[ix(P.cpos[i], lane)] = (LT)P.cval[i];
             }
             __syncthreads();
+            tile_mark(S, prof, 1);
             // ---- refactorisation with the forward substitution of F fused in
             tile_program<LT>(P.tfac_ops, phf, P.fac_nph, lu, x, lane, warp, step);
+            tile_mark(S, prof, 2);
             {
                 int zero = 0;
                 if (step)
@@ -362,10 +383,12 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
             __syncthreads();
             const bool solve = S.state[lane] == kStep;
             // ---- backward substitution and the pivot scaling
+            tile_mark(S, prof, 6);
             tile_program<LT>(P.tbwd_ops, phb, P.bwd_nph, lu, x, lane, warp, solve);
             if (solve)
                 for (int k = warp; k < m; k += kW) x[ix(k, lane)] = lu_div(x[ix(k, lane)], lu[ix(P.dpos[k], lane)]);
             __syncthreads();
+            tile_mark(S, prof, 4);
             const bool refine = solve && S.refine[lane] != 0;
             if (REFINE && S.nrefine > 0) {
                 // ---- refinement against the FP64 Jacobian: rhs = F - J dx, solved again
@@ -398,12 +421,15 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
                         if (iq >= 0) x[ix(iq, lane)] = (LT)(F.y - accQ);
                     }
                 __syncthreads();
+                tile_mark(S, prof, 5);
                 tile_program<LT>(P.tfwd_ops, phw, P.fwd_nph, lu, x, lane, warp, refine);
+                tile_mark(S, prof, 3);
                 tile_program<LT>(P.tbwd_ops, phb, P.bwd_nph, lu, x, lane, warp, refine);
                 if (refine)
                     for (int k = warp; k < m; k += kW)
                         x[ix(k, lane)] = lu_div(x[ix(k, lane)], lu[ix(P.dpos[k], lane)]);
                 __syncthreads();
+                tile_mark(S, prof, 4);
             }
             // ---- voltage update
             double lmin = 1.0;
@@ -462,6 +488,10 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
             }
         }
         __syncthreads();
+    }
+    if (prof && tid == 0) {
+        tile_mark(S, prof, 6);
+        for (int k = 0; k < kPhaseSlots; ++k) A.phase_cycles[(size_t)blockIdx.x * kPhaseSlots + k] = S.pc[k];
     }
 }
 
