@@ -4,11 +4,16 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdint>
 #include <cstring>
 #include <functional>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
+
+#include <unistd.h>
 
 #include "pf_capi_internal.hpp"
 #include "pf_engine.cuh"
@@ -30,6 +35,84 @@ int fail(int code, const std::string &msg) {
 int cuda_fail(cudaError_t e, const char *where) {
     g_err = std::string(where) + ": " + cudaGetErrorString(e);
     return -2;
+}
+
+// Host threads for the per-case preparation of large N-1 batches: a pool started on first use
+// and kept for the life of the process (never joined: its threads sleep on a condition variable
+// between calls).  One parallel region at a time; a caller that finds the pool busy (another
+// host thread preparing a batch), or a process forked after the pool started (which has none of
+// its threads), runs its region on its own thread.
+class HostPool {
+  public:
+    static HostPool &get() {
+        static HostPool *pool = new HostPool();
+        return *pool;
+    }
+    int threads() const { return (int)workers_.size() + 1; }
+    // fn(t, nt) for t = 0 .. nt-1, t = 0 on the calling thread
+    void run(int nt, const std::function<void(int, int)> &fn) {
+        nt = std::max(1, std::min(nt, threads()));
+        if (getpid() != owner_) nt = 1;
+        if (nt == 1) {
+            fn(0, 1);
+            return;
+        }
+        std::unique_lock<std::mutex> region(busy_, std::try_to_lock);
+        if (!region.owns_lock()) {
+            fn(0, 1);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            job_ = &fn;
+            njob_ = nt;
+            pending_ = nt - 1;
+            ++gen_;
+        }
+        cv_.notify_all();
+        fn(0, nt);
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [&] { return pending_ == 0; });
+        job_ = nullptr;
+    }
+
+  private:
+    HostPool() : owner_(getpid()) {
+        const int hw = (int)std::thread::hardware_concurrency();
+        const int nw = std::max(0, std::min(hw, 16) - 1);
+        for (int i = 0; i < nw; ++i) {
+            workers_.emplace_back([this, i] { loop(i + 1); });
+            workers_.back().detach();
+        }
+    }
+    void loop(int id) {
+        long long seen = 0;
+        std::unique_lock<std::mutex> lk(m_);
+        for (;;) {
+            cv_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+            if (id >= njob_) continue;
+            const std::function<void(int, int)> *f = job_;
+            const int nt = njob_;
+            lk.unlock();
+            (*f)(id, nt);
+            lk.lock();
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    pid_t owner_;
+    std::vector<std::thread> workers_;
+    std::mutex busy_, m_;
+    std::condition_variable cv_, done_;
+    const std::function<void(int, int)> *job_ = nullptr;
+    int njob_ = 0, pending_ = 0;
+    long long gen_ = 0;
+};
+
+// [lo, hi) of part t of nt equal parts of [0, n)
+inline void part_range(int n, int t, int nt, int &lo, int &hi) {
+    lo = (int)((long long)n * t / nt);
+    hi = (int)((long long)n * (t + 1) / nt);
 }
 
 // Entry points that take device pointers launch on the current device: it must be the device the
@@ -299,6 +382,13 @@ int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl,
     size_t oyt = push(bi, P.ytarget), oyj = push(bi, P.yjpos);
     size_t ofill = push(bi, P.fillpos), ocpos = push(bi, P.cpos), ocj = push(bi, P.cjpos);
     size_t oxP = push(bi, P.xP), oxQ = push(bi, P.xQ), oxVa = push(bi, P.xVa), oxVm = push(bi, P.xVm);
+    std::vector<int> ycol(2 * (size_t)P.nnzY, -1);
+    if ((int)P.xVa.size() == P.n && (int)P.xVm.size() == P.n && (int)P.Rj.size() >= P.nnzY)
+        for (int p = 0; p < P.nnzY; ++p) {
+            ycol[2 * (size_t)p] = P.xVa[P.Rj[p]];
+            ycol[2 * (size_t)p + 1] = P.xVm[P.Rj[p]];
+        }
+    const size_t oycol = push(bi, ycol);
     size_t ofo = push(bi, P.factor.ops), ofb = push(bi, P.factor.base), ofw = push(bi, P.factor.width);
     size_t obo = push(bi, P.backward.ops), obb = push(bi, P.backward.base), obw = push(bi, P.backward.width);
     size_t owo = push(bi, P.forward.ops), owb = push(bi, P.forward.base), oww = push(bi, P.forward.width);
@@ -381,6 +471,7 @@ int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl,
     d.xQ = I(oxQ);
     d.xVa = I(oxVa);
     d.xVm = I(oxVm);
+    d.ycol = reinterpret_cast<const int2 *>(bI + oycol);
     d.xSlack = P.xSlack;
     d.wJ = D(owJ);
     d.fac_ops = I4(ofo);
@@ -1252,29 +1343,68 @@ int pf_n1_prepare(pf_plan *pl, int ncases, const int *case_ptr, const int *coef_
                   const double *coef_val_ri, int *solvable, int *ovr_ptr, int *ovr_pos, double *ovr_val_ri, int cap) {
     if (!pl || ncases < 0 || !case_ptr || !solvable || !ovr_ptr) return fail(-1, "pf_n1_prepare: null argument");
     const cplx *cv = reinterpret_cast<const cplx *>(coef_val_ri);
-    std::vector<int> opos;
-    std::vector<cplx> oval;
+    // per case, in parallel over contiguous parts of the cases: the overrides (status -1: a
+    // coefficient outside the pattern, -2: more than kMaxOverrides entries, 0: islanded,
+    // 1: solvable); then, in case order, the outputs and the first error, as a serial pass would
+    struct Part {
+        std::vector<int> status, first, pos;
+        std::vector<cplx> val;
+    };
+    HostPool &pool = HostPool::get();
+    const int nt = ncases >= 256 ? pool.threads() : 1;
+    std::vector<Part> parts(nt);
+    pool.run(nt, [&](int t, int nparts) {
+        int lo, hi;
+        part_range(ncases, t, nparts, lo, hi);
+        Part &pt = parts[t];
+        std::vector<int> opos;
+        std::vector<cplx> oval;
+        for (int c = lo; c < hi; ++c) {
+            int st;
+            if (case_overrides(pl->P, case_ptr[c], case_ptr[c + 1], coef_row, coef_col, cv, opos, oval) != 0)
+                st = -1;
+            else if ((int)opos.size() > l2g::kMaxOverrides)
+                st = -2;
+            else
+                st = case_connected(pl, opos, oval) ? 1 : 0;
+            pt.status.push_back(st);
+            pt.first.push_back((int)pt.pos.size());
+            if (st == 1) {
+                pt.pos.insert(pt.pos.end(), opos.begin(), opos.end());
+                pt.val.insert(pt.val.end(), oval.begin(), oval.end());
+            }
+            if (st < 0) break;  // the serial pass stops at this case
+        }
+        pt.first.push_back((int)pt.pos.size());
+    });
     int w = 0, ns = 0;
     ovr_ptr[0] = 0;
-    for (int c = 0; c < ncases; ++c) {
-        if (case_overrides(pl->P, case_ptr[c], case_ptr[c + 1], coef_row, coef_col, cv, opos, oval) != 0)
-            return fail(-1, "pf_n1_prepare: case " + std::to_string(c) +
-                                " removes a coefficient that is not in the Ybus pattern");
-        if ((int)opos.size() > l2g::kMaxOverrides)
-            return fail(-1, "pf_n1_prepare: case " + std::to_string(c) + " changes more than 32 Ybus entries");
-        solvable[c] = case_connected(pl, opos, oval) ? 1 : 0;
-        if (!solvable[c]) continue;
-        if (w + (int)opos.size() > cap) return -3;
-        for (size_t i = 0; i < opos.size(); ++i) {
-            if (ovr_pos) ovr_pos[w] = opos[i];
-            if (ovr_val_ri) {
-                ovr_val_ri[2 * w] = oval[i].real();
-                ovr_val_ri[2 * w + 1] = oval[i].imag();
+    for (int t = 0; t < nt; ++t) {
+        const Part &pt = parts[t];
+        int lo, hi;
+        part_range(ncases, t, nt, lo, hi);
+        for (int i = 0; i < (int)pt.status.size(); ++i) {
+            const int c = lo + i, st = pt.status[i];
+            if (st == -1)
+                return fail(-1, "pf_n1_prepare: case " + std::to_string(c) +
+                                    " removes a coefficient that is not in the Ybus pattern");
+            if (st == -2)
+                return fail(-1, "pf_n1_prepare: case " + std::to_string(c) + " changes more than 32 Ybus entries");
+            solvable[c] = st;
+            if (!st) continue;
+            const int k0 = pt.first[i], k1 = pt.first[i + 1];
+            if (w + (k1 - k0) > cap) return -3;
+            for (int k = k0; k < k1; ++k) {
+                if (ovr_pos) ovr_pos[w] = pt.pos[k];
+                if (ovr_val_ri) {
+                    ovr_val_ri[2 * w] = pt.val[k].real();
+                    ovr_val_ri[2 * w + 1] = pt.val[k].imag();
+                }
+                ++w;
             }
-            ++w;
+            ++ns;
+            ovr_ptr[ns] = w;
         }
-        ++ns;
-        ovr_ptr[ns] = w;
     }
     return w;
 }
@@ -1286,28 +1416,41 @@ int pf_n1_order(const pf_plan *pl, int ninst, const int *ovr_ptr, const int *ovr
     const l2g::Plan &P = pl->P;
     const cplx *V = reinterpret_cast<const cplx *>(V0_ri);
     const cplx *ov = reinterpret_cast<const cplx *>(ovr_val_ri);
+    // score: max over the changed rows r of |dS_r|^2 (the squares rank as the magnitudes do),
+    // dS_r = V_r conj(sum over the instance's changed entries (r, c) of dY V_c), at V0
     std::vector<double> score(ninst, 0.0);
-    std::vector<std::pair<int, cplx>> rowsum;
-    for (int i = 0; i < ninst; ++i) {
-        // dS_r = V_r conj(sum over the instance's changed entries (r, c) of dY V_c), at V0
-        rowsum.clear();
-        for (int k = ovr_ptr[i]; k < ovr_ptr[i + 1]; ++k) {
-            const int p = ovr_pos[k];
-            if (p < 0 || p >= P.nnzY) return fail(-1, "pf_n1_order: override position out of range");
-            const int r = P.Rrow[p], c = P.Rj[p];
-            const cplx dI = (ov[k] - P.Rx[p]) * V[c];
-            bool found = false;
-            for (auto &e : rowsum)
-                if (e.first == r) {
-                    e.second += dI;
-                    found = true;
+    std::vector<char> bad(ninst, 0);
+    HostPool &pool = HostPool::get();
+    const int nt = ninst >= 256 ? pool.threads() : 1;
+    pool.run(nt, [&](int t, int nparts) {
+        int lo, hi;
+        part_range(ninst, t, nparts, lo, hi);
+        std::vector<std::pair<int, cplx>> rowsum;
+        for (int i = lo; i < hi; ++i) {
+            rowsum.clear();
+            for (int k = ovr_ptr[i]; k < ovr_ptr[i + 1]; ++k) {
+                const int p = ovr_pos[k];
+                if (p < 0 || p >= P.nnzY) {
+                    bad[i] = 1;
+                    break;
                 }
-            if (!found) rowsum.push_back({r, dI});
+                const int r = P.Rrow[p], c = P.Rj[p];
+                const cplx dI = (ov[k] - P.Rx[p]) * V[c];
+                bool found = false;
+                for (auto &e : rowsum)
+                    if (e.first == r) {
+                        e.second += dI;
+                        found = true;
+                    }
+                if (!found) rowsum.push_back({r, dI});
+            }
+            double s = 0.0;
+            for (auto &e : rowsum) s = std::max(s, std::norm(V[e.first] * std::conj(e.second)));
+            score[i] = s;
         }
-        double s = 0.0;
-        for (auto &e : rowsum) s = std::max(s, std::abs(V[e.first] * std::conj(e.second)));
-        score[i] = s;
-    }
+    });
+    for (int i = 0; i < ninst; ++i)
+        if (bad[i]) return fail(-1, "pf_n1_order: override position out of range");
     for (int i = 0; i < ninst; ++i) order[i] = i;
     std::stable_sort(order, order + ninst, [&](int a, int b) { return score[a] > score[b]; });
     return 0;

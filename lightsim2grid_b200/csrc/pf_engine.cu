@@ -194,28 +194,68 @@ __device__ void mismatch(const DevPlan &P, Shared &S, const double2 *__restrict_
 }
 
 // dS/dVm and dS/dVa at V scattered into the LU array (and into Jout when requested).
-template <typename LT>
+// ZERO_ALL: the LU region (shared memory) is cleared whole with 16-byte stores before the
+// entries are written, in place of the gather of the fill-in positions.
+template <typename LT, bool ZERO_ALL>
 __device__ void jacobian_fill(const DevPlan &P, Shared &S, const double2 *__restrict__ V,
                               const double2 *__restrict__ Ibus, LT *lu, double *Jout) {
-    for (int p = threadIdx.x; p < P.nnzY; p += blockDim.x) {
-        const int r = P.Rrow[p], c = P.Rj[p];
-        double dvar, dvai;
-        double2 dvm;
-        dsbus(ybus_value(P, S, p), V[r], V[c], r == c, r == c ? Ibus[r] : make_double2(0.0, 0.0), dvar, dvai, dvm);
-        const int4 t = P.ytarget[p];
-        if (t.x >= 0) lu[t.x] = (LT)dvar;
-        if (t.y >= 0) lu[t.y] = (LT)dvai;
-        if (t.z >= 0) lu[t.z] = (LT)dvm.x;
-        if (t.w >= 0) lu[t.w] = (LT)dvm.y;
-        if (Jout) {
-            const int4 j = P.yjpos[p];
-            if (j.x >= 0) Jout[j.x] = dvar;
-            if (j.y >= 0) Jout[j.y] = dvai;
-            if (j.z >= 0) Jout[j.z] = dvm.x;
-            if (j.w >= 0) Jout[j.w] = dvm.y;
+    if constexpr (ZERO_ALL) {
+        // lu is 4-byte aligned; the head up to the first 16-byte boundary and the tail are scalar
+        const int head = (int)(((16 - ((size_t)lu & 15)) & 15) / sizeof(LT));
+        const int h = head < P.nnzLU ? head : P.nnzLU;
+        if ((int)threadIdx.x < h) lu[threadIdx.x] = (LT)0;
+        const int nvec = (P.nnzLU - h) * (int)sizeof(LT) / 16;
+        float4 *v4 = reinterpret_cast<float4 *>(lu + h);
+        for (int i = threadIdx.x; i < nvec; i += blockDim.x) v4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        const int t0 = h + nvec * 16 / (int)sizeof(LT);
+        if ((int)threadIdx.x < P.nnzLU - t0) lu[t0 + threadIdx.x] = (LT)0;
+        __syncthreads();
+    }
+    constexpr int U = 2;  // entries per thread whose loads are issued together
+    const int bd = blockDim.x;
+    for (int p0 = threadIdx.x; p0 < P.nnzY; p0 += U * bd) {
+        int r[U], c[U];
+        double2 y[U], vr[U], vc[U], ib[U];
+        int4 t[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int p = p0 + u * bd;
+            const bool ok = p < P.nnzY;
+            r[u] = ok ? P.Rrow[p] : 0;
+            c[u] = ok ? P.Rj[p] : 1;
+            t[u] = ok ? P.ytarget[p] : make_int4(-1, -1, -1, -1);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int p = p0 + u * bd;
+            const bool ok = p < P.nnzY;
+            y[u] = ok ? ybus_value(P, S, p) : make_double2(0.0, 0.0);
+            vr[u] = ok ? V[r[u]] : make_double2(1.0, 0.0);
+            vc[u] = ok ? V[c[u]] : make_double2(1.0, 0.0);
+            ib[u] = (ok && r[u] == c[u]) ? Ibus[r[u]] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int p = p0 + u * bd;
+            if (p >= P.nnzY) break;
+            double dvar, dvai;
+            double2 dvm;
+            dsbus(y[u], vr[u], vc[u], r[u] == c[u], ib[u], dvar, dvai, dvm);
+            if (t[u].x >= 0) lu[t[u].x] = (LT)dvar;
+            if (t[u].y >= 0) lu[t[u].y] = (LT)dvai;
+            if (t[u].z >= 0) lu[t[u].z] = (LT)dvm.x;
+            if (t[u].w >= 0) lu[t[u].w] = (LT)dvm.y;
+            if (Jout) {
+                const int4 j = P.yjpos[p];
+                if (j.x >= 0) Jout[j.x] = dvar;
+                if (j.y >= 0) Jout[j.y] = dvai;
+                if (j.z >= 0) Jout[j.z] = dvm.x;
+                if (j.w >= 0) Jout[j.w] = dvm.y;
+            }
         }
     }
-    for (int i = threadIdx.x; i < P.nfill; i += blockDim.x) lu[P.fillpos[i]] = (LT)0;
+    if constexpr (!ZERO_ALL)
+        for (int i = threadIdx.x; i < P.nfill; i += blockDim.x) lu[P.fillpos[i]] = (LT)0;
     for (int i = threadIdx.x; i < P.nconst; i += blockDim.x) {
         lu[P.cpos[i]] = (LT)P.cval[i];
         if (Jout) Jout[P.cjpos[i]] = P.cval[i];
@@ -349,10 +389,17 @@ __device__ __forceinline__ void run_lu_program(const uint2 *cops, const int4 *op
     }
 }
 
-// z(k) / U(k, k): the backward program keeps z undivided
-template <typename LT, typename XT>
-__device__ __forceinline__ void scale_by_pivots(const DevPlan &P, const LT *lu, XT *x) {
-    for (int k = threadIdx.x; k < P.m; k += blockDim.x) x[k] = lu_div(x[k], (XT)lu[P.dpos[k]]);
+// z(k) / U(k, k): the backward program keeps z undivided.  CHECK: a zero pivot also sets
+// S.piv_err (seen by every thread after the closing barrier).
+template <typename LT, typename XT, bool CHECK = false>
+__device__ __forceinline__ void scale_by_pivots(const DevPlan &P, Shared &S, const LT *lu, XT *x) {
+    int zero = 0;
+    for (int k = threadIdx.x; k < P.m; k += blockDim.x) {
+        const LT d = lu[P.dpos[k]];
+        if (CHECK) zero |= d == (LT)0;
+        x[k] = lu_div(x[k], (XT)d);
+    }
+    if (CHECK && zero) S.piv_err = 1;
     __syncthreads();
 }
 
@@ -370,24 +417,46 @@ template <typename XT>
 __device__ void newton_residual(const DevPlan &P, Shared &S, const double2 *__restrict__ V,
                                 const double2 *__restrict__ Ibus, const double2 *__restrict__ Fbus,
                                 const double *__restrict__ dxg, XT *x) {
+    // RU entries of a row at a time: their columns' step positions (ycol) load with the
+    // column indices, so one round of loads brings V, the step values and Y for all of them
+    constexpr int RU = 2;
     for (int r = threadIdx.x; r < P.n; r += blockDim.x) {
         const int ip = P.xP[r], iq = P.xQ[r];
         if (ip < 0 && iq < 0) continue;
         const double2 vr = V[r];
         double accP = 0.0, accQ = 0.0;
-        const int p1 = P.Rp[r + 1];
-        for (int p = P.Rp[r]; p < p1; ++p) {
-            const int c = P.Rj[p];
-            const int ia = P.xVa[c], im = P.xVm[c];
-            const double dA = ia >= 0 ? dxg[ia] : 0.0;
-            const double dM = im >= 0 ? dxg[im] : 0.0;
-            if (ia < 0 && im < 0) continue;
-            double dvar, dvai;
-            double2 dvm;
-            dsbus(ybus_value(P, S, p), vr, V[c], r == c, r == c ? Ibus[r] : make_double2(0.0, 0.0), dvar, dvai,
-                  dvm);
-            accP += dvar * dA + dvm.x * dM;
-            accQ += dvai * dA + dvm.y * dM;
+        const int p0 = P.Rp[r], p1 = P.Rp[r + 1];
+        for (int p = p0; p < p1; p += RU) {
+            int c[RU];
+            int2 xc[RU];
+#pragma unroll
+            for (int u = 0; u < RU; ++u) {
+                const bool ok = p + u < p1;
+                c[u] = ok ? P.Rj[p + u] : r;
+                xc[u] = ok ? P.ycol[p + u] : make_int2(-1, -1);
+            }
+            double2 y[RU], vc[RU];
+            double dA[RU], dM[RU];
+            bool diag = false;
+#pragma unroll
+            for (int u = 0; u < RU; ++u) {
+                const bool use = xc[u].x >= 0 || xc[u].y >= 0;
+                y[u] = use ? ybus_value(P, S, p + u) : make_double2(0.0, 0.0);
+                vc[u] = use ? V[c[u]] : make_double2(1.0, 0.0);
+                dA[u] = xc[u].x >= 0 ? dxg[xc[u].x] : 0.0;
+                dM[u] = xc[u].y >= 0 ? dxg[xc[u].y] : 0.0;
+                diag |= use && c[u] == r;
+            }
+            const double2 ib = diag ? Ibus[r] : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int u = 0; u < RU; ++u) {
+                if (xc[u].x < 0 && xc[u].y < 0) continue;
+                double dvar, dvai;
+                double2 dvm;
+                dsbus(y[u], vr, vc[u], r == c[u], r == c[u] ? ib : make_double2(0.0, 0.0), dvar, dvai, dvm);
+                accP += dvar * dA[u] + dvm.x * dM[u];
+                accQ += dvai * dA[u] + dvm.y * dM[u];
+            }
         }
         if (P.distributed && ip >= 0) accP += P.wJ[r] * dxg[P.xSlack];
         const double2 F = Fbus[r];
@@ -566,24 +635,25 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
             const bool reuse = REFINE && have_lu && Jout == nullptr && norm < A.reuse_below;
             tr.mark();
             if (!reuse) {
-                jacobian_fill<LT>(P, S, V, Ibus, lu, Jout);
+                jacobian_fill<LT, LU_SMEM>(P, S, V, Ibus, lu, Jout);
                 __syncthreads();
                 pr.mark(1);
                 // refactorisation with the forward substitution of the right-hand side fused in
                 run_lu_program<LT, XT, LU_SMEM>(P.fac_cops, P.fac_ops, L.sb_fac, L.sw_fac, P.fac_nph, m, lu, x, tr);
-                check_pivots<LT>(P, S, lu);
                 pr.mark(2);
-                if (S.piv_err) {
-                    err = 6;  // SolverReFactor
-                    break;
-                }
                 have_lu = true;
             } else {
                 run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr);
                 pr.mark(3);
             }
             run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr);
-            scale_by_pivots<LT, XT>(P, lu, x);
+            // a zero pivot of the refactorisation is detected here: the backward program ran on
+            // non-finite values, which are dropped with the step
+            scale_by_pivots<LT, XT, true>(P, S, lu, x);
+            if (S.piv_err) {
+                err = 6;  // SolverReFactor
+                break;
+            }
             pr.mark(4);
             if (refine_now) {
                 for (int k = tid; k < m; k += blockDim.x) dxg[k] = (double)x[k];
@@ -592,31 +662,56 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 __syncthreads();
                 run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr);
                 run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr);
-                scale_by_pivots<LT, XT>(P, lu, x);
+                scale_by_pivots<LT, XT>(P, S, lu, x);
                 pr.mark(5);
             }
             // voltage update
             double lmin = 1.0;
-            for (int b = tid; b < n; b += blockDim.x) {
-                double vm, va;
-                if (P.distributed) {
-                    vm = Vm[b];
-                    va = Va[b];
-                } else {
-                    const double2 v = V[b];
-                    vm = cabs2(v);
-                    va = atan2(v.y, v.x);
+            // pairs of buses: their loads (voltages, step positions, then the step
+            // values) are issued together before the arithmetic of the first bus
+            {
+                constexpr int R = 2;
+                const int bd = blockDim.x;
+                for (int b0 = tid; b0 < n; b0 += R * bd) {
+                    double vm[R], va[R];
+                    int ia[R], im[R];
+#pragma unroll
+                    for (int i = 0; i < R; ++i) {
+                        const int b = b0 + i * bd;
+                        const bool ok = b < n;
+                        ia[i] = ok ? P.xVa[b] : -1;
+                        im[i] = ok ? P.xVm[b] : -1;
+                        if (P.distributed) {
+                            vm[i] = ok ? Vm[b] : 1.0;
+                            va[i] = ok ? Va[b] : 0.0;
+                        } else {
+                            const double2 v = ok ? V[b] : make_double2(1.0, 0.0);
+                            vm[i] = cabs2(v);
+                            va[i] = atan2(v.y, v.x);
+                        }
+                    }
+                    double da[R], dm[R];
+#pragma unroll
+                    for (int i = 0; i < R; ++i) {
+                        da[i] = ia[i] >= 0 ? (refine_now ? dxg[ia[i]] + (double)x[ia[i]] : (double)x[ia[i]]) : 0.0;
+                        dm[i] = im[i] >= 0 ? (refine_now ? dxg[im[i]] + (double)x[im[i]] : (double)x[im[i]]) : 0.0;
+                    }
+#pragma unroll
+                    for (int i = 0; i < R; ++i) {
+                        const int b = b0 + i * bd;
+                        if (b >= n) break;
+                        double a = va[i], mg = vm[i];
+                        if (ia[i] >= 0) a -= da[i];
+                        if (im[i] >= 0) mg -= dm[i];
+                        double sn, cs;
+                        sincos(a, &sn, &cs);
+                        V[b] = make_double2(mg * cs, mg * sn);
+                        if (Vs) Vs[b] = make_double2(mg * cs, mg * sn);
+                        Vm[b] = mg;
+                        Va[b] = a;
+                        lmin = fmin(lmin, mg);
+                    }
                 }
-                const int ia = P.xVa[b], im = P.xVm[b];
-                if (ia >= 0) va -= refine_now ? dxg[ia] + (double)x[ia] : (double)x[ia];
-                if (im >= 0) vm -= refine_now ? dxg[im] + (double)x[im] : (double)x[im];
-                double sn, cs;
-                sincos(va, &sn, &cs);
-                V[b] = make_double2(vm * cs, vm * sn);
-                if (Vs) Vs[b] = make_double2(vm * cs, vm * sn);
-                Vm[b] = vm;
-                Va[b] = va;
-                lmin = fmin(lmin, vm);
             }
             if (P.distributed) {
                 const double dxs =
@@ -879,7 +974,7 @@ __global__ void __launch_bounds__(512, 1) dc_batch_kernel(const DevPlan P, const
             } else {
                 run_lu_program<double, double, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu,
                                                         x, tr);
-                scale_by_pivots<double, double>(P, lu, x);
+                scale_by_pivots<double, double>(P, S, lu, x);
                 double lmax = 0.0;
                 int lbad = 0;
                 for (int k = tid; k < m; k += blockDim.x) {
