@@ -382,13 +382,6 @@ int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl,
     size_t oyt = push(bi, P.ytarget), oyj = push(bi, P.yjpos);
     size_t ofill = push(bi, P.fillpos), ocpos = push(bi, P.cpos), ocj = push(bi, P.cjpos);
     size_t oxP = push(bi, P.xP), oxQ = push(bi, P.xQ), oxVa = push(bi, P.xVa), oxVm = push(bi, P.xVm);
-    std::vector<int> ycol(2 * (size_t)P.nnzY, -1);
-    if ((int)P.xVa.size() == P.n && (int)P.xVm.size() == P.n && (int)P.Rj.size() >= P.nnzY)
-        for (int p = 0; p < P.nnzY; ++p) {
-            ycol[2 * (size_t)p] = P.xVa[P.Rj[p]];
-            ycol[2 * (size_t)p + 1] = P.xVm[P.Rj[p]];
-        }
-    const size_t oycol = push(bi, ycol);
     size_t ofo = push(bi, P.factor.ops), ofb = push(bi, P.factor.base), ofw = push(bi, P.factor.width);
     size_t obo = push(bi, P.backward.ops), obb = push(bi, P.backward.base), obw = push(bi, P.backward.width);
     size_t owo = push(bi, P.forward.ops), owb = push(bi, P.forward.base), oww = push(bi, P.forward.width);
@@ -471,7 +464,6 @@ int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl,
     d.xQ = I(oxQ);
     d.xVa = I(oxVa);
     d.xVm = I(oxVm);
-    d.ycol = reinterpret_cast<const int2 *>(bI + oycol);
     d.xSlack = P.xSlack;
     d.wJ = D(owJ);
     d.fac_ops = I4(ofo);

@@ -411,67 +411,60 @@ __device__ void check_pivots(const DevPlan &P, Shared &S, const LT *lu) {
     __syncthreads();
 }
 
-// FP64 residual of the Newton system, F - J dx, written as the next right-hand side.
-// J dx is formed row by row from dS/dV (the FP64 Jacobian, never stored).
+// FP64 residual of the Newton system, F - J dx, written as the next right-hand side.  J is the
+// linearisation of S(V) = V conj(Y V) in the polar unknowns (the dS/dVa, dS/dVm of
+// BaseNRAlgo::_dSbus_dV, BaseNRAlgo.tpp:228-257), so J dx is formed from the voltage
+// step dV = V / |V| dVm + j V dVa:  J dx = dV conj(I) + V conj(Y dV)  (I = Y V, the current
+// injections of the mismatch), plus the slack-absorption column of a distributed slack.
+// Two passes: dV per bus into the slab, then one Ybus row product per equation row.
 template <typename XT>
 __device__ void newton_residual(const DevPlan &P, Shared &S, const double2 *__restrict__ V,
                                 const double2 *__restrict__ Ibus, const double2 *__restrict__ Fbus,
-                                const double *__restrict__ dxg, XT *x) {
-    // RU entries of a row at a time: their columns' step positions (ycol) load with the
-    // column indices, so one round of loads brings V, the step values and Y for all of them
-    constexpr int RU = 2;
-    for (int r = threadIdx.x; r < P.n; r += blockDim.x) {
+                                const double *__restrict__ dxg, double2 *__restrict__ dV, XT *x) {
+    const int bd = blockDim.x;
+    for (int b0 = threadIdx.x; b0 < P.n; b0 += 2 * bd) {
+        int ia[2], im[2];
+        double2 v[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int b = b0 + i * bd;
+            const bool ok = b < P.n;
+            ia[i] = ok ? P.xVa[b] : -1;
+            im[i] = ok ? P.xVm[b] : -1;
+            v[i] = ok ? V[b] : make_double2(1.0, 0.0);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int b = b0 + i * bd;
+            if (b >= P.n) break;
+            const double dA = ia[i] >= 0 ? dxg[ia[i]] : 0.0;
+            const double dM = im[i] >= 0 ? dxg[im[i]] / cabs2(v[i]) : 0.0;
+            dV[b] = make_double2(v[i].x * dM - v[i].y * dA, v[i].y * dM + v[i].x * dA);  // V (dM/|V| + j dA)
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < P.n; r += bd) {
         const int ip = P.xP[r], iq = P.xQ[r];
         if (ip < 0 && iq < 0) continue;
-        const double2 vr = V[r];
-        double accP = 0.0, accQ = 0.0;
-        const int p0 = P.Rp[r], p1 = P.Rp[r + 1];
-        for (int p = p0; p < p1; p += RU) {
-            int c[RU];
-            int2 xc[RU];
-#pragma unroll
-            for (int u = 0; u < RU; ++u) {
-                const bool ok = p + u < p1;
-                c[u] = ok ? P.Rj[p + u] : r;
-                xc[u] = ok ? P.ycol[p + u] : make_int2(-1, -1);
-            }
-            double2 y[RU], vc[RU];
-            double dA[RU], dM[RU];
-            bool diag = false;
-#pragma unroll
-            for (int u = 0; u < RU; ++u) {
-                const bool use = xc[u].x >= 0 || xc[u].y >= 0;
-                y[u] = use ? ybus_value(P, S, p + u) : make_double2(0.0, 0.0);
-                vc[u] = use ? V[c[u]] : make_double2(1.0, 0.0);
-                dA[u] = xc[u].x >= 0 ? dxg[xc[u].x] : 0.0;
-                dM[u] = xc[u].y >= 0 ? dxg[xc[u].y] : 0.0;
-                diag |= use && c[u] == r;
-            }
-            const double2 ib = diag ? Ibus[r] : make_double2(0.0, 0.0);
-#pragma unroll
-            for (int u = 0; u < RU; ++u) {
-                if (xc[u].x < 0 && xc[u].y < 0) continue;
-                double dvar, dvai;
-                double2 dvm;
-                dsbus(y[u], vr, vc[u], r == c[u], r == c[u] ? ib : make_double2(0.0, 0.0), dvar, dvai, dvm);
-                accP += dvar * dA[u] + dvm.x * dM[u];
-                accQ += dvai * dA[u] + dvm.y * dM[u];
-            }
-        }
-        if (P.distributed && ip >= 0) accP += P.wJ[r] * dxg[P.xSlack];
+        const double2 yd = ybus_row_product(P, S, dV, r);
+        const double2 vr = V[r], dvr = dV[r], ir = Ibus[r];
+        double jP = dvr.x * ir.x + dvr.y * ir.y + (vr.x * yd.x + vr.y * yd.y);
+        const double jQ = dvr.y * ir.x - dvr.x * ir.y + (vr.y * yd.x - vr.x * yd.y);
+        if (P.distributed && ip >= 0) jP += P.wJ[r] * dxg[P.xSlack];
         const double2 F = Fbus[r];
-        if (ip >= 0) x[ip] = (XT)(F.x - accP);
-        if (iq >= 0) x[iq] = (XT)(F.y - accQ);
+        if (ip >= 0) x[ip] = (XT)(F.x - jP);
+        if (iq >= 0) x[iq] = (XT)(F.y - jQ);
     }
 }
-
 // Where one plan's data lives for a CTA: shared memory x | LU (LU_SMEM: one index space, LU at
 // element lu_offset) | phase tables, and the CTA's slab of the scratch memory.
+// slab bytes per bus: V, Ibus, Fbus, the refinement's voltage step dV (16 B each), Vm, Va (8 B each)
+constexpr size_t kBusSlabBytes = 80;
 template <typename LT, typename XT>
 struct Layout {
     XT *x;
     LT *lu;
-    double2 *V, *Ibus, *Fbus;
+    double2 *V, *Ibus, *Fbus, *dV;
     double *Vm, *Va, *dxg;
     int *sb_fac, *sb_bwd, *sb_fwd, *sw_fac, *sw_bwd, *sw_fwd;
 };
@@ -486,10 +479,11 @@ __device__ __forceinline__ Layout<LT, XT> make_layout(const DevPlan &P, const Ba
     L.V = reinterpret_cast<double2 *>(slab);
     L.Ibus = L.V + n;
     L.Fbus = L.Ibus + n;
-    L.Vm = reinterpret_cast<double *>(L.Fbus + n);
+    L.dV = L.Fbus + n;
+    L.Vm = reinterpret_cast<double *>(L.dV + n);
     L.Va = L.Vm + n;
     L.dxg = L.Va + n;
-    const size_t bus_bytes = (((size_t)n * 64 + (size_t)m * 8) + 255) & ~(size_t)255;
+    const size_t bus_bytes = (((size_t)n * kBusSlabBytes + (size_t)m * 8) + 255) & ~(size_t)255;
     L.lu = LU_SMEM ? reinterpret_cast<LT *>(dyn + xbytes) : reinterpret_cast<LT *>(slab + bus_bytes);
     L.sb_fac = reinterpret_cast<int *>(dyn + xbytes +
                                        (LU_SMEM ? (((size_t)P.nnzLU * sizeof(LT) + 15) & ~(size_t)15) : 0));
@@ -658,7 +652,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
             if (refine_now) {
                 for (int k = tid; k < m; k += blockDim.x) dxg[k] = (double)x[k];
                 __syncthreads();
-                newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, x);
+                newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, L.dV, x);
                 __syncthreads();
                 run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr);
                 run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr);
@@ -1332,7 +1326,7 @@ cudaError_t launch_scatter_case_rows(const double2 *src, const int *errs, const 
 }
 
 size_t slab_bytes(const DevPlan &P, int lu_bytes, bool lu_in_smem) {
-    size_t bus = (((size_t)P.n * 64 + (size_t)P.m * 8) + 255) & ~(size_t)255;
+    size_t bus = (((size_t)P.n * kBusSlabBytes + (size_t)P.m * 8) + 255) & ~(size_t)255;
     size_t lu = lu_in_smem ? 0 : (((size_t)P.nnzLU * lu_bytes + 255) & ~(size_t)255);
     return bus + lu;
 }

@@ -22,7 +22,6 @@ struct DevPlan {
     const double *cval;
     int nconst;
     const int *xP, *xQ, *xVa, *xVm;
-    const int2 *ycol;        // per CSR position: (xVa, xVm) of its column
     int xSlack;
     const double *wJ;        // distributed slack: J(P(r), 0) per bus (0 if none)
     // phase programs (see pf_plan.hpp): operations as int4 (x, y, z, w | kind << 28) and

@@ -143,6 +143,8 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
     double *Vm = reinterpret_cast<double *>(q);
     q += al256((size_t)n * kLanes * 8);
     double *Va = reinterpret_cast<double *>(q);
+    q += al256((size_t)n * kLanes * 8);
+    double2 *dV = reinterpret_cast<double2 *>(q);  // the refinement's voltage step
     const bool prof = A.phase_cycles != nullptr;
     if (tid == 0) {
         S.exhausted = 0;
@@ -395,30 +397,35 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
                 if (refine)
                     for (int k = warp; k < m; k += kW) dxg[ix(k, lane)] = (double)x[ix(k, lane)];
                 __syncthreads();
+                // J dx = dV conj(I) + V conj(Y dV), dV = V / |V| dVm + j V dVa: the linearisation
+                // of S(V) = V conj(Y V) that the Jacobian holds (as the one-CTA kernel forms it)
+                if (refine)
+                    for (int b = warp; b < n; b += kW) {
+                        const int ia = P.xVa[b], im = P.xVm[b];
+                        const double2 v = V[ix(b, lane)];
+                        const double dA = ia >= 0 ? dxg[ix(ia, lane)] : 0.0;
+                        const double dM = im >= 0 ? dxg[ix(im, lane)] / cabs2(v) : 0.0;
+                        dV[ix(b, lane)] = make_double2(v.x * dM - v.y * dA, v.y * dM + v.x * dA);
+                    }
+                __syncthreads();
                 if (refine)
                     for (int r = warp; r < n; r += kW) {
                         const int ip = P.xP[r], iq = P.xQ[r];
                         if (ip < 0 && iq < 0) continue;
-                        const double2 vr = V[ix(r, lane)];
-                        double accP = 0.0, accQ = 0.0;
+                        double2 yd = make_double2(0.0, 0.0);
                         const int p1 = P.Rp[r + 1];
                         for (int p = P.Rp[r]; p < p1; ++p) {
-                            const int c = P.Rj[p];
-                            const int ia = P.xVa[c], im = P.xVm[c];
-                            if (ia < 0 && im < 0) continue;
-                            const double dA = ia >= 0 ? dxg[ix(ia, lane)] : 0.0;
-                            const double dM = im >= 0 ? dxg[ix(im, lane)] : 0.0;
-                            double dvar, dvai;
-                            double2 dvm;
-                            dsbus(ybus_lane(P, S, p, lane), vr, V[ix(c, lane)], r == c,
-                                  r == c ? Ib[ix(r, lane)] : make_double2(0.0, 0.0), dvar, dvai, dvm);
-                            accP += dvar * dA + dvm.x * dM;
-                            accQ += dvai * dA + dvm.y * dM;
+                            const double2 y = ybus_lane(P, S, p, lane), d = dV[ix(P.Rj[p], lane)];
+                            yd.x += y.x * d.x - y.y * d.y;
+                            yd.y += y.x * d.y + y.y * d.x;
                         }
-                        if (P.distributed && ip >= 0) accP += P.wJ[r] * dxg[ix(P.xSlack, lane)];
+                        const double2 vr = V[ix(r, lane)], dvr = dV[ix(r, lane)], ir = Ib[ix(r, lane)];
+                        double jP = dvr.x * ir.x + dvr.y * ir.y + (vr.x * yd.x + vr.y * yd.y);
+                        const double jQ = dvr.y * ir.x - dvr.x * ir.y + (vr.y * yd.x - vr.x * yd.y);
+                        if (P.distributed && ip >= 0) jP += P.wJ[r] * dxg[ix(P.xSlack, lane)];
                         const double2 F = Fb[ix(r, lane)];
-                        if (ip >= 0) x[ix(ip, lane)] = (LT)(F.x - accP);
-                        if (iq >= 0) x[ix(iq, lane)] = (LT)(F.y - accQ);
+                        if (ip >= 0) x[ix(ip, lane)] = (LT)(F.x - jP);
+                        if (iq >= 0) x[ix(iq, lane)] = (LT)(F.y - jQ);
                     }
                 __syncthreads();
                 tile_mark(S, prof, 5);
@@ -508,7 +515,7 @@ cudaError_t launch_tile_variant(const DevPlan &P, const BatchArgs &A, int grid, 
 size_t tile_slab_bytes(const DevPlan &P, int lu_bytes) {
     const size_t L = kLanes;
     return al256((size_t)(P.nnzLU + 1) * L * lu_bytes) + al256((size_t)P.m * L * lu_bytes) + al256((size_t)P.m * L * 8) +
-           3 * al256((size_t)P.n * L * 16) + 2 * al256((size_t)P.n * L * 8);
+           4 * al256((size_t)P.n * L * 16) + 2 * al256((size_t)P.n * L * 8);
 }
 
 size_t tile_smem_bytes(const DevPlan &P) { return (size_t)(P.fac_nph + P.bwd_nph + P.fwd_nph) * sizeof(int2); }
