@@ -22,7 +22,9 @@ typedef struct pf_plan pf_plan;
 typedef struct pf_options {
     int precision;          /* 0: FP64 LU and solves (plain form); 1: FP32 LU and solves with
                                FP64 mismatch, update and convergence test (mixed form)        */
-    int threads;            /* threads per CTA (multiple of 32, <= 512); 0: chosen by size   */
+    int threads;            /* threads per CTA (multiple of 32; Newton plans <= 768, DC and
+                               fast-decoupled plans <= 512); 0: chosen by size (768 for
+                               Newton plans of more than 4000 unknowns)                     */
     int lu_placement;       /* 0 auto, 1 shared memory, 2 global memory                      */
     int fuse_forward;       /* forward substitution fused into the refactorisation program.
                                0: default (on), 1: on, 2: off                                  */
@@ -41,8 +43,8 @@ typedef struct pf_options {
                                to 5e-8 pu from the FP64 ones instead of 3e-10               */
     int batch_layout;       /* Newton batches of independent instances (no time-series chain):
                                0 auto: batch-interleaved for plans whose LU stays in global
-                               memory with at least 40,000 entries (2,848 buses FP64, 6,515 buses)
-                               and 4 jobs per SM or more, else one CTA per instance; 1 one CTA
+                               memory with at least 60,000 entries (6,515 buses) and 4 jobs per
+                               SM or more, else one CTA per instance; 1 one CTA
                                per instance; 2
                                batch-interleaved: 32 instances per CTA, one per lane, every value
                                stored as 32 consecutive per-instance values (coalesced, the batch

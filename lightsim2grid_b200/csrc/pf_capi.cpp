@@ -627,10 +627,11 @@ void release(pf_plan *pl) {
 // chain), no per-launch diagnostics (J output, phase cycles or trace, LU reuse), and option
 // batch_layout 2, or auto (0) for plans whose LU stays in global memory and has at least
 // kAutoTileLU entries, with several jobs per SM.  Measured on all N-1 outages: 6,515 buses mixed
-// 77.1 against 105.6 ms, FP64 70.4 against 139.8 ms; 2,848 buses FP64 18.4 against 20.7 ms.  Where
-// the LU sits in shared memory (up to 2,848 buses mixed, 1,354 buses FP64) one CTA per instance
-// is faster (2,848 mixed: 11.2 against 20.8 ms).
-constexpr int kAutoTileLU = 40000;
+// 74.4 against 85.7 ms (one 768-thread CTA per instance), FP64 70 against 107 ms; 2,848 buses FP64
+// (48,682 LU entries) 17.6 against 17.5 ms, so it stays on one CTA per instance.  Where the LU
+// sits in shared memory (up to 2,848 buses mixed, 1,354 buses FP64) one CTA per instance is
+// faster (2,848 mixed: 9.4 against 20.4 ms).
+constexpr int kAutoTileLU = 60000;
 
 bool use_tile(const pf_plan *pl, const l2g::BatchArgs &a) {
     if (pl->P.dc || pl->P.fdpf || a.chain || a.Jout || a.trace || a.reuse_below > 0) return false;
@@ -1113,8 +1114,9 @@ int pf_plan_create(int n, const int *colptr, const int *rowind, const double *yb
     {
         const int m_est = npv + (distributed && nslack > 1 ? nslack - 1 : 0) + 2 * npq + (distributed ? 1 : 0);
         int thr = pl->opt.threads;
-        if (thr <= 0) thr = m_est > 2000 ? 512 : (m_est > 300 ? 256 : 128);
-        thr = std::max(32, std::min(512, (thr / 32) * 32));
+        // the largest plans run 768 threads (24 warps hide more of a phase's latency)
+        if (thr <= 0) thr = m_est > 4000 ? 768 : (m_est > 2000 ? 512 : (m_est > 300 ? 256 : 128));
+        thr = std::max(32, std::min(768, (thr / 32) * 32));
         po.threads = thr;
         pl->threads = thr;
     }

@@ -31,6 +31,7 @@ namespace {
 struct Shared {
     double red[32];
     int ired[32];
+    unsigned long long pc[kPhaseSlots];  // per-phase SM cycles (thread 0, when profiled)
     int opos[kMaxOverrides];
     double2 oval[kMaxOverrides];
     int novr;
@@ -456,6 +457,61 @@ __device__ void newton_residual(const DevPlan &P, Shared &S, const double2 *__re
         if (iq >= 0) x[iq] = (XT)(F.y - jQ);
     }
 }
+// The voltage update of a Newton step: Va -= dVa, Vm -= dVm (the FP32 step plus, when refined, the
+// FP64 first step), V = Vm e^(j Va) into the slab (and the shared copy Vs); returns the thread's
+// smallest new magnitude.  Pairs of buses: their loads (voltages, step positions, then the step
+// values) are issued together before the arithmetic of the first bus.
+template <typename XT>
+__device__ double voltage_update(const DevPlan &P, double2 *__restrict__ V, double2 *__restrict__ Vs,
+                                           double *__restrict__ Vm, double *__restrict__ Va,
+                                           const double *__restrict__ dxg, const XT *x, bool refine_now) {
+    const int n = P.n;
+    double lmin = 1.0;
+    constexpr int R = 2;
+    const int bd = blockDim.x;
+    for (int b0 = threadIdx.x; b0 < n; b0 += R * bd) {
+        double vm[R], va[R];
+        int ia[R], im[R];
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int b = b0 + i * bd;
+            const bool ok = b < n;
+            ia[i] = ok ? P.xVa[b] : -1;
+            im[i] = ok ? P.xVm[b] : -1;
+            if (P.distributed) {
+                vm[i] = ok ? Vm[b] : 1.0;
+                va[i] = ok ? Va[b] : 0.0;
+            } else {
+                const double2 v = ok ? V[b] : make_double2(1.0, 0.0);
+                vm[i] = cabs2(v);
+                va[i] = atan2(v.y, v.x);
+            }
+        }
+        double da[R], dm[R];
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            da[i] = ia[i] >= 0 ? (refine_now ? dxg[ia[i]] + (double)x[ia[i]] : (double)x[ia[i]]) : 0.0;
+            dm[i] = im[i] >= 0 ? (refine_now ? dxg[im[i]] + (double)x[im[i]] : (double)x[im[i]]) : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int b = b0 + i * bd;
+            if (b >= n) break;
+            double a = va[i], mg = vm[i];
+            if (ia[i] >= 0) a -= da[i];
+            if (im[i] >= 0) mg -= dm[i];
+            double sn, cs;
+            sincos(a, &sn, &cs);
+            V[b] = make_double2(mg * cs, mg * sn);
+            if (Vs) Vs[b] = make_double2(mg * cs, mg * sn);
+            Vm[b] = mg;
+            Va[b] = a;
+            lmin = fmin(lmin, mg);
+        }
+    }
+    return lmin;
+}
+
 // Where one plan's data lives for a CTA: shared memory x | LU (LU_SMEM: one index space, LU at
 // element lu_offset) | phase tables, and the CTA's slab of the scratch memory.
 // slab bytes per bus: V, Ibus, Fbus, the refinement's voltage step dV (16 B each), Vm, Va (8 B each)
@@ -511,12 +567,14 @@ struct Prof {
     bool on;
     int traced;
     unsigned long long tmark;
-    unsigned long long pc[kPhaseSlots];
-    __device__ __forceinline__ void start(bool o) {
+    unsigned long long *pc;  // Shared::pc: the counters stay out of the registers
+    __device__ __forceinline__ void start(bool o, unsigned long long *counters) {
         on = o;
         traced = 0;
+        pc = counters;
         tmark = o ? clock64() : 0;
-        for (int i = 0; i < kPhaseSlots; ++i) pc[i] = 0;
+        if (o)
+            for (int i = 0; i < kPhaseSlots; ++i) pc[i] = 0;
     }
     __device__ __forceinline__ void mark(int slot) {
         if (on) {
@@ -660,53 +718,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 pr.mark(5);
             }
             // voltage update
-            double lmin = 1.0;
-            // pairs of buses: their loads (voltages, step positions, then the step
-            // values) are issued together before the arithmetic of the first bus
-            {
-                constexpr int R = 2;
-                const int bd = blockDim.x;
-                for (int b0 = tid; b0 < n; b0 += R * bd) {
-                    double vm[R], va[R];
-                    int ia[R], im[R];
-#pragma unroll
-                    for (int i = 0; i < R; ++i) {
-                        const int b = b0 + i * bd;
-                        const bool ok = b < n;
-                        ia[i] = ok ? P.xVa[b] : -1;
-                        im[i] = ok ? P.xVm[b] : -1;
-                        if (P.distributed) {
-                            vm[i] = ok ? Vm[b] : 1.0;
-                            va[i] = ok ? Va[b] : 0.0;
-                        } else {
-                            const double2 v = ok ? V[b] : make_double2(1.0, 0.0);
-                            vm[i] = cabs2(v);
-                            va[i] = atan2(v.y, v.x);
-                        }
-                    }
-                    double da[R], dm[R];
-#pragma unroll
-                    for (int i = 0; i < R; ++i) {
-                        da[i] = ia[i] >= 0 ? (refine_now ? dxg[ia[i]] + (double)x[ia[i]] : (double)x[ia[i]]) : 0.0;
-                        dm[i] = im[i] >= 0 ? (refine_now ? dxg[im[i]] + (double)x[im[i]] : (double)x[im[i]]) : 0.0;
-                    }
-#pragma unroll
-                    for (int i = 0; i < R; ++i) {
-                        const int b = b0 + i * bd;
-                        if (b >= n) break;
-                        double a = va[i], mg = vm[i];
-                        if (ia[i] >= 0) a -= da[i];
-                        if (im[i] >= 0) mg -= dm[i];
-                        double sn, cs;
-                        sincos(a, &sn, &cs);
-                        V[b] = make_double2(mg * cs, mg * sn);
-                        if (Vs) Vs[b] = make_double2(mg * cs, mg * sn);
-                        Vm[b] = mg;
-                        Va[b] = a;
-                        lmin = fmin(lmin, mg);
-                    }
-                }
-            }
+            const double lmin = voltage_update<XT>(P, V, Vs, Vm, Va, dxg, x, refine_now);
             if (P.distributed) {
                 const double dxs =
                     refine_now ? dxg[P.xSlack] + (double)x[P.xSlack] : (double)x[P.xSlack];
@@ -739,7 +751,7 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
         if (tid == 0) {
             A.iters[inst] = it;
             A.errs[inst] = err;
-            pr.pc[7] += 1;
+            if (pr.on) pr.pc[7] += 1;
         }
         __syncthreads();
         if (A.chain && err != 0) {
@@ -764,14 +776,16 @@ __device__ __noinline__ void fp64_rerun(const DevPlan &P, const BatchArgs &A, Sh
     stage_tables<double, double>(P, L);
     __syncthreads();
     Prof pr;
-    pr.start(false);
+    pr.start(false, S.pc);
     solve_job<double, double, false, false>(P, A, S, L, first, count, pr);
 }
 
 // QUEUE: the device-resident request loop (jobs from M.q); a variant of its own so that the
 // other launches keep their registers.
-template <typename LT, typename XT, bool LU_SMEM, bool REFINE, bool QUEUE>
-__global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, const BatchArgs A0, const MultiArgs M) {
+// MAXT: the launch bound, 512 or 768 threads.  768 threads (24 warps) hide more of the phases'
+// latency than 512 at 80 instead of 128 registers: the large plans run with it.
+template <typename LT, typename XT, bool LU_SMEM, bool REFINE, bool QUEUE, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) nr_batch_kernel(const DevPlan P0, const BatchArgs A0, const MultiArgs M) {
     extern __shared__ __align__(16) unsigned char dyn[];
     __shared__ Shared S;
     // the plan and batch of the current job, in shared memory: a launch of one plan (M.segs
@@ -785,7 +799,7 @@ __global__ void __launch_bounds__(512, 1) nr_batch_kernel(const DevPlan P0, cons
     int *const counter = multi ? M.job_counter : A0.job_counter;
     const int njobs = multi ? M.njobs : (A0.njobs_dev ? min(A0.njobs, *A0.njobs_dev) : A0.njobs);
     Prof pr;
-    pr.start(A0.phase_cycles != nullptr && tid == 0);
+    pr.start(A0.phase_cycles != nullptr && tid == 0, S.pc);
     int cur = -1;
     Layout<LT, XT> L{};
     __shared__ QueueJob qjob;
@@ -1276,13 +1290,22 @@ __global__ void __launch_bounds__(MAXT, MINB) fdpf_batch_kernel(const DevPlan P0
     }
 }
 
+template <typename LT, typename XT, bool SM, bool RF, bool Q, int MAXT>
+cudaError_t launch_variant_t(const DevPlan &P, const BatchArgs &A, const MultiArgs &M, int threads, int grid,
+                             size_t smem, cudaStream_t st) {
+    cudaError_t e = allow_max_smem(reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, Q, MAXT>));
+    if (e != cudaSuccess) return e;
+    nr_batch_kernel<LT, XT, SM, RF, Q, MAXT><<<grid, threads, smem, st>>>(P, A, M);
+    return cudaGetLastError();
+}
+
+// threads above 512 take the 768-thread variant
 template <typename LT, typename XT, bool SM, bool RF, bool Q>
 cudaError_t launch_variant_q(const DevPlan &P, const BatchArgs &A, const MultiArgs &M, int threads, int grid,
                              size_t smem, cudaStream_t st) {
-    cudaError_t e = allow_max_smem(reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, Q>));
-    if (e != cudaSuccess) return e;
-    nr_batch_kernel<LT, XT, SM, RF, Q><<<grid, threads, smem, st>>>(P, A, M);
-    return cudaGetLastError();
+    if (threads > 768) return cudaErrorInvalidValue;
+    if (threads > 512) return launch_variant_t<LT, XT, SM, RF, Q, 768>(P, A, M, threads, grid, smem, st);
+    return launch_variant_t<LT, XT, SM, RF, Q, 512>(P, A, M, threads, grid, smem, st);
 }
 
 template <typename LT, typename XT, bool SM, bool RF>
@@ -1295,11 +1318,11 @@ cudaError_t launch_variant(const DevPlan &P, const BatchArgs &A, const MultiArgs
 template <typename LT, typename XT, bool SM, bool RF>
 int occupancy_variant(int threads, size_t smem) {
     int nb = 0;
-    if (allow_max_smem(reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, false>)) != cudaSuccess)
-        return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, nr_batch_kernel<LT, XT, SM, RF, false>, threads, smem) !=
-        cudaSuccess)
-        return 0;
+    if (threads > 768) return 0;
+    const void *fn = threads > 512 ? reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, false, 768>)
+                                   : reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, false, 512>);
+    if (allow_max_smem(fn) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess) return 0;
     return nb;
 }
 
