@@ -782,14 +782,15 @@ def run_ours(args):
             "error_vs_oracle": err_vs_oracle,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "nr_batch_kernel<float,float,1,1>",
+                         "kernel": "nr_batch_kernel<float,float,1,1,0,{}>".format(
+                             768 if mixed["dev"].plan.info()["threads"] > 512 else 512),
                          "algorithmic_bytes_per_launch": mixed["abytes"],
                          "algorithmic_bytes_per_instance_iteration": mixed["per_it"],
                          "kernel_ms": 1e3 * kt,
                          "binding": {
                              "resource": "not HBM: the LU and solve vector stay in shared memory and the slab in L2; "
-                                         "shared-memory wavefronts in the wide phases and the dependent phase "
-                                         "chain (one barrier per elimination level) set the time",
+                                         "the SM's issue and latency set the time (dependent ALU chains, L2 round "
+                                         "trips, one barrier per elimination level, shared-memory wavefronts)",
                              "dram_bytes_per_instance_iteration": prof.get("traffic_bytes_per_instance_iteration"),
                              "l2_bytes_per_instance_iteration": prof.get("l2_bytes_per_instance_iteration"),
                              "smem_wavefronts_per_instance_iteration": prof.get(
