@@ -498,6 +498,50 @@ int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl,
     return 0;
 }
 
+// Narrow phases of the packed programs that run on a few warps with their operations staged in
+// shared memory (DevPlan::nar_*): the factor's and the forward program's last phases and the
+// backward program's first ones, each at most kNarrowThreads wide, as many as `budget` bytes
+// of shared memory hold (factor first, then backward, then forward, each range grown from its
+// narrow end).  A phase there costs shared-memory latency and a barrier of those warps instead
+// of a block barrier that waits for the next operations' global loads.
+constexpr int kNarrowThreads = 128;
+
+void narrow_phases(const l2g::Plan &P, l2g::DevPlan &d, size_t budget) {
+    for (int k = 0; k < 3; ++k) d.nar_a[k] = d.nar_b[k] = d.nar_first[k] = 0;
+    for (int k = 0; k < 4; ++k) d.nar_off[k] = 0;
+    d.nar_warps = 0;
+    if (!d.compact) return;
+    const size_t slack = 16;  // alignment of the staged area
+    size_t left = budget > slack ? budget - slack : 0;
+    const l2g::Plan::Program *pr[3] = {&P.factor, &P.backward, &P.forward};
+    int widest = 0, off = 0;
+    for (int k = 0; k < 3; ++k) {
+        const l2g::Plan::Program &g = *pr[k];
+        const int nph = g.nphases();
+        int a = nph, b = nph;  // suffix [a, nph) for the factor and forward programs
+        if (k == 1) a = b = 0;  // prefix [0, b) for the backward program
+        for (;;) {
+            const int p = k == 1 ? b : a - 1;
+            if (p < 0 || p >= nph || g.width[p] > kNarrowThreads) break;
+            const size_t bytes = (size_t)(g.base[p + 1] - g.base[p]) * 8;
+            if (bytes > left) break;
+            left -= bytes;
+            widest = std::max(widest, g.width[p]);
+            if (k == 1) ++b;
+            else --a;
+        }
+        if (b - a < 2) a = b = 0;  // a single phase is not worth a range
+        d.nar_a[k] = a;
+        d.nar_b[k] = b;
+        d.nar_first[k] = b > a ? g.base[a] : 0;
+        d.nar_off[k] = off;
+        off += b > a ? g.base[b] - g.base[a] : 0;
+    }
+    d.nar_off[3] = off;
+    d.nar_warps = (widest + 31) / 32;
+    if (off == 0) d.nar_warps = 0;
+}
+
 int upload(pf_plan *pl) {
     int rc = upload_plan(pl->P, pl->dp, pl->d_int, pl->d_dbl, nullptr);
     if (rc || !pl->P.fdpf) return rc;
@@ -570,6 +614,10 @@ int configure(pf_plan *pl) {
         return fail(-1, "pf_plan_create: the solve vector does not fit in shared memory");
     pl->lu_in_smem = pl->opt.lu_placement == 2 ? false : fits;
     pl->smem = pl->lu_in_smem ? sm_in : sm_out;
+    if (pl->lu_in_smem && thr <= 512) {  // the 768-thread kernel runs every phase block-wide
+        narrow_phases(pl->P, pl->dp, (size_t)optin - static_smem - pl->smem);
+        pl->smem = l2g::smem_bytes(pl->dp, lub, xb, true);
+    }
     pl->slab = l2g::slab_bytes(pl->dp, lub, pl->lu_in_smem);
     pl->refine = pl->precision == 1 && pl->opt.refine != 2;
     int occ = l2g::nr_occupancy(pl->precision, pl->lu_in_smem, pl->refine, thr, pl->smem);

@@ -362,6 +362,26 @@ __device__ __forceinline__ void run_phase(const OP *__restrict__ ops, const int 
     tr.mark();
 }
 
+// Phases [a, b) of a program on the first `nwarps` warps: operations from the shared-memory copy
+// `sops` (the program's operations from phase a on), one barrier of those warps per phase (no
+// global load in flight at it), the other warps go straight to the closing block barrier.
+template <typename OP, typename F>
+__device__ __forceinline__ void run_narrow(const OP *sops, const int *sb, const int *sw, int a, int b, int nwarps,
+                                           F &&apply, Trace &tr) {
+    const int nt = nwarps * 32;
+    if ((int)threadIdx.x < nt) {
+        const int o0 = sb[a];
+        for (int p = a; p < b; ++p) {
+            const int w = sw[p], e = sb[p + 1] - o0;
+            if ((int)threadIdx.x < w)
+                for (int k = sb[p] - o0 + threadIdx.x; k < e; k += w) apply(sops[k]);
+            asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+            tr.mark();
+        }
+    }
+    __syncthreads();
+}
+
 template <typename OP, typename F>
 __device__ void run_program(const OP *__restrict__ ops, const int *sb, const int *sw, int nph, OP none, F &&apply,
                             Trace &tr) {
@@ -375,15 +395,44 @@ __device__ void run_program(const OP *__restrict__ ops, const int *sb, const int
     }
 }
 
+// The same with phases [na, nb) on the first `nwarps` warps (run_narrow): block-wide phases
+// [0, na), the narrow ones, block-wide [nb, nph).
+template <typename OP, typename F>
+__device__ void run_program_narrow(const OP *__restrict__ ops, const int *sb, const int *sw, int nph, OP none,
+                                   F &&apply, Trace &tr, int na, int nb, const OP *sops, int nwarps) {
+    if (nph <= 0) return;
+    if (nb <= na) na = nb = nph;
+    for (int part = 0; part < 2; ++part) {
+        const int from = part == 0 ? 0 : nb, to = part == 0 ? na : nph;
+        if (from < to) {
+            OpPair<OP> A, B;
+            load_first2<OP>(ops, sb, sw, to, from, A, none);
+            for (int p = from; p < to; p += 2) {
+                run_phase<OP>(ops, sb, sw, to, p, A, B, none, apply, tr);
+                if (p + 1 >= to) break;
+                run_phase<OP>(ops, sb, sw, to, p + 1, B, A, none, apply, tr);
+            }
+        }
+        if (part == 0 && na < nb) run_narrow<OP>(sops, sb, sw, na, nb, nwarps, apply, tr);
+    }
+}
+
 // One program over the LU layout of the kernel variant: packed operations over the shared
 // index space, or int4 operations over the global LU and the shared solve vector.
-template <typename LT, typename XT, bool LU_SMEM>
+// NARROW: `nar` is the narrow range of this program (phases [nar.x, nar.y) on nar.z warps,
+// operations staged at `sops`), packed layout only.
+template <typename LT, typename XT, bool LU_SMEM, bool NARROW = false>
 __device__ __forceinline__ void run_lu_program(const uint2 *cops, const int4 *ops, const int *sb, const int *sw,
-                                               int nph, int m, LT *lu, XT *x, Trace &tr) {
+                                               int nph, int m, LT *lu, XT *x, Trace &tr,
+                                               int3 nar = make_int3(0, 0, 0), const uint2 *sops = nullptr) {
     if constexpr (LU_SMEM) {
         static_assert(sizeof(LT) == sizeof(XT), "the packed layout needs one element type");
         const uint2 none = make_uint2((unsigned)m | ((unsigned)m << 16), (unsigned)m | ((unsigned)m << 16));
-        run_program<uint2>(cops, sb, sw, nph, none, [x](const uint2 o) { run_op_packed<XT>(o, x); }, tr);
+        if constexpr (NARROW)
+            run_program_narrow<uint2>(cops, sb, sw, nph, none, [x](const uint2 o) { run_op_packed<XT>(o, x); }, tr,
+                                      nar.x, nar.y, sops, nar.z);
+        else
+            run_program<uint2>(cops, sb, sw, nph, none, [x](const uint2 o) { run_op_packed<XT>(o, x); }, tr);
     } else {
         run_program<int4>(ops, sb, sw, nph, empty_op<int4>(), [lu, x](const int4 o) { run_op<LT, XT>(o, lu, x); },
                           tr);
@@ -523,6 +572,7 @@ struct Layout {
     double2 *V, *Ibus, *Fbus, *dV;
     double *Vm, *Va, *dxg;
     int *sb_fac, *sb_bwd, *sb_fwd, *sw_fac, *sw_bwd, *sw_fwd;
+    uint2 *nar_ops[3];  // staged operations of the narrow phases (packed layout)
 };
 
 template <typename LT, typename XT, bool LU_SMEM>
@@ -548,6 +598,12 @@ __device__ __forceinline__ Layout<LT, XT> make_layout(const DevPlan &P, const Ba
     L.sw_fac = L.sb_fwd + P.fwd_nph + 1;
     L.sw_bwd = L.sw_fac + P.fac_nph;
     L.sw_fwd = L.sw_bwd + P.bwd_nph;
+    {
+        // the narrow phases' operations after the tables, 8-byte aligned
+        const size_t off = (size_t)((reinterpret_cast<unsigned char *>(L.sw_fwd + P.fwd_nph) - dyn + 7) & ~(size_t)7);
+        uint2 *base = reinterpret_cast<uint2 *>(dyn + off);
+        for (int k = 0; k < 3; ++k) L.nar_ops[k] = base + P.nar_off[k];
+    }
     return L;
 }
 
@@ -560,6 +616,13 @@ __device__ __forceinline__ void stage_tables(const DevPlan &P, const Layout<LT, 
     for (int i = threadIdx.x; i < P.fac_nph; i += blockDim.x) L.sw_fac[i] = P.fac_width[i];
     for (int i = threadIdx.x; i < P.bwd_nph; i += blockDim.x) L.sw_bwd[i] = P.bwd_width[i];
     for (int i = threadIdx.x; i < P.fwd_nph; i += blockDim.x) L.sw_fwd[i] = P.fwd_width[i];
+    if (P.compact) {
+        const uint2 *cops[3] = {P.fac_cops, P.bwd_cops, P.fwd_cops};
+        for (int k = 0; k < 3; ++k) {
+            const int cnt = P.nar_off[k + 1] - P.nar_off[k];
+            for (int i = threadIdx.x; i < cnt; i += blockDim.x) L.nar_ops[k][i] = cops[k][P.nar_first[k] + i];
+        }
+    }
 }
 
 // Per-phase SM cycles, measured by thread 0 between the barriers that end each phase.
@@ -589,7 +652,9 @@ struct Prof {
 // inputs (start voltages, injections, overrides) are read through L2 only (ld.global.cg): in the
 // device-resident request loop one launch serves many requests whose inputs reuse device
 // addresses, and an SM's L1 could still hold an earlier request's lines.
-template <typename LT, typename XT, bool LU_SMEM, bool REFINE>
+// NARROW: the narrow phases of the packed programs run on their few warps (the 512-thread
+// variants; at 768 threads the registers it takes cost more than it saves).
+template <typename LT, typename XT, bool LU_SMEM, bool REFINE, bool NARROW>
 __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, Shared &S, const Layout<LT, XT> &L,
                                           int first, int count, Prof &pr) {
     const int tid = threadIdx.x;
@@ -691,14 +756,17 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 __syncthreads();
                 pr.mark(1);
                 // refactorisation with the forward substitution of the right-hand side fused in
-                run_lu_program<LT, XT, LU_SMEM>(P.fac_cops, P.fac_ops, L.sb_fac, L.sw_fac, P.fac_nph, m, lu, x, tr);
+                run_lu_program<LT, XT, LU_SMEM, NARROW>(P.fac_cops, P.fac_ops, L.sb_fac, L.sw_fac, P.fac_nph, m, lu, x, tr,
+                                                make_int3(P.nar_a[0], P.nar_b[0], P.nar_warps), L.nar_ops[0]);
                 pr.mark(2);
                 have_lu = true;
             } else {
-                run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr);
+                run_lu_program<LT, XT, LU_SMEM, NARROW>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr,
+                                                make_int3(P.nar_a[2], P.nar_b[2], P.nar_warps), L.nar_ops[2]);
                 pr.mark(3);
             }
-            run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr);
+            run_lu_program<LT, XT, LU_SMEM, NARROW>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr,
+                                            make_int3(P.nar_a[1], P.nar_b[1], P.nar_warps), L.nar_ops[1]);
             // a zero pivot of the refactorisation is detected here: the backward program ran on
             // non-finite values, which are dropped with the step
             scale_by_pivots<LT, XT, true>(P, S, lu, x);
@@ -712,8 +780,10 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 __syncthreads();
                 newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, L.dV, x);
                 __syncthreads();
-                run_lu_program<LT, XT, LU_SMEM>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr);
-                run_lu_program<LT, XT, LU_SMEM>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr);
+                run_lu_program<LT, XT, LU_SMEM, NARROW>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr,
+                                                make_int3(P.nar_a[2], P.nar_b[2], P.nar_warps), L.nar_ops[2]);
+                run_lu_program<LT, XT, LU_SMEM, NARROW>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr,
+                                            make_int3(P.nar_a[1], P.nar_b[1], P.nar_warps), L.nar_ops[1]);
                 scale_by_pivots<LT, XT>(P, S, lu, x);
                 pr.mark(5);
             }
@@ -777,7 +847,7 @@ __device__ __noinline__ void fp64_rerun(const DevPlan &P, const BatchArgs &A, Sh
     __syncthreads();
     Prof pr;
     pr.start(false, S.pc);
-    solve_job<double, double, false, false>(P, A, S, L, first, count, pr);
+    solve_job<double, double, false, false, false>(P, A, S, L, first, count, pr);
 }
 
 // QUEUE: the device-resident request loop (jobs from M.q); a variant of its own so that the
@@ -842,7 +912,7 @@ __global__ void __launch_bounds__(MAXT, 1) nr_batch_kernel(const DevPlan P0, con
         }
         const int first = queue ? qjob.first : (multi ? M.job_first[job] : A0.job_first[job]);
         const int count = queue ? qjob.count : (multi ? M.job_count[job] : A0.job_count[job]);
-        solve_job<LT, XT, LU_SMEM, REFINE>(seg.P, seg.A, S, L, first, count, pr);
+        solve_job<LT, XT, LU_SMEM, REFINE, (MAXT <= 512)>(seg.P, seg.A, S, L, first, count, pr);
         __syncthreads();
         if constexpr (REFINE) {
             if (seg.A.fp64_inline) {
@@ -1358,7 +1428,9 @@ size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem) 
     size_t xb = lu_in_smem ? (size_t)P.lu_offset * x_bytes : (((size_t)P.m * x_bytes + 15) & ~(size_t)15);
     size_t lb = lu_in_smem ? (((size_t)P.nnzLU * lu_bytes + 15) & ~(size_t)15) : 0;
     size_t bb = (size_t)(2 * (P.fac_nph + P.bwd_nph + P.fwd_nph) + 3) * sizeof(int);
-    return xb + lb + bb;
+    // staged operations of the narrow phases (make_layout places them after the tables)
+    const size_t nb = P.nar_off[3] > 0 ? (((xb + lb + bb + 7) & ~(size_t)7) - (xb + lb + bb)) + (size_t)P.nar_off[3] * 8 : 0;
+    return xb + lb + bb + nb;
 }
 
 template <bool SM>

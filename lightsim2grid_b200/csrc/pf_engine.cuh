@@ -33,6 +33,12 @@ struct DevPlan {
     // packed operations of the shared-memory layout (x and LU in one index space)
     int compact, lu_offset;
     const uint2 *fac_cops, *bwd_cops, *fwd_cops;
+    // narrow phases of the packed programs (shared-memory LU): phases [nar_a[k], nar_b[k]) of
+    // program k (0 factor, 1 backward, 2 forward) run on the first nar_warps warps only, between
+    // barriers of those warps, with their operations staged in shared memory once per plan
+    int nar_a[3], nar_b[3], nar_warps;
+    int nar_first[3];   // program k's operation index of the first staged operation (base[nar_a])
+    int nar_off[4];     // staged operations of program k at [nar_off[k], nar_off[k + 1])
     const int *dpos;         // pivot position per column (m)
     int dc, slack0;          // DC plan (B = Re(Ybus) without the slack) and its slack bus
     const double *luval;     // constant factor values (LU layout) of a fast-decoupled system
