@@ -23,8 +23,9 @@ typedef struct pf_options {
     int precision;          /* 0: FP64 LU and solves (plain form); 1: FP32 LU and solves with
                                FP64 mismatch, update and convergence test (mixed form)        */
     int threads;            /* threads per CTA (multiple of 32; Newton plans <= 768, DC and
-                               fast-decoupled plans <= 512); 0: chosen by size (768 for
-                               Newton plans of more than 4000 unknowns)                     */
+                               fast-decoupled plans <= 512); 0: chosen by size (Newton plans
+                               of more than 4000 unknowns: 640 in the mixed form, 768 in
+                               FP64)                                                        */
     int lu_placement;       /* 0 auto, 1 shared memory, 2 global memory                      */
     int fuse_forward;       /* forward substitution fused into the refactorisation program.
                                0: default (on), 1: on, 2: off                                  */

@@ -90,7 +90,7 @@ def schedule_candidates(m):
 
 def n1_candidates(m, n):
     """Candidates for N-1 batches of a grid with m unknowns and n buses."""
-    threads = (128, 256) if m < 600 else ((256, 512) if m < 4000 else (512, 768))
+    threads = (128, 256) if m < 600 else ((256, 512) if m < 4000 else (512, 640, 768))
     out = []
     for t in threads:
         for c in schedule_candidates(m):
@@ -172,7 +172,7 @@ def tune_n1(grid, branches, precision=1, candidates=None, repeat=3, device=None,
     return dict(best["options"]), table
 
 
-def tune_uneven(parts, precision=1, repeat=3, device=None, threads=(256, 512, 768), schedules=True):
+def tune_uneven(parts, precision=1, repeat=3, device=None, threads=(256, 512, 640, 768), schedules=True):
     """Picks the options of a launch over several grids (``parts``: (name, grid, branches)):
     for each grid the schedule options (elimination order and level slack, placement) that run
     its own sample fastest, then the launch's thread count with those.  Returns (options for

@@ -614,7 +614,7 @@ int configure(pf_plan *pl) {
         return fail(-1, "pf_plan_create: the solve vector does not fit in shared memory");
     pl->lu_in_smem = pl->opt.lu_placement == 2 ? false : fits;
     pl->smem = pl->lu_in_smem ? sm_in : sm_out;
-    if (pl->lu_in_smem && thr <= 512) {  // the 768-thread kernel runs every phase block-wide
+    if (pl->lu_in_smem && thr <= 640) {  // the 768-thread kernel runs every phase block-wide
         narrow_phases(pl->P, pl->dp, (size_t)optin - static_smem - pl->smem);
         pl->smem = l2g::smem_bytes(pl->dp, lub, xb, true);
     }
@@ -1162,8 +1162,9 @@ int pf_plan_create(int n, const int *colptr, const int *rowind, const double *yb
     {
         const int m_est = npv + (distributed && nslack > 1 ? nslack - 1 : 0) + 2 * npq + (distributed ? 1 : 0);
         int thr = pl->opt.threads;
-        // the largest plans run 768 threads (24 warps hide more of a phase's latency)
-        if (thr <= 0) thr = m_est > 4000 ? 768 : (m_est > 2000 ? 512 : (m_est > 300 ? 256 : 128));
+        // the largest plans run 640 (mixed form) or 768 threads (FP64 form)
+        if (thr <= 0)
+            thr = m_est > 4000 ? (pl->opt.precision ? 640 : 768) : (m_est > 2000 ? 512 : (m_est > 300 ? 256 : 128));
         thr = std::max(32, std::min(768, (thr / 32) * 32));
         po.threads = thr;
         pl->threads = thr;

@@ -652,8 +652,8 @@ struct Prof {
 // inputs (start voltages, injections, overrides) are read through L2 only (ld.global.cg): in the
 // device-resident request loop one launch serves many requests whose inputs reuse device
 // addresses, and an SM's L1 could still hold an earlier request's lines.
-// NARROW: the narrow phases of the packed programs run on their few warps (the 512-thread
-// variants; at 768 threads the registers it takes cost more than it saves).
+// NARROW: the narrow phases of the packed programs run on their few warps (the 512- and
+// 640-thread variants; at 768 threads the registers it takes cost more than it saves).
 template <typename LT, typename XT, bool LU_SMEM, bool REFINE, bool NARROW>
 __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, Shared &S, const Layout<LT, XT> &L,
                                           int first, int count, Prof &pr) {
@@ -852,8 +852,9 @@ __device__ __noinline__ void fp64_rerun(const DevPlan &P, const BatchArgs &A, Sh
 
 // QUEUE: the device-resident request loop (jobs from M.q); a variant of its own so that the
 // other launches keep their registers.
-// MAXT: the launch bound, 512 or 768 threads.  768 threads (24 warps) hide more of the phases'
-// latency than 512 at 80 instead of 128 registers: the large plans run with it.
+// MAXT: the launch bound, 512, 640 or 768 threads.  More warps hide more of the phases' latency
+// at fewer registers per thread (128, 96, 80): the large plans run 640 (mixed form, with the
+// narrow phases on a few warps) or 768 threads (FP64 form).
 template <typename LT, typename XT, bool LU_SMEM, bool REFINE, bool QUEUE, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1) nr_batch_kernel(const DevPlan P0, const BatchArgs A0, const MultiArgs M) {
     extern __shared__ __align__(16) unsigned char dyn[];
@@ -912,7 +913,7 @@ __global__ void __launch_bounds__(MAXT, 1) nr_batch_kernel(const DevPlan P0, con
         }
         const int first = queue ? qjob.first : (multi ? M.job_first[job] : A0.job_first[job]);
         const int count = queue ? qjob.count : (multi ? M.job_count[job] : A0.job_count[job]);
-        solve_job<LT, XT, LU_SMEM, REFINE, (MAXT <= 512)>(seg.P, seg.A, S, L, first, count, pr);
+        solve_job<LT, XT, LU_SMEM, REFINE, (MAXT <= 640)>(seg.P, seg.A, S, L, first, count, pr);
         __syncthreads();
         if constexpr (REFINE) {
             if (seg.A.fp64_inline) {
@@ -1369,12 +1370,13 @@ cudaError_t launch_variant_t(const DevPlan &P, const BatchArgs &A, const MultiAr
     return cudaGetLastError();
 }
 
-// threads above 512 take the 768-thread variant
+// the variant of the smallest launch bound (512, 640, 768) that covers `threads`
 template <typename LT, typename XT, bool SM, bool RF, bool Q>
 cudaError_t launch_variant_q(const DevPlan &P, const BatchArgs &A, const MultiArgs &M, int threads, int grid,
                              size_t smem, cudaStream_t st) {
     if (threads > 768) return cudaErrorInvalidValue;
-    if (threads > 512) return launch_variant_t<LT, XT, SM, RF, Q, 768>(P, A, M, threads, grid, smem, st);
+    if (threads > 640) return launch_variant_t<LT, XT, SM, RF, Q, 768>(P, A, M, threads, grid, smem, st);
+    if (threads > 512) return launch_variant_t<LT, XT, SM, RF, Q, 640>(P, A, M, threads, grid, smem, st);
     return launch_variant_t<LT, XT, SM, RF, Q, 512>(P, A, M, threads, grid, smem, st);
 }
 
@@ -1389,8 +1391,9 @@ template <typename LT, typename XT, bool SM, bool RF>
 int occupancy_variant(int threads, size_t smem) {
     int nb = 0;
     if (threads > 768) return 0;
-    const void *fn = threads > 512 ? reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, false, 768>)
-                                   : reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, false, 512>);
+    const void *fn = threads > 640   ? reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, false, 768>)
+                     : threads > 512 ? reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, false, 640>)
+                                     : reinterpret_cast<const void *>(nr_batch_kernel<LT, XT, SM, RF, false, 512>);
     if (allow_max_smem(fn) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess) return 0;
     return nb;
