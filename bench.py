@@ -842,6 +842,8 @@ def run_case(argv):
     ap.add_argument("--level-slack", type=int, default=0)
     ap.add_argument("--handoff-lanes", type=int, default=0)
     ap.add_argument("--no-trace", action="store_true", help="skip the phase-cycle and trace launches")
+    ap.add_argument("--cpu", action="store_true",
+                    help="also time the CPU oracle's N-1 loop on the same outages (all host threads)")
     args = ap.parse_args(argv)
 
     import torch
@@ -908,7 +910,20 @@ def run_case(argv):
         check = {"flags_equal": bool(np.array_equal(er == 0, ef == 0)),
                  "max_dV_vs_fp64": float(_dv(V[both], Vf[both]).max()) if both.any() else None,
                  "iterations_fp64": int(itf.sum())}
-    out = {"grid": args.grid, "cases": d.ns, "precision": args.precision, "ms": times, "check": check,
+    cpu = None
+    if args.cpu and not (args.dc or args.fdpf >= 0):
+        from oracle import oracle as orc
+
+        orc.build()
+        P = _host_threads()
+        ob = _oracle_batch(g, Vn, _n1_arrays(g, branches)[0])
+        ob.prepare(P)
+        ob.run(P)
+        ok, _, conv, _, _, dt = ob.run(P)
+        assert ok
+        cpu = {"pf_per_s": float(conv.sum() / dt), "ms": 1e3 * dt, "threads": P, "converged": int(conv.sum()),
+               "cpu_model": _cpu_model(), "kind": "port"}
+    out = {"grid": args.grid, "cases": d.ns, "precision": args.precision, "ms": times, "check": check, "cpu": cpu,
            "converged": int((er == 0).sum()), "iterations": int(it.sum()),
            "pf_per_s": float((er == 0).sum() / (np.mean(times) * 1e-3)),
            "cycles_per_iteration_per_cta": cpi, "phase_share": phase_share, "plan": d.plan.info(),

@@ -40,6 +40,16 @@ GRID_SIZES = {
 NAMED_SEEDS = {"grid14": 14, "grid118": 118, "grid300": 300, "grid1354": 1354, "grid2848": 2848,
                "grid6515": 6516}
 
+#: Higher-fill variants of the named grids, for sensitivity measurements: the same buses,
+#: branch count and PV count, but ``chords`` of the extra branches drawn uniformly at random
+#: among all unconnected bus pairs instead of from the nearest neighbours (long-range chords
+#: make the factor fill grow fast).  name -> (base grid, chords, seed).
+CHORD_GRIDS = {
+    "grid2848c100": ("grid2848", 100, 2848),
+    "grid2848c300": ("grid2848", 300, 2848),
+    "grid2848c929": ("grid2848", 929, 2848),
+}
+
 
 def _knn_pairs(pts, k):
     n = pts.shape[0]
@@ -90,8 +100,10 @@ def _graph_field(n, f, t, rng, n_smooth):
     return z / sd if sd > 0 else z
 
 
-def make_grid(n_bus, n_branch, n_pv, seed=0, knn=8, smooth=16):
-    """Build one seeded synthetic grid; returns ``(GridModel, V_true)``."""
+def make_grid(n_bus, n_branch, n_pv, seed=0, knn=8, smooth=16, chords=0):
+    """Build one seeded synthetic grid; returns ``(GridModel, V_true)``.  ``chords``: how many
+    of the extra branches are drawn uniformly at random among the bus pairs not yet connected
+    (long-range lines) instead of from the nearest-neighbour pairs."""
     if n_branch < n_bus - 1:
         raise ValueError("a connected grid needs at least n_bus - 1 branches")
     rng = np.random.default_rng(seed)
@@ -124,9 +136,17 @@ def make_grid(n_bus, n_branch, n_pv, seed=0, knn=8, smooth=16):
     n_extra = n_branch - (n_bus - 1)
     if n_extra > len(rest):
         raise ValueError("not enough nearest-neighbour pairs for {} extra branches".format(n_extra))
+    chords = min(max(int(chords), 0), n_extra)
     length = np.array([np.hypot(*(pts[a] - pts[b])) for (a, b) in rest])
     key = length * rng.uniform(0.5, 1.5, size=len(rest))
-    extra = [rest[i] for i in np.argsort(key, kind="stable")[:n_extra]]
+    extra = [rest[i] for i in np.argsort(key, kind="stable")[:n_extra - chords]]
+    used = set(tree) | set(extra)
+    while len(extra) < n_extra:
+        a, b = (int(v) for v in rng.integers(0, n_bus, size=2))
+        e = (min(a, b), max(a, b))
+        if a != b and e not in used:
+            used.add(e)
+            extra.append(e)
     edges = tree + extra
     perm = rng.permutation(len(edges))
     edges = [edges[i] for i in perm]
@@ -166,6 +186,10 @@ def make_grid(n_bus, n_branch, n_pv, seed=0, knn=8, smooth=16):
 
 
 def make_named_grid(name, seed=None):
+    if name in CHORD_GRIDS:
+        base, chords, s0 = CHORD_GRIDS[name]
+        n, nbr, npv = GRID_SIZES[base]
+        return make_grid(n, nbr, npv, seed=s0 if seed is None else seed, chords=chords)
     n, nbr, npv = GRID_SIZES[name]
     if seed is None:
         # default seed = bus count, except grid6515 whose seed 6515 draws a case that
