@@ -118,6 +118,8 @@ typedef struct pf_plan_info {
        for: per group of lanes the banks serve together and per operand, the most distinct
        words in one bank.  0 when the plan's LU is not in shared memory.                       */
     long long smem_wavefronts_factor, smem_wavefronts_backward, smem_wavefronts_forward;
+    /* steps of the dense tail (the trailing block factorised as one dense matrix), 0: none */
+    int tail_k;
 } pf_plan_info;
 
 /* A batch whose inputs and outputs are already in device memory (pointers from

@@ -34,7 +34,7 @@ class PfPlanInfo(ctypes.Structure):
                 ("lu_in_shared", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("grid", ctypes.c_int),
                 ("slab_bytes", ctypes.c_longlong), ("shared_bytes", ctypes.c_longlong),
                 ("smem_wavefronts_factor", ctypes.c_longlong), ("smem_wavefronts_backward", ctypes.c_longlong),
-                ("smem_wavefronts_forward", ctypes.c_longlong)]
+                ("smem_wavefronts_forward", ctypes.c_longlong), ("tail_k", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

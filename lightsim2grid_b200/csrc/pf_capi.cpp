@@ -411,6 +411,7 @@ int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl,
     size_t otfo = push(bi, tf.ops), otbo = push(bi, tb.ops), otwo = push(bi, tw.ops);
     size_t otfp = push(bi, tf.phase), otbp = push(bi, tb.phase), otwp = push(bi, tw.phase);
     size_t odpos = push(bi, P.dpos);
+    size_t otail = push(bi, P.tail_map);
     std::vector<double> rx(2 * (size_t)P.nnzY);
     for (int i = 0; i < P.nnzY; ++i) {
         rx[2 * i] = P.Rx[i].real();
@@ -495,6 +496,9 @@ int upload_plan(const l2g::Plan &P, l2g::DevPlan &d, void *&d_int, void *&d_dbl,
     d.tfac_phase = tiled ? I(otfp) : nullptr;
     d.tbwd_phase = tiled ? I(otbp) : nullptr;
     d.tfwd_phase = tiled ? I(otwp) : nullptr;
+    d.tail_ct = P.tail_k > 0 ? P.tail_ct : P.m;
+    d.tail_k = P.tail_k;
+    d.tail_map = P.tail_k > 0 ? I(otail) : nullptr;
     return 0;
 }
 
@@ -612,7 +616,9 @@ int configure(pf_plan *pl) {
     if (pl->opt.lu_placement == 1 && !fits) return fail(-1, "pf_plan_create: LU does not fit in shared memory");
     if (sm_out + static_smem > (size_t)optin)
         return fail(-1, "pf_plan_create: the solve vector does not fit in shared memory");
-    pl->lu_in_smem = pl->opt.lu_placement == 2 ? false : fits;
+    if (P.tail_k > 0 && pl->opt.lu_placement == 1)
+        return fail(-1, "pf_plan_create: a plan with a dense tail keeps its LU in global memory");
+    pl->lu_in_smem = pl->opt.lu_placement == 2 || P.tail_k > 0 ? false : fits;
     pl->smem = pl->lu_in_smem ? sm_in : sm_out;
     if (pl->lu_in_smem && thr <= 640) {  // the 768-thread kernel runs every phase block-wide
         narrow_phases(pl->P, pl->dp, (size_t)optin - static_smem - pl->smem);
@@ -683,6 +689,7 @@ constexpr int kAutoTileLU = 60000;
 
 bool use_tile(const pf_plan *pl, const l2g::BatchArgs &a) {
     if (pl->P.dc || pl->P.fdpf || a.chain || a.Jout || a.trace || a.reuse_below > 0) return false;
+    if (pl->P.tail_k > 0) return false;  // the dense tail runs in the one-CTA kernel
     if (pl->opt.batch_layout == 2) return true;
     return pl->opt.batch_layout == 0 && !pl->lu_in_smem && pl->P.nnzLU >= kAutoTileLU && a.njobs >= 4 * pl->num_sms;
 }
@@ -1324,6 +1331,7 @@ int pf_plan_info_get(const pf_plan *pl, pf_plan_info *info) {
     info->smem_wavefronts_factor = packed ? l2g::smem_wavefronts(P, P.factor) : 0;
     info->smem_wavefronts_backward = packed ? l2g::smem_wavefronts(P, P.backward) : 0;
     info->smem_wavefronts_forward = packed ? l2g::smem_wavefronts(P, P.forward) : 0;
+    info->tail_k = P.tail_k;
     return 0;
 }
 
@@ -1871,6 +1879,37 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
     auto scale = [&](std::vector<double> &v, const double *u) {
         for (int k = 0; k < m; ++k) v[k] = v[k] / u[P.dpos[k]];
     };
+    // the dense tail, as the kernel runs it: after the factor program the block is gathered and
+    // factorised without pivoting (unit lower L), its pivots written back to the LU diagonal; the
+    // block's forward substitution follows the factor (or forward) program, its backward
+    // substitution (undivided values, as the backward program) precedes the backward program
+    const int tk = P.tail_k, tc = P.tail_ct;
+    std::vector<double> D;
+    auto tail_factor = [&]() {
+        if (tk == 0) return;
+        D.assign((size_t)tk * tk, 0.0);
+        for (size_t e = 0; e < D.size(); ++e)
+            if (P.tail_map[e] >= 0) D[e] = lu[P.tail_map[e]];
+        for (int c = 0; c < tk; ++c) {
+            const double piv = D[(size_t)c * tk + c];
+            for (int i = c + 1; i < tk; ++i) {
+                const double l = D[(size_t)i * tk + c] / piv;
+                D[(size_t)i * tk + c] = l;
+                for (int j = c + 1; j < tk; ++j) D[(size_t)i * tk + j] -= l * D[(size_t)c * tk + j];
+            }
+        }
+        for (int c = 0; c < tk; ++c) lu[P.dpos[tc + c]] = D[(size_t)c * tk + c];
+    };
+    auto tail_forward = [&](std::vector<double> &v) {
+        for (int c = 0; c < tk; ++c)
+            for (int i = c + 1; i < tk; ++i) v[tc + i] -= D[(size_t)i * tk + c] * v[tc + c];
+    };
+    auto tail_backward = [&](std::vector<double> &v) {
+        for (int c = tk - 1; c >= 0; --c) {
+            const double w = v[tc + c] / D[(size_t)c * tk + c];
+            for (int i = 0; i < c; ++i) v[tc + i] -= D[(size_t)i * tk + c] * w;
+        }
+    };
     const std::vector<double> lu0 = lu, xs0 = xs;
     // the bank-conflict placement of the packed programs gives the same bits: every written
     // value keeps its thread and the order of its operations.  Checked for the placement of this
@@ -1930,13 +1969,17 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         }
     }
     run(P.factor);
+    tail_factor();
+    tail_forward(xs);
     for (int k = 0; k < m; ++k)
         if (lu[P.dpos[k]] == 0.0) return fail(l2g::SolverReFactor, "schedule check: zero pivot");
+    tail_backward(xs);
     run(P.backward);
     scale(xs, lu.data());
     // the instance-interleaved batch programs (groups per warp, chunk after chunk) give the same
-    // bits: every written value sees its operations in the same order
-    {
+    // bits: every written value sees its operations in the same order (plans without a dense
+    // tail: the interleaved kernel runs those only)
+    if (tk == 0) {
         std::vector<double> lt = lu0, xt = xs0;
         auto run_tile = [&](const l2g::Plan::Program &pr, std::vector<double> &v) {
             l2g::TileProgram tp;
@@ -1972,7 +2015,7 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         for (int k = 0; k < m; ++k)
             if (y3[k] != y4[k]) return fail(-1, "schedule check: batch-interleaved forward program disagrees");
     }
-    if (!s0.empty()) {
+    if (!s0.empty() && tk == 0) {
         const int L = l2g::compact_lu_offset(m);
         run_packed(P.factor);
         run_packed(P.backward);
@@ -1992,6 +2035,8 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         for (int f = 0; f < m; ++f) y2[P.pinv[f]] = b[f];
         xs = y2;
         run(P.forward);
+        tail_forward(xs);
+        tail_backward(xs);
         run(P.backward);
         scale(xs, lu.data());
         double dmax = 0.0, amax = 0.0;
@@ -2022,6 +2067,7 @@ int pf_host_schedule_solve(int n, const int *colptr, const int *rowind, const do
         info->smem_wavefronts_factor = l2g::smem_wavefronts(P, P.factor);
         info->smem_wavefronts_backward = l2g::smem_wavefronts(P, P.backward);
         info->smem_wavefronts_forward = l2g::smem_wavefronts(P, P.forward);
+        info->tail_k = P.tail_k;
     }
     return 0;
 }

@@ -29,7 +29,7 @@ namespace {
 
 
 struct Shared {
-    double red[32];
+    double red[32];  // block reductions; the dense tail's backward substitution (one panel's values)
     int ired[32];
     unsigned long long pc[kPhaseSlots];  // per-phase SM cycles (thread 0, when profiled)
     int opos[kMaxOverrides];
@@ -561,6 +561,222 @@ __device__ double voltage_update(const DevPlan &P, double2 *__restrict__ V, doub
     return lmin;
 }
 
+
+// ---------------------------------------------------------------- dense tail
+// The trailing block of steps [tail_ct, tail_ct + k) of a plan with a dense tail, as a dense
+// row-major k x k matrix D in the CTA's slab (row stride tail_ld(k), a multiple of 4 values, so
+// that every row starts on 16 bytes).  After the factor program has applied the pivots before
+// the block (their updates of the block are the Schur complement of the sparse part),
+// tail_factor gathers the block from the LU and factorises it without pivoting, right-looking
+// in panels of tail_panel<LT>() columns: (a) the panel (rows [J, k)) staged in shared memory and
+// factorised there, one barrier per pivot; then, chunk after chunk of kTailChunk columns right of
+// the panel, (b) their U rows staged in shared memory and solved there (L of the panel's
+// diagonal block is unit lower) and (c) the trailing rows minus L U, each thread a register tile
+// of outputs read and written with 16-byte accesses.  Its pivots go back to the LU diagonal,
+// where the pivot scaling and the zero-pivot check read them.  Shared memory:
+// tail_smem_bytes(k) (the staging area also serves the substitutions' diagonal blocks).
+constexpr int kTailChunk = 128;
+template <typename LT>
+__host__ __device__ constexpr int tail_panel() { return sizeof(LT) == 4 ? 32 : 16; }
+__host__ __device__ inline int tail_ld(int k) { return (k + 3) & ~3; }
+__host__ __device__ inline size_t tail_smem_bytes(int k, int lu_bytes) {
+    const int nb = lu_bytes == 4 ? 32 : 16;
+    // the panel (k rows of nb + 1 values), then the chunk of U rows from a 16-byte boundary
+    return k > 0 ? ((((size_t)k * (nb + 1) + 3) & ~(size_t)3) + (size_t)nb * kTailChunk) * lu_bytes : 0;
+}
+
+// four consecutive values at a 16-byte boundary
+__device__ __forceinline__ void ld4(const float *p, float (&v)[4]) {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ld4(const double *p, double (&v)[4]) {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void st4(float *p, const float (&v)[4]) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double *p, const double (&v)[4]) {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+
+template <typename LT>
+__device__ __noinline__ void tail_factor(const DevPlan &P, LT *lu, LT *D, LT *sm) {
+    constexpr int NB = tail_panel<LT>();
+    constexpr int NP = NB + 1;  // panel row stride: the rows of one column fall in different banks
+    constexpr int TR = sizeof(LT) == 4 ? 4 : 2, TC = 4;  // register tile of the trailing update
+    const int k = P.tail_k, ld = tail_ld(k), tid = threadIdx.x, bd = blockDim.x;
+    const int kk = k * k;
+    // gather, four entries per thread in flight
+    for (int e0 = tid; e0 < kk; e0 += 4 * bd) {
+        int p[4];
+        LT v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) p[u] = e0 + u * bd < kk ? P.tail_map[e0 + u * bd] : -1;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = p[u] >= 0 ? lu[p[u]] : (LT)0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = e0 + u * bd;
+            if (e < kk) D[(size_t)(e / k) * ld + e % k] = v[u];
+        }
+    }
+    __syncthreads();
+    LT *Ap = sm;                     // panel: Ap[(i - J) * NP + c], rows [J, k)
+    // U rows of the panel, one chunk: Bc[c * kTailChunk + q], from a 16-byte boundary (read with
+    // 16-byte loads; sm itself is 16-byte aligned)
+    LT *Bc = sm + (((size_t)k * NP + 3) & ~(size_t)3);
+    for (int J = 0; J < k; J += NB) {
+        const int jb = min(NB, k - J), J1 = J + jb, rows = k - J;
+        for (int e = tid; e < rows * NB; e += bd) {
+            const int i = e / NB, c = e - i * NB;
+            Ap[i * NP + c] = c < jb ? D[(size_t)(J + i) * ld + J + c] : (LT)0;
+        }
+        __syncthreads();
+        // (a) the panel, pivot after pivot
+        for (int c = 0; c < jb; ++c) {
+            const LT piv = Ap[c * NP + c];
+            for (int i = c + 1 + tid; i < rows; i += bd) {
+                LT *row = Ap + (size_t)i * NP;
+                const LT l = row[c] / piv;
+                row[c] = l;
+                for (int j = c + 1; j < jb; ++j) row[j] -= l * Ap[c * NP + j];
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < rows * NB; e += bd) {
+            const int i = e / NB, c = e - i * NB;
+            if (c < jb) D[(size_t)(J + i) * ld + J + c] = Ap[i * NP + c];
+        }
+        if (J1 >= k) break;
+        const int M = k - J1, tr = (M + TR - 1) / TR;
+        for (int j0 = J1; j0 < k; j0 += kTailChunk) {
+            const int w = min(kTailChunk, k - j0), tc = (w + TC - 1) / TC;
+            for (int e = tid; e < NB * kTailChunk; e += bd) {
+                const int c = e / kTailChunk, q = e - c * kTailChunk;
+                Bc[e] = (c < jb && q < w) ? D[(size_t)(J + c) * ld + j0 + q] : (LT)0;
+            }
+            __syncthreads();
+            // (b) the chunk's U rows, one thread per column
+            for (int q = tid; q < w; q += bd)
+                for (int c = 0; c < jb; ++c) {
+                    const LT u = Bc[c * kTailChunk + q];
+                    for (int i = c + 1; i < jb; ++i) Bc[i * kTailChunk + q] -= Ap[i * NP + c] * u;
+                }
+            __syncthreads();
+            for (int e = tid; e < jb * kTailChunk; e += bd) {
+                const int c = e / kTailChunk, q = e - c * kTailChunk;
+                if (q < w) D[(size_t)(J + c) * ld + j0 + q] = Bc[e];
+            }
+            // (c) the trailing rows: a tile of TR rows x 4 columns per thread (columns past the
+            // block's last fall in the row padding; their values are never read as entries)
+            for (int t = tid; t < tr * tc; t += bd) {
+                const int ti = t / tc, tj = t - ti * tc;
+                const int i0 = J1 + ti * TR, q0 = tj * TC;
+                LT acc[TR][TC];
+#pragma unroll
+                for (int r = 0; r < TR; ++r) {
+                    if (i0 + r < k) ld4(D + (size_t)(i0 + r) * ld + j0 + q0, acc[r]);
+                    else acc[r][0] = acc[r][1] = acc[r][2] = acc[r][3] = (LT)0;
+                }
+                const LT *arow = Ap + (size_t)(i0 - J) * NP;
+#pragma unroll 4
+                for (int c = 0; c < NB; ++c) {
+                    LT a[TR], bq[TC];
+#pragma unroll
+                    for (int r = 0; r < TR; ++r) a[r] = i0 + r < k ? arow[r * NP + c] : (LT)0;
+                    ld4(Bc + c * kTailChunk + q0, bq);
+#pragma unroll
+                    for (int r = 0; r < TR; ++r)
+#pragma unroll
+                        for (int q = 0; q < TC; ++q) acc[r][q] -= a[r] * bq[q];
+                }
+#pragma unroll
+                for (int r = 0; r < TR; ++r)
+                    if (i0 + r < k) st4(D + (size_t)(i0 + r) * ld + j0 + q0, acc[r]);
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    for (int c = tid; c < k; c += bd) lu[P.dpos[P.tail_ct + c]] = D[(size_t)c * ld + c];
+    __syncthreads();
+}
+
+// Forward substitution of the block (unit lower L of tail_factor) on x[tail_ct, tail_ct + k),
+// after the forward pushes of the pivots before the block: per panel of 32 rows, the diagonal
+// block staged in shared memory (`sm`, row stride 33), warp 0 solves it (a lane per row, values exchanged by
+// shuffles), then every thread updates rows below it.
+template <typename LT, typename XT>
+__device__ __noinline__ void tail_forward(const DevPlan &P, const LT *D, XT *x, LT *sm) {
+    const int k = P.tail_k, ld = tail_ld(k), tid = threadIdx.x, bd = blockDim.x;
+    XT *xt = x + P.tail_ct;
+    for (int J = 0; J < k; J += 32) {
+        const int jb = min(32, k - J), J1 = J + jb;
+        for (int e = tid; e < jb * 32; e += bd) {
+            const int a = e >> 5, b = e & 31;
+            sm[a * 33 + b] = b < jb ? D[(size_t)(J + a) * ld + J + b] : (LT)0;
+        }
+        __syncthreads();
+        if (tid < 32) {
+            XT v = tid < jb ? xt[J + tid] : (XT)0;
+            for (int c = 0; c < jb; ++c) {
+                const XT vc = __shfl_sync(0xffffffffu, v, c);
+                if (tid > c && tid < jb) v -= (XT)sm[tid * 33 + c] * vc;
+            }
+            if (tid < jb) xt[J + tid] = v;
+        }
+        __syncthreads();
+        for (int i = J1 + tid; i < k; i += bd) {
+            XT v = xt[i];
+            const LT *row = D + (size_t)i * ld + J;
+            for (int c = 0; c < jb; ++c) v -= (XT)row[c] * xt[J + c];
+            xt[i] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// Backward substitution of the block, before the backward program, in its convention: the values
+// stay undivided (z(c) = U(c, c) x(c)) and a push divides by the pivot; the pivot scaling after
+// the program divides them.  Per panel from the last: the diagonal block staged in shared
+// memory, warp 0 solves it and leaves the panel's z(c) / U(c, c) in S.red, then every thread
+// updates the rows above it.
+template <typename LT, typename XT>
+__device__ __noinline__ void tail_backward(const DevPlan &P, Shared &S, const LT *D, XT *x, LT *sm) {
+    const int k = P.tail_k, ld = tail_ld(k), tid = threadIdx.x, bd = blockDim.x;
+    XT *xt = x + P.tail_ct;
+    const int last = ((k - 1) / 32) * 32;
+    for (int J = last; J >= 0; J -= 32) {
+        const int jb = min(32, k - J);
+        for (int e = tid; e < jb * 32; e += bd) {
+            const int a = e >> 5, b = e & 31;
+            sm[a * 33 + b] = b < jb ? D[(size_t)(J + a) * ld + J + b] : (LT)0;
+        }
+        __syncthreads();
+        if (tid < 32) {
+            XT z = tid < jb ? xt[J + tid] : (XT)0;
+            for (int c = jb - 1; c >= 0; --c) {
+                const XT zc = __shfl_sync(0xffffffffu, z, c);
+                const XT w = zc / (XT)sm[c * 33 + c];
+                if (tid == c) S.red[c] = (double)w;
+                if (tid < c) z -= (XT)sm[tid * 33 + c] * w;
+            }
+            if (tid < jb) xt[J + tid] = z;
+        }
+        __syncthreads();
+        for (int i = tid; i < J; i += bd) {
+            XT v = xt[i];
+            const LT *row = D + (size_t)i * ld + J;
+            for (int c = 0; c < jb; ++c) v -= (XT)row[c] * (XT)S.red[c];
+            xt[i] = v;
+        }
+        __syncthreads();
+    }
+}
+
 // Where one plan's data lives for a CTA: shared memory x | LU (LU_SMEM: one index space, LU at
 // element lu_offset) | phase tables, and the CTA's slab of the scratch memory.
 // slab bytes per bus: V, Ibus, Fbus, the refinement's voltage step dV (16 B each), Vm, Va (8 B each)
@@ -569,6 +785,8 @@ template <typename LT, typename XT>
 struct Layout {
     XT *x;
     LT *lu;
+    LT *D;    // dense tail block (global-memory LU plans with a tail)
+    LT *tsm;  // its staging area in shared memory
     double2 *V, *Ibus, *Fbus, *dV;
     double *Vm, *Va, *dxg;
     int *sb_fac, *sb_bwd, *sb_fwd, *sw_fac, *sw_bwd, *sw_fwd;
@@ -591,6 +809,8 @@ __device__ __forceinline__ Layout<LT, XT> make_layout(const DevPlan &P, const Ba
     L.dxg = L.Va + n;
     const size_t bus_bytes = (((size_t)n * kBusSlabBytes + (size_t)m * 8) + 255) & ~(size_t)255;
     L.lu = LU_SMEM ? reinterpret_cast<LT *>(dyn + xbytes) : reinterpret_cast<LT *>(slab + bus_bytes);
+    L.D = LU_SMEM ? nullptr
+                  : reinterpret_cast<LT *>(slab + bus_bytes + (((size_t)P.nnzLU * sizeof(LT) + 255) & ~(size_t)255));
     L.sb_fac = reinterpret_cast<int *>(dyn + xbytes +
                                        (LU_SMEM ? (((size_t)P.nnzLU * sizeof(LT) + 15) & ~(size_t)15) : 0));
     L.sb_bwd = L.sb_fac + P.fac_nph + 1;
@@ -603,6 +823,8 @@ __device__ __forceinline__ Layout<LT, XT> make_layout(const DevPlan &P, const Ba
         const size_t off = (size_t)((reinterpret_cast<unsigned char *>(L.sw_fwd + P.fwd_nph) - dyn + 7) & ~(size_t)7);
         uint2 *base = reinterpret_cast<uint2 *>(dyn + off);
         for (int k = 0; k < 3; ++k) L.nar_ops[k] = base + P.nar_off[k];
+        // the dense tail's staging area after the tables, 16-byte aligned (global-memory LU)
+        L.tsm = LU_SMEM ? nullptr : reinterpret_cast<LT *>(dyn + ((off + 15) & ~(size_t)15));
     }
     return L;
 }
@@ -758,12 +980,24 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 // refactorisation with the forward substitution of the right-hand side fused in
                 run_lu_program<LT, XT, LU_SMEM, NARROW>(P.fac_cops, P.fac_ops, L.sb_fac, L.sw_fac, P.fac_nph, m, lu, x, tr,
                                                 make_int3(P.nar_a[0], P.nar_b[0], P.nar_warps), L.nar_ops[0]);
+                if constexpr (!LU_SMEM) {
+                    if (P.tail_k > 0) {
+                        tail_factor<LT>(P, lu, L.D, L.tsm);
+                        tail_forward<LT, XT>(P, L.D, x, L.tsm);
+                    }
+                }
                 pr.mark(2);
                 have_lu = true;
             } else {
                 run_lu_program<LT, XT, LU_SMEM, NARROW>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr,
                                                 make_int3(P.nar_a[2], P.nar_b[2], P.nar_warps), L.nar_ops[2]);
+                if constexpr (!LU_SMEM) {
+                    if (P.tail_k > 0) tail_forward<LT, XT>(P, L.D, x, L.tsm);
+                }
                 pr.mark(3);
+            }
+            if constexpr (!LU_SMEM) {
+                if (P.tail_k > 0) tail_backward<LT, XT>(P, S, L.D, x, L.tsm);
             }
             run_lu_program<LT, XT, LU_SMEM, NARROW>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr,
                                             make_int3(P.nar_a[1], P.nar_b[1], P.nar_warps), L.nar_ops[1]);
@@ -782,6 +1016,12 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 __syncthreads();
                 run_lu_program<LT, XT, LU_SMEM, NARROW>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr,
                                                 make_int3(P.nar_a[2], P.nar_b[2], P.nar_warps), L.nar_ops[2]);
+                if constexpr (!LU_SMEM) {
+                    if (P.tail_k > 0) {
+                        tail_forward<LT, XT>(P, L.D, x, L.tsm);
+                        tail_backward<LT, XT>(P, S, L.D, x, L.tsm);
+                    }
+                }
                 run_lu_program<LT, XT, LU_SMEM, NARROW>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr,
                                             make_int3(P.nar_a[1], P.nar_b[1], P.nar_warps), L.nar_ops[1]);
                 scale_by_pivots<LT, XT>(P, S, lu, x);
@@ -1424,7 +1664,9 @@ cudaError_t launch_scatter_case_rows(const double2 *src, const int *errs, const 
 size_t slab_bytes(const DevPlan &P, int lu_bytes, bool lu_in_smem) {
     size_t bus = (((size_t)P.n * kBusSlabBytes + (size_t)P.m * 8) + 255) & ~(size_t)255;
     size_t lu = lu_in_smem ? 0 : (((size_t)P.nnzLU * lu_bytes + 255) & ~(size_t)255);
-    return bus + lu;
+    // the dense tail block after the LU (global-memory LU plans only)
+    size_t tail = lu_in_smem ? 0 : (((size_t)P.tail_k * (size_t)tail_ld(P.tail_k) * lu_bytes + 255) & ~(size_t)255);
+    return bus + lu + tail;
 }
 
 size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem) {
@@ -1433,6 +1675,9 @@ size_t smem_bytes(const DevPlan &P, int lu_bytes, int x_bytes, bool lu_in_smem) 
     size_t bb = (size_t)(2 * (P.fac_nph + P.bwd_nph + P.fwd_nph) + 3) * sizeof(int);
     // staged operations of the narrow phases (make_layout places them after the tables)
     const size_t nb = P.nar_off[3] > 0 ? (((xb + lb + bb + 7) & ~(size_t)7) - (xb + lb + bb)) + (size_t)P.nar_off[3] * 8 : 0;
+    // the dense tail's staging area, 16-byte aligned after the tables (global-memory LU)
+    if (!lu_in_smem && P.tail_k > 0)
+        return ((xb + lb + bb + nb + 7) & ~(size_t)7) + 16 + tail_smem_bytes(P.tail_k, lu_bytes);
     return xb + lb + bb + nb;
 }
 

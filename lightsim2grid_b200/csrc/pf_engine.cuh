@@ -46,6 +46,11 @@ struct DevPlan {
     // operations (kind 7 padding) and, per phase, the first chunk and the number of rounds
     const int4 *tfac_ops, *tbwd_ops, *tfwd_ops;
     const int *tfac_phase, *tbwd_phase, *tfwd_phase;
+    // dense tail (global-memory LU plans): steps [tail_ct, tail_ct + tail_k) factorised and
+    // substituted as one dense row-major block in the CTA's slab; tail_map: LU position of each
+    // block entry (-1 outside the pattern)
+    int tail_ct, tail_k;
+    const int *tail_map;
 };
 
 // One batch launch.

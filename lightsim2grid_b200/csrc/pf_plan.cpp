@@ -774,6 +774,43 @@ void make_csr(Plan &P) {
 // fill maps for the matrix whose pattern is P.Jp / P.Ji (m = P.m columns), whose entry t takes
 // its values from Ybus position jsrc[t] (part jkind[t]) or the constant jconst[t] (jsrc < 0),
 // and whose values for the first factorisation are Jx.
+// Dense tail of a plan.  The fill of a grid with long-range branches gathers in the last
+// columns of the elimination order (minimum degree leaves the dense separator for last), where
+// the phase programs would run hundreds of levels of scattered single updates.  When the
+// trailing block of the largest size tail_k in [kTailMin, kTailMax] whose LU pattern is at least
+// kTailDensity full exists, steps [tail_ct, m) become a dense tail: the factor program keeps the
+// updates by the pivots before tail_ct (the Schur complement the sparse part contributes to the
+// block) and their pushes, the forward program the pushes of those pivots, and the backward
+// program the pushes into the rows before tail_ct (those of the block's columns first, at level
+// 0).  The kernel gathers the block into a dense matrix after the factor program, factorises it
+// without pivoting (the plan's pivots are already in the block's order) and runs the block's
+// substitutions densely, in the programs' conventions (undivided backward values).
+void choose_tail(Plan &P) {
+    const int m = P.m;
+    P.tail_ct = m;
+    P.tail_k = 0;
+    P.tail_map.clear();
+    if (m < kTailMin) return;
+    // entries of the trailing block from step c on: LU positions with min(row, column) >= c
+    std::vector<long long> cnt(m + 1, 0);
+    for (int k = 0; k < m; ++k)
+        for (int p = P.colstart[k]; p < P.colstart[k + 1]; ++p) cnt[std::min(P.Urow_k[p], k)]++;
+    for (int c = m - 1; c >= 0; --c) cnt[c] += cnt[c + 1];
+    int best = 0;
+    for (int k = kTailMin; k <= std::min(kTailMax, m); ++k)
+        if ((double)cnt[m - k] >= kTailDensity * (double)k * (double)k) best = k;
+    if (best == 0) return;
+    const int ct = m - best;
+    P.tail_ct = ct;
+    P.tail_k = best;
+    P.tail_map.assign((size_t)best * best, -1);
+    for (int k = ct; k < m; ++k)
+        for (int p = P.colstart[k]; p < P.colstart[k + 1]; ++p) {
+            const int r = P.Urow_k[p];
+            if (r >= ct) P.tail_map[(size_t)(r - ct) * best + (k - ct)] = p;
+        }
+}
+
 int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, std::string &msg) {
     const int m = P.m;
     std::ostringstream err;
@@ -907,6 +944,12 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
                                    ? compact_lu_offset(m)
                                    : -1;
     P.bank_lanes = packed_lu_base >= 0 ? (opt.elem_bytes == 8 ? 16 : 32) : 0;
+    // a dense tail only where the LU cannot sit in shared memory (no packed layout)
+    P.tail_ct = m;
+    P.tail_k = 0;
+    P.tail_map.clear();
+    if (opt.dense_tail && packed_lu_base < 0) choose_tail(P);
+    const int ct = P.tail_ct;
     // U row lists: for pivot c, the columns j > c with U(c, j) != 0 and the position of U(c, j)
     std::vector<std::vector<std::pair<int, int>>> urows(m);
     for (int k = 0; k < m; ++k)
@@ -955,7 +998,8 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         for (int l = 0; l < nplev; ++l) {
             B.begin();
             if (l < nlev)
-                for (int c : bylevel[l])
+                for (int c : bylevel[l]) {
+                    if (c >= ct) continue;  // the dense tail factorises the block
                     for (auto &e : urows[c]) {
                         const int j = e.first;
                         for (int p = P.colstart[j]; p < P.colstart[j + 1]; ++p) rowpos[P.Urow_k[p]] = p;
@@ -969,8 +1013,11 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
                         }
                         for (int p = P.colstart[j]; p < P.colstart[j + 1]; ++p) rowpos[P.Urow_k[p]] = -1;
                     }
-            for (int k : bypush[l])
+                }
+            for (int k : bypush[l]) {
+                if (k >= ct) continue;
                 for (int t = 0; t < P.lcount[k]; ++t) B.add(Lrows[k][t], P.lstart[k] + t, k, P.dpos[k], 2);
+            }
             B.end();
         }
         B.finish();
@@ -979,9 +1026,12 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         // backward substitution U z = y, from the last pivot: blevel(k) = 1 + max over U(k, j)
         std::vector<int> blev(m, 0);
         int nb = 0;
+        // (with a dense tail, the block's values are final before the program: its columns push
+        // into the rows before the block at level 0)
         for (int k = m - 1; k >= 0; --k) {
             int lv = 0;
-            for (auto &e : urows[k]) lv = std::max(lv, blev[e.first] + 1);
+            if (k < ct)
+                for (auto &e : urows[k]) lv = std::max(lv, blev[e.first] + 1);
             blev[k] = lv;
             nb = std::max(nb, lv + 1);
         }
@@ -998,7 +1048,8 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         for (int l = 0; l < nb; ++l) {
             B.begin();
             for (int k : byb[l])
-                for (int p = P.colstart[k]; p < P.dpos[k]; ++p) B.add(P.Urow_k[p], p, k, P.dpos[k], 2);
+                for (int p = P.colstart[k]; p < P.dpos[k]; ++p)
+                    if (P.Urow_k[p] < ct) B.add(P.Urow_k[p], p, k, P.dpos[k], 2);
             B.end();
         }
         B.finish();
@@ -1023,8 +1074,10 @@ int analyze_lu(Plan &P, const std::vector<double> &Jx, const PlanOptions &opt, s
         B.spread = opt.spread_clusters;
         for (int l = 0; l < nf; ++l) {
             B.begin();
-            for (int k : byf[l])
+            for (int k : byf[l]) {
+                if (k >= ct) continue;
                 for (int t = 0; t < P.lcount[k]; ++t) B.add(Lrows[k][t], P.lstart[k] + t, k, P.dpos[k], 2);
+            }
             B.end();
         }
         B.finish();
@@ -1261,7 +1314,9 @@ int build_dc_plan(Plan &P, int n, const int *Yp, const int *Yi, const cplx *Yx, 
     for (int c = 0; c < m; ++c) P.Jp[c + 1] = std::max(P.Jp[c + 1], P.Jp[c]);
     std::vector<double> Bx(P.Ji.size());
     for (size_t t = 0; t < Bx.size(); ++t) Bx[t] = Yx[P.jsrc[t]].real();
-    const int rc = analyze_lu(P, Bx, opt, msg);
+    PlanOptions o2 = opt;
+    o2.dense_tail = false;  // the DC kernel has no dense tail
+    const int rc = analyze_lu(P, Bx, o2, msg);
     if (rc != NoError) return rc;
     // bus maps: right-hand side Re(Sbus(b)) at xP[b], angle at xVa[b]
     P.xP.assign(n, -1);
@@ -1315,7 +1370,9 @@ int fdpf_system(Plan &S, int n, const RealCsc &B, const std::vector<int> &ids, c
         return NoError;
     }
     std::string sub;
-    const int rc = analyze_lu(S, Bx, opt, sub);
+    PlanOptions o2 = opt;
+    o2.dense_tail = false;  // the fast-decoupled kernel has no dense tail
+    const int rc = analyze_lu(S, Bx, o2, sub);
     if (rc != NoError) {
         msg = std::string("build_fdpf_plan: ") + what + ": " + sub;
         return rc;

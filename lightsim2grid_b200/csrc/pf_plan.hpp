@@ -114,6 +114,12 @@ struct Plan {
     std::vector<int> xVa, xVm;        // update: Va / Vm correction of bus b -> solution index
     int xSlack = -1;                  // distributed slack: solution index of slack_absorbed
 
+    // dense tail: the last tail_k steps [tail_ct, m) form a trailing block dense enough to be
+    // factorised and substituted as one dense matrix (row-major, tail_k x tail_k) instead of by
+    // the phase programs, whose operations inside the block were taken out (see dense_tail)
+    int tail_ct = 0, tail_k = 0;      // tail_k == 0: none
+    std::vector<int> tail_map;        // tail_k^2: LU position of block entry (a, b), -1 if outside the pattern
+
     // statistics
     long long flops_refactor = 0;     // multiply-adds of one refactorisation
     int levels_refactor = 0, levels_fwd = 0, levels_bwd = 0;
@@ -140,7 +146,15 @@ struct PlanOptions {
                                       // minimum degree only
     int level_slack = 2;              // minimum degree prefers, among the vertices of degree at most
                                       // the minimum + level_slack, the one of lowest level; 0: off
+    bool dense_tail = true;           // Newton plans whose LU cannot sit in shared memory: the dense
+                                      // trailing block, when there is one, becomes a dense tail
 };
+
+// Trailing blocks of at least kTailMin and at most kTailMax steps, whose LU pattern is at least
+// kTailDensity full, are factorised as dense tails.
+constexpr int kTailMin = 256;
+constexpr int kTailMax = 768;
+constexpr double kTailDensity = 0.5;
 
 // Builds a plan.  Ybus CSC (n x n, complex), V0 and Sbus (used for the first
 // factorisation's pivots).  Returns an Err code; `msg` receives a description on failure.
