@@ -565,6 +565,9 @@ def _serve(seconds, rate, device, reserved_sms=None, large_request_ctas=0, devic
     nb = {k: v.n_bus for k, v in grids.items()}
     nbr = {k: v.nb_powerline() for k, v in grids.items()}
     srv.serve(make_requests(nb, rate=rate, duration=min(1.0, seconds), seed=12345, branches_of=nbr))  # warm-up
+    for g in SERVE_GRIDS:
+        for kind in ("pf", "n1"):
+            srv.native.latency_split(g, kind, reset=True)
     reqs = make_requests(nb, rate=rate, duration=seconds, seed=2024, branches_of=nbr)
     done = srv.serve(reqs, realtime=True)
     st = latency_stats(done)
@@ -579,7 +582,9 @@ def _serve(seconds, rate, device, reserved_sms=None, large_request_ctas=0, devic
                 per["{}/{}".format(g, kind)] = {"p50_ms": float(np.percentile(lat, 50) * 1e3),
                                                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "count": int(lat.size),
                                                 "submit_lag_p99_ms": float(np.percentile(lag, 99) * 1e3) if lag.size
-                                                else None}
+                                                else None,
+                                                # the serving core's clock: admission wait and device time
+                                                "core": srv.native.latency_split(g, kind)}
     st.update({"duration_s": seconds, "arrival_rate": rate, "grids": list(SERVE_GRIDS), "per_class": per,
                "reserved_sms": reserved_sms, "large_request_ctas": large_request_ctas,
                "mode": "device-resident request loop" if device_loop else "one launch per request",

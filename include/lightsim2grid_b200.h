@@ -393,6 +393,12 @@ int pf_server_configure(pf_server *server, int reserved_sms, int large_request_c
    queued or running.  Results are those of the launch-per-request mode, bit for bit. */
 int pf_server_device_loop(pf_server *server, int enable, int ctas_shared, int ctas_global);
 int pf_server_state(const pf_server *server, int *pending, int *inflight, long long *bytes_in_use);
+/* Latency split of a server's finished requests of one grid and kind (no counterpart in the
+   reference): out[0..1] = p50 / p99 of the admission wait (pf_server_submit to the launch or
+   publication by pf_server_poll), out[2..3] = p50 / p99 of the device time (that to the
+   pf_server_poll that saw the request finished), in ms of the host's steady clock; out[4] = how
+   many requests.  reset != 0 clears the figures after reading them. */
+int pf_server_latency_split(pf_server *server, int grid, int kind, double *out, int reset);
 void pf_server_destroy(pf_server *server);
 
 /* Scratch bytes pf_batch_device_scratch needs to run `ctas` CTAs at once (at most the plan's

@@ -77,7 +77,7 @@ SYMBOLS = ("pf_last_error", "pf_plan_create", "pf_plan_destroy", "pf_plan_info_g
            "pf_flows_device", "pf_flows_host", "pf_ybus_positions", "pf_assemble_ybus_device",
            "pf_set_ybus_values_device", "pf_assemble_sbus_device", "pf_dc_plan_create", "pf_server_create",
            "pf_server_submit", "pf_server_poll", "pf_server_state", "pf_server_destroy", "pf_fdpf_plan_create", "pf_n1_order",
-           "pf_server_configure", "pf_server_device_loop")
+           "pf_server_configure", "pf_server_device_loop", "pf_server_latency_split")
 
 
 def load(path=None):
@@ -159,6 +159,8 @@ def load(path=None):
     lib.pf_server_device_loop.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.pf_server_state.restype = ctypes.c_int
     lib.pf_server_state.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.pf_server_latency_split.restype = ctypes.c_int
+    lib.pf_server_latency_split.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
     lib.pf_server_destroy.restype = None
     lib.pf_server_destroy.argtypes = [ctypes.c_void_p]
     lib.pf_dc_plan_create.restype = ctypes.c_int

@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <complex>
 #include <condition_variable>
 #include <cstring>
@@ -36,6 +37,11 @@ int fail(const std::string &msg) {
 }
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// host clock for the latency split (seconds)
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 // First-fit allocator over [0, size): holes sorted by offset, coalesced on release.
 struct Arena {
@@ -128,6 +134,8 @@ struct Req {
     int ctas = 0;        // CTAs of its launch
     int sms = 0;         // SMs those CTAs occupy (large requests)
     int cls = -1;        // device loop: the loop class that runs it
+    bool slot_freed = false;  // delivered by the polling thread, slot already returned
+    double t_sub = 0.0, t_adm = 0.0;  // host clock at submission and at admission (launch or publish)
 };
 
 // Device-resident request loop: the grids whose plans share an LU placement form a class, served by
@@ -176,20 +184,24 @@ struct pf_server {
     std::vector<Req *> inflight;
     // SM reservation for small requests (see kSmallWork)
     int num_sms = 1, reserved_sms = 0, large_ctas = 1 << 30, large_sms_inflight = 0;
-    // delivery: copying a finished request's rows from pinned staging into the caller's arrays
-    // (megabytes for N-1 batches of the large grids) runs on worker threads, so the polling thread
-    // keeps admitting and completing other requests meanwhile
+    // delivery: copying a finished large request's rows from pinned staging into the caller's
+    // arrays (megabytes for N-1 batches of the large grids) runs on worker threads, so the polling
+    // thread keeps admitting and completing other requests meanwhile; small requests' rows are
+    // copied by the polling thread itself and returned by the same poll
     std::vector<std::thread> workers;
     mutable std::mutex mu;
     std::condition_variable cv;
     std::deque<Req *> to_deliver;   // device work done, rows not yet copied
-    std::vector<Req *> delivered;   // rows copied: slot and id returned by the next poll
+    std::vector<Req *> delivered;   // rows copied: slot (unless freed) and id returned by the next poll
     bool stop = false;
     // device-resident request loop (pf_server_device_loop)
     bool loop = false;
     std::vector<LoopClass> classes;
     int *done_host = nullptr, *done_dev = nullptr;  // mapped: instances finished per slot
     int req_seq = 0;
+    // latency split per grid and kind (index 2 * grid + kind): admission wait (submission to
+    // launch or publication) and device time (that to the poll that saw it finished), ms
+    std::vector<std::vector<float>> wait_ms, run_ms;
 };
 
 namespace {
@@ -469,6 +481,14 @@ void delivery_worker(pf_server *s) {
     }
 }
 
+// percentile q (0..1) of v (sorted in place), nearest rank
+double pct(std::vector<float> &v, double q) {
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    const size_t k = std::min(v.size() - 1, (size_t)(q * (double)(v.size() - 1) + 0.5));
+    return v[k];
+}
+
 }  // namespace
 
 extern "C" {
@@ -531,6 +551,8 @@ int pf_server_create(const pf_server_grid *grids, int ngrids, long long hbm_budg
         return fail(std::string("pf_server_create: device memory: ") + cudaGetErrorString(e));
     }
     s->arena.init(s->budget);
+    s->wait_ms.assign(2 * s->grids.size(), {});
+    s->run_ms.assign(2 * s->grids.size(), {});
     s->slots.resize(slots);
     int prio_low = 0, prio_high = 0;
     cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
@@ -574,6 +596,7 @@ int pf_server_submit(pf_server *s, long long id, int grid, int kind, const doubl
         !errs_out || (kind == 0 && !scale) || (kind == 1 && (nbranches <= 0 || !branches)))
         return fail("pf_server_submit: invalid argument");
     Req *r = new Req();
+    r->t_sub = now_s();
     r->id = id;
     r->grid = grid;
     r->kind = kind;
@@ -608,7 +631,7 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
         size_t k = 0;
         for (; k < s->delivered.size() && nd < cap; ++k) {
             Req *r = s->delivered[k];
-            (s->slots[r->slot].high ? s->free_high : s->free_low).push_back(r->slot);
+            if (!r->slot_freed) (s->slots[r->slot].high ? s->free_high : s->free_low).push_back(r->slot);
             done_ids[nd++] = r->id;
             delete r;
         }
@@ -637,16 +660,38 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
             }
             if (q != cudaSuccess) return fail(std::string("pf_server_poll: ") + cudaGetErrorString(q));
         }
+        {
+            const double t = now_s();
+            s->wait_ms[2 * r->grid + r->kind].push_back((float)((r->t_adm - r->t_sub) * 1e3));
+            s->run_ms[2 * r->grid + r->kind].push_back((float)((t - r->t_adm) * 1e3));
+        }
         if (!r->small) s->large_sms_inflight -= r->sms;
         s->arena.release(r->off, r->bytes);
         s->in_use -= align256(r->bytes);
+        s->inflight[i] = s->inflight.back();
+        s->inflight.pop_back();
+        if (r->small) {
+            // a small request's rows (at most kSmallWork x 16 bytes) are copied here and its id
+            // returned by this poll: handed to the workers it would wait behind the megabyte
+            // copies of large N-1 results queued before it
+            deliver(s, r);
+            (s->slots[r->slot].high ? s->free_high : s->free_low).push_back(r->slot);
+            if (nd < cap) {
+                done_ids[nd++] = r->id;
+                delete r;
+            } else {
+                // no room in the caller's array: the slot is free, the id comes with the next poll
+                r->slot_freed = true;
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->delivered.push_back(r);
+            }
+            continue;
+        }
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->to_deliver.push_back(r);
         }
         queued = true;
-        s->inflight[i] = s->inflight.back();
-        s->inflight.pop_back();
     }
     if (queued) s->cv.notify_all();
     // the loops: one that left (its CTAs ran out of published jobs) while requests of its class are
@@ -699,6 +744,7 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
         std::vector<int> &pool = pref.empty() ? other : pref;
         r->slot = pool.back();
         pool.pop_back();
+        r->t_adm = now_s();
         int rc = 0;
         if (r->cls >= 0) {
             if (r->ninst > 0) rc = publish(s, r);
@@ -796,6 +842,22 @@ int pf_server_configure(pf_server *s, int reserved_sms, int large_request_ctas) 
     if (!s || reserved_sms < 0 || large_request_ctas < 0) return fail("pf_server_configure: invalid argument");
     s->reserved_sms = std::min(reserved_sms, s->num_sms - 1);
     s->large_ctas = large_request_ctas > 0 ? large_request_ctas : (1 << 30);
+    return 0;
+}
+
+int pf_server_latency_split(pf_server *s, int grid, int kind, double *out, int reset) {
+    if (!s || grid < 0 || grid >= (int)s->grids.size() || (kind != 0 && kind != 1) || !out)
+        return fail("pf_server_latency_split: invalid argument");
+    std::vector<float> &w = s->wait_ms[2 * grid + kind], &d = s->run_ms[2 * grid + kind];
+    out[0] = pct(w, 0.5);
+    out[1] = pct(w, 0.99);
+    out[2] = pct(d, 0.5);
+    out[3] = pct(d, 0.99);
+    out[4] = (double)d.size();
+    if (reset) {
+        w.clear();
+        d.clear();
+    }
     return 0;
 }
 
