@@ -13,6 +13,8 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double cabs2(double2 a) { return sqrt(a.x * a.x + a.y * a.y); }
 
+constexpr double kPi = 3.141592653589793;
+
 // dS/dVa and dS/dVm of Ybus entry (r, c), as BaseNRAlgo::_dSbus_dV (BaseNRAlgo.tpp:228-257)
 __device__ __forceinline__ void dsbus(double2 y, double2 vr, double2 vc, bool diag, double2 ib, double &dvar,
                                       double &dvai, double2 &dvm) {

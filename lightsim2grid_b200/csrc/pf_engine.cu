@@ -171,15 +171,16 @@ __device__ void mismatch(const DevPlan &P, Shared &S, const double2 *__restrict_
     int lbad = 0;
     const double sa = S.slack_absorbed;
     for (int r = threadIdx.x; r < P.n; r += blockDim.x) {
+        // the row's own loads are issued before the row product (they do not depend on it)
+        const double2 sb = __ldcg(Sbus + r);
+        const int ip = P.xP[r], iq = P.xQ[r];
         const double2 s = ybus_row_product(P, S, V, r);
         Ibus[r] = s;
         const double2 vr = V[r];
-        const double2 sb = __ldcg(Sbus + r);
         double mr = vr.x * s.x + vr.y * s.y - sb.x;  // V * conj(I) - S
         const double mi = vr.y * s.x - vr.x * s.y - sb.y;
         if (P.distributed) mr += sa * P.w[r];
         Fbus[r] = make_double2(mr, mi);
-        const int ip = P.xP[r], iq = P.xQ[r];
         if (ip >= 0) {
             x[ip] = (XT)mr;
             lmax = fmax(lmax, fabs(mr));
@@ -508,8 +509,13 @@ __device__ void newton_residual(const DevPlan &P, Shared &S, const double2 *__re
 }
 // The voltage update of a Newton step: Va -= dVa, Vm -= dVm (the FP32 step plus, when refined, the
 // FP64 first step), V = Vm e^(j Va) into the slab (and the shared copy Vs); returns the thread's
-// smallest new magnitude.  Pairs of buses: their loads (voltages, step positions, then the step
-// values) are issued together before the arithmetic of the first bus.
+// smallest new magnitude.  Pairs of buses: their loads (magnitudes and angles, step positions, then
+// the step values) are issued together before the arithmetic of the first bus.
+// The reference re-derives Vm = |V| and Va = arg(V) before every update (BaseNRSingleSlackAlgo.tpp:
+// 131-132), which changes them only where the last magnitude was negative or the angle left
+// (-pi, pi]; elsewhere they equal the updated values up to rounding.  So a bus keeps its updated Vm
+// and Va and only those buses take |V| and arg(V) (two FP64 library calls per bus fewer: the update
+// is bound by FP64 arithmetic).  The distributed-slack form keeps its own block-wide re-derivation.
 template <typename XT>
 __device__ double voltage_update(const DevPlan &P, double2 *__restrict__ V, double2 *__restrict__ Vs,
                                            double *__restrict__ Vm, double *__restrict__ Va,
@@ -527,14 +533,8 @@ __device__ double voltage_update(const DevPlan &P, double2 *__restrict__ V, doub
             const bool ok = b < n;
             ia[i] = ok ? P.xVa[b] : -1;
             im[i] = ok ? P.xVm[b] : -1;
-            if (P.distributed) {
-                vm[i] = ok ? Vm[b] : 1.0;
-                va[i] = ok ? Va[b] : 0.0;
-            } else {
-                const double2 v = ok ? V[b] : make_double2(1.0, 0.0);
-                vm[i] = cabs2(v);
-                va[i] = atan2(v.y, v.x);
-            }
+            vm[i] = ok ? Vm[b] : 1.0;
+            va[i] = ok ? Va[b] : 0.0;
         }
         double da[R], dm[R];
 #pragma unroll
@@ -551,11 +551,17 @@ __device__ double voltage_update(const DevPlan &P, double2 *__restrict__ V, doub
             if (im[i] >= 0) mg -= dm[i];
             double sn, cs;
             sincos(a, &sn, &cs);
-            V[b] = make_double2(mg * cs, mg * sn);
-            if (Vs) Vs[b] = make_double2(mg * cs, mg * sn);
+            const double2 v = make_double2(mg * cs, mg * sn);
+            V[b] = v;
+            if (Vs) Vs[b] = v;
+            lmin = fmin(lmin, mg);
+            if (!P.distributed && !(mg >= 0.0 && fabs(a) <= kPi)) {
+                // the reference's re-derivation, where it changes the values (or they are not finite)
+                mg = cabs2(v);
+                a = atan2(v.y, v.x);
+            }
             Vm[b] = mg;
             Va[b] = a;
-            lmin = fmin(lmin, mg);
         }
     }
     return lmin;

@@ -442,24 +442,23 @@ __global__ void __launch_bounds__(1024, 1) nr_tile_kernel(const DevPlan P, const
             double lmin = 1.0;
             if (solve)
                 for (int r = warp; r < n; r += kW) {
-                    double vm, va;
-                    if (P.distributed) {
-                        vm = Vm[ix(r, lane)];
-                        va = Va[ix(r, lane)];
-                    } else {
-                        const double2 v = V[ix(r, lane)];
-                        vm = cabs2(v);
-                        va = atan2(v.y, v.x);
-                    }
+                    // Vm and Va as updated, re-derived from V only where that changes them (as
+                    // in the one-CTA kernel's voltage_update)
+                    double vm = Vm[ix(r, lane)], va = Va[ix(r, lane)];
                     const int ia = P.xVa[r], im = P.xVm[r];
                     if (ia >= 0) va -= refine ? dxg[ix(ia, lane)] + (double)x[ix(ia, lane)] : (double)x[ix(ia, lane)];
                     if (im >= 0) vm -= refine ? dxg[ix(im, lane)] + (double)x[ix(im, lane)] : (double)x[ix(im, lane)];
                     double sn, cs;
                     sincos(va, &sn, &cs);
-                    V[ix(r, lane)] = make_double2(vm * cs, vm * sn);
+                    const double2 v = make_double2(vm * cs, vm * sn);
+                    V[ix(r, lane)] = v;
+                    lmin = fmin(lmin, vm);
+                    if (!P.distributed && !(vm >= 0.0 && fabs(va) <= kPi)) {
+                        vm = cabs2(v);
+                        va = atan2(v.y, v.x);
+                    }
                     Vm[ix(r, lane)] = vm;
                     Va[ix(r, lane)] = va;
-                    lmin = fmin(lmin, vm);
                 }
             if (P.distributed) {
                 S.red[warp][lane] = lmin;
