@@ -182,6 +182,12 @@ def _algorithmic_bytes(info, iters, b):
     return float(np.sum(iters) * per_it + len(iters) * per_inst), per_it
 
 
+def _launch_bound(threads):
+    """The Newton kernel's launch-bound template argument for a thread count (the library runs
+    the 512-, 640- or 768-thread variant)."""
+    return 768 if threads > 640 else (640 if threads > 512 else 512)
+
+
 def _dv(a, b):
     """Per row: max over buses of max(|d|V||, |d angle|) (pu, rad)."""
     dm = np.abs(np.abs(a) - np.abs(b))
@@ -833,7 +839,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "nr_batch_kernel<float,float,1,1,0,{}>".format(
-                             768 if mixed["dev"].plan.info()["threads"] > 512 else 512),
+                             _launch_bound(mixed["dev"].plan.info()["threads"])),
                          "algorithmic_bytes_per_launch": mixed["abytes"],
                          "algorithmic_bytes_per_instance_iteration": mixed["per_it"],
                          "kernel_ms": 1e3 * kt,
