@@ -130,6 +130,29 @@ def test_edge_cases_match_oracle():
             assert _vdiff(s.get_V(), o.get_V()) <= TOL_FP64, name
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("distributed", [False, True])
+def test_angles_across_pi_match_oracle(precision, distributed):
+    """Start voltages turned by 3.1 rad: the angles of many buses cross pi during the iterations,
+    where the reference's re-derivation of Va = arg(V) wraps them (BaseNRSingleSlackAlgo.tpp:
+    131-132); the engine must give the oracle's flags, iterations and voltages."""
+    c = grid_problem("grid118")
+    V0 = c["V0"] * np.exp(1j * 3.1)
+    for scale in (1.0, 1.5):
+        args = (c["Ybus"], V0, scale * c["Sbus"], c["ref"], c["weights"], c["pv"], c["pq"], 10, 1e-8)
+        o = OracleNR(distributed)
+        ok_o = o.compute_pf(*args)
+        s = _solvers()[(distributed, precision)]()
+        ok = s.compute_pf(*args)
+        assert ok == ok_o
+        if precision == 0:
+            assert s.get_nb_iter() == o.get_nb_iter()
+        if ok:
+            V = s.get_V()
+            assert np.abs(np.angle(V)).max() > 3.0  # the solution sits across the wrap
+            assert np.abs(V - o.get_V()).max() <= (TOL_FP64 if precision == 0 else TOL_MIXED)
+
+
 def _n1(c, ncases=None):
     g = c["grid"]
     nb = g.nb_powerline() if ncases is None else min(ncases, g.nb_powerline())

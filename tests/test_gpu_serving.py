@@ -99,3 +99,27 @@ def test_device_loop_equals_launch_per_request(server):
         a = again[rid]
         assert np.array_equal(r.errs, a.errs) and np.array_equal(r.iters, a.iters), rid
         assert np.array_equal(r.V, a.V), rid
+
+
+def test_latency_split_counts_every_request(server):
+    """pf_server_latency_split: per grid and kind, every finished request is counted once, with
+    non-negative admission wait and device time, and reset clears the counts."""
+    g = server.grids
+    for name in g:
+        for kind in ("pf", "n1"):
+            server.native.latency_split(name, kind, reset=True)
+    reqs = _requests(server, seed=31, duration=0.03)
+    done = server.serve(reqs, realtime=True)
+    assert len(done) == len(reqs)
+    total = 0
+    for name in g:
+        for kind in ("pf", "n1"):
+            n = sum(1 for r in done if r.grid == name and r.kind == kind)
+            sp = server.native.latency_split(name, kind, reset=True)
+            assert sp["count"] == n, (name, kind)
+            if n:
+                assert 0.0 <= sp["wait_p50_ms"] <= sp["wait_p99_ms"]
+                assert 0.0 <= sp["device_p50_ms"] <= sp["device_p99_ms"]
+            assert server.native.latency_split(name, kind)["count"] == 0
+            total += n
+    assert total == len(reqs)
