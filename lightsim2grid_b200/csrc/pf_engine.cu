@@ -467,9 +467,10 @@ __device__ void check_pivots(const DevPlan &P, Shared &S, const LT *lu) {
 // BaseNRAlgo::_dSbus_dV, BaseNRAlgo.tpp:228-257), so J dx is formed from the voltage
 // step dV = V / |V| dVm + j V dVa:  J dx = dV conj(I) + V conj(Y dV)  (I = Y V, the current
 // injections of the mismatch), plus the slack-absorption column of a distributed slack.
-// Two passes: dV per bus into the slab, then one Ybus row product per equation row.
+// Two passes: dV per bus into the slab, then one Ybus row product per equation row.  Returns
+// max |F - J dx| to every thread (infinity when a value is not finite).
 template <typename XT>
-__device__ void newton_residual(const DevPlan &P, Shared &S, const double2 *__restrict__ V,
+__device__ double newton_residual(const DevPlan &P, Shared &S, const double2 *__restrict__ V,
                                 const double2 *__restrict__ Ibus, const double2 *__restrict__ Fbus,
                                 const double *__restrict__ dxg, double2 *__restrict__ dV, XT *x) {
     const int bd = blockDim.x;
@@ -494,6 +495,8 @@ __device__ void newton_residual(const DevPlan &P, Shared &S, const double2 *__re
         }
     }
     __syncthreads();
+    double lmax = 0.0;
+    int lbad = 0;
     for (int r = threadIdx.x; r < P.n; r += bd) {
         const int ip = P.xP[r], iq = P.xQ[r];
         if (ip < 0 && iq < 0) continue;
@@ -503,13 +506,28 @@ __device__ void newton_residual(const DevPlan &P, Shared &S, const double2 *__re
         const double jQ = dvr.y * ir.x - dvr.x * ir.y + (vr.y * yd.x - vr.x * yd.y);
         if (P.distributed && ip >= 0) jP += P.wJ[r] * dxg[P.xSlack];
         const double2 F = Fbus[r];
-        if (ip >= 0) x[ip] = (XT)(F.x - jP);
-        if (iq >= 0) x[iq] = (XT)(F.y - jQ);
+        if (ip >= 0) {
+            const double rp = F.x - jP;
+            x[ip] = (XT)rp;
+            lmax = fmax(lmax, fabs(rp));
+            lbad |= !isfinite(rp);
+        }
+        if (iq >= 0) {
+            const double rq = F.y - jQ;
+            x[iq] = (XT)rq;
+            lmax = fmax(lmax, fabs(rq));
+            lbad |= !isfinite(rq);
+        }
     }
+    double rmax;
+    int bad;
+    block_norm(S, lmax, lbad, rmax, bad);
+    return bad ? INFINITY : rmax;
 }
-// The voltage update of a Newton step: Va -= dVa, Vm -= dVm (the FP32 step plus, when refined, the
-// FP64 first step), V = Vm e^(j Va) into the slab (and the shared copy Vs); returns the thread's
-// smallest new magnitude.  Pairs of buses: their loads (magnitudes and angles, step positions, then
+// The voltage update of a Newton step: Va -= dVa, Vm -= dVm (the FP32 step x; when refined, the
+// FP64 first step dxg plus xw times the correction x, xw = 0 when the correction was skipped),
+// V = Vm e^(j Va) into the slab (and the shared copy Vs); returns the thread's smallest new
+// magnitude.  Pairs of buses: their loads (magnitudes and angles, step positions, then
 // the step values) are issued together before the arithmetic of the first bus.
 // The reference re-derives Vm = |V| and Va = arg(V) before every update (BaseNRSingleSlackAlgo.tpp:
 // 131-132), which changes them only where the last magnitude was negative or the angle left
@@ -519,7 +537,8 @@ __device__ void newton_residual(const DevPlan &P, Shared &S, const double2 *__re
 template <typename XT>
 __device__ double voltage_update(const DevPlan &P, double2 *__restrict__ V, double2 *__restrict__ Vs,
                                            double *__restrict__ Vm, double *__restrict__ Va,
-                                           const double *__restrict__ dxg, const XT *x, bool refine_now) {
+                                           const double *__restrict__ dxg, const XT *x, bool refine_now,
+                                           double xw) {
     const int n = P.n;
     double lmin = 1.0;
     constexpr int R = 2;
@@ -539,8 +558,8 @@ __device__ double voltage_update(const DevPlan &P, double2 *__restrict__ V, doub
         double da[R], dm[R];
 #pragma unroll
         for (int i = 0; i < R; ++i) {
-            da[i] = ia[i] >= 0 ? (refine_now ? dxg[ia[i]] + (double)x[ia[i]] : (double)x[ia[i]]) : 0.0;
-            dm[i] = im[i] >= 0 ? (refine_now ? dxg[im[i]] + (double)x[im[i]] : (double)x[im[i]]) : 0.0;
+            da[i] = ia[i] >= 0 ? (refine_now ? dxg[ia[i]] + xw * (double)x[ia[i]] : (double)x[ia[i]]) : 0.0;
+            dm[i] = im[i] >= 0 ? (refine_now ? dxg[im[i]] + xw * (double)x[im[i]] : (double)x[im[i]]) : 0.0;
         }
 #pragma unroll
         for (int i = 0; i < R; ++i) {
@@ -1015,10 +1034,17 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 break;
             }
             pr.mark(4);
+            // the refinement's correction solve is skipped when the residual of the FP32 step is
+            // below a hundredth of the tolerance: the correction would move the next mismatch by
+            // less than that (J e = r), and the final voltages by at most |J^-1| tol / 100
+            double xw = 1.0;
             if (refine_now) {
                 for (int k = tid; k < m; k += blockDim.x) dxg[k] = (double)x[k];
                 __syncthreads();
-                newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, L.dV, x);
+                const double rmax = newton_residual<XT>(P, S, V, Ibus, Fbus, dxg, L.dV, x);
+                if (rmax < 0.01 * A.tol) xw = 0.0;
+            }
+            if (refine_now && xw != 0.0) {
                 __syncthreads();
                 run_lu_program<LT, XT, LU_SMEM, NARROW>(P.fwd_cops, P.fwd_ops, L.sb_fwd, L.sw_fwd, P.fwd_nph, m, lu, x, tr,
                                                 make_int3(P.nar_a[2], P.nar_b[2], P.nar_warps), L.nar_ops[2]);
@@ -1031,13 +1057,13 @@ __device__ __forceinline__ void solve_job(const DevPlan &P, const BatchArgs &A, 
                 run_lu_program<LT, XT, LU_SMEM, NARROW>(P.bwd_cops, P.bwd_ops, L.sb_bwd, L.sw_bwd, P.bwd_nph, m, lu, x, tr,
                                             make_int3(P.nar_a[1], P.nar_b[1], P.nar_warps), L.nar_ops[1]);
                 scale_by_pivots<LT, XT>(P, S, lu, x);
-                pr.mark(5);
             }
+            if (refine_now) pr.mark(5);
             // voltage update
-            const double lmin = voltage_update<XT>(P, V, Vs, Vm, Va, dxg, x, refine_now);
+            const double lmin = voltage_update<XT>(P, V, Vs, Vm, Va, dxg, x, refine_now, xw);
             if (P.distributed) {
                 const double dxs =
-                    refine_now ? dxg[P.xSlack] + (double)x[P.xSlack] : (double)x[P.xSlack];
+                    refine_now ? dxg[P.xSlack] + xw * (double)x[P.xSlack] : (double)x[P.xSlack];
                 const double vmin = block_min(S, lmin);  // contains barriers
                 if (tid == 0) S.slack_absorbed -= dxs;
                 if (vmin < 0.0) {
