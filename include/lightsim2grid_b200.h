@@ -35,7 +35,9 @@ typedef struct pf_options {
                                launch).  0: default (on), 1: on, 2: off                         */
     int max_ctas_per_sm;    /* cap on resident CTAs per SM; 0: occupancy limit               */
     int refine;             /* mixed form: refine Newton steps once against the FP64
-                               Jacobian.  0: default (on), 1: on, 2: off                       */
+                               Jacobian (the one-CTA kernel skips the correction solve when
+                               the FP64 residual is below tol / 100).  0: default (on), 1: on,
+                               2: off                                                         */
     double refine_threshold;/* ... the steps taken from ||F||_inf below this; 0: 1e-3          */
     double lu_reuse_threshold;/* mixed form: refined steps taken from ||F||_inf below this reuse
                                the previous iteration's LU instead of refactorising (capped at

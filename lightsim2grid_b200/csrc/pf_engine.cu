@@ -14,7 +14,9 @@
 // of independent operations, coloured on the host into conflict-free phases, one barrier
 // per phase, no atomics -- the result is deterministic.  LU values live in shared memory
 // when they fit, else in the CTA's global slab (L2 resident).  The mixed form (FP32 LU)
-// refines every Newton step once against the FP64 Jacobian, computed on the fly from dS/dV.
+// refines the Newton steps taken close to the solution once against the FP64 Jacobian,
+// computed on the fly from dS/dV (the correction solve is skipped when the FP64 residual is
+// already below a hundredth of the tolerance).
 #include "pf_engine.cuh"
 #include "pf_device_math.cuh"
 
