@@ -597,19 +597,23 @@ __device__ double voltage_update(const DevPlan &P, double2 *__restrict__ V, doub
 // tail_factor gathers the block from the LU and factorises it without pivoting, right-looking
 // in panels of tail_panel<LT>() columns: (a) the panel (rows [J, k)) staged in shared memory and
 // factorised there, one barrier per pivot; then, chunk after chunk of kTailChunk columns right of
-// the panel, (b) their U rows staged in shared memory and solved there (L of the panel's
+// the panel, (b) their U rows staged in shared memory (row stride kTailChunkLd) and solved there,
+// a warp per column and a lane per row, the pivots' values passed by shuffles (L of the panel's
 // diagonal block is unit lower) and (c) the trailing rows minus L U, each thread a register tile
 // of outputs read and written with 16-byte accesses.  Its pivots go back to the LU diagonal,
 // where the pivot scaling and the zero-pivot check read them.  Shared memory:
 // tail_smem_bytes(k) (the staging area also serves the substitutions' diagonal blocks).
 constexpr int kTailChunk = 128;
+// row stride of the staged U rows: rows start on 16 bytes, and the lanes of a warp reading one
+// column (a lane per row) fall in 8 different banks
+constexpr int kTailChunkLd = kTailChunk + 4;
 template <typename LT>
 __host__ __device__ constexpr int tail_panel() { return sizeof(LT) == 4 ? 32 : 16; }
 __host__ __device__ inline int tail_ld(int k) { return (k + 3) & ~3; }
 __host__ __device__ inline size_t tail_smem_bytes(int k, int lu_bytes) {
     const int nb = lu_bytes == 4 ? 32 : 16;
     // the panel (k rows of nb + 1 values), then the chunk of U rows from a 16-byte boundary
-    return k > 0 ? ((((size_t)k * (nb + 1) + 3) & ~(size_t)3) + (size_t)nb * kTailChunk) * lu_bytes : 0;
+    return k > 0 ? ((((size_t)k * (nb + 1) + 3) & ~(size_t)3) + (size_t)nb * kTailChunkLd) * lu_bytes : 0;
 }
 
 // four consecutive values at a 16-byte boundary
@@ -652,7 +656,7 @@ __device__ __noinline__ void tail_factor(const DevPlan &P, LT *lu, LT *D, LT *sm
     }
     __syncthreads();
     LT *Ap = sm;                     // panel: Ap[(i - J) * NP + c], rows [J, k)
-    // U rows of the panel, one chunk: Bc[c * kTailChunk + q], from a 16-byte boundary (read with
+    // U rows of the panel, one chunk: Bc[c * kTailChunkLd + q], from a 16-byte boundary (read with
     // 16-byte loads; sm itself is 16-byte aligned)
     LT *Bc = sm + (((size_t)k * NP + 3) & ~(size_t)3);
     for (int J = 0; J < k; J += NB) {
@@ -683,19 +687,27 @@ __device__ __noinline__ void tail_factor(const DevPlan &P, LT *lu, LT *D, LT *sm
             const int w = min(kTailChunk, k - j0), tc = (w + TC - 1) / TC;
             for (int e = tid; e < NB * kTailChunk; e += bd) {
                 const int c = e / kTailChunk, q = e - c * kTailChunk;
-                Bc[e] = (c < jb && q < w) ? D[(size_t)(J + c) * ld + j0 + q] : (LT)0;
+                Bc[c * kTailChunkLd + q] = (c < jb && q < w) ? D[(size_t)(J + c) * ld + j0 + q] : (LT)0;
             }
             __syncthreads();
-            // (b) the chunk's U rows, one thread per column
-            for (int q = tid; q < w; q += bd)
-                for (int c = 0; c < jb; ++c) {
-                    const LT u = Bc[c * kTailChunk + q];
-                    for (int i = c + 1; i < jb; ++i) Bc[i * kTailChunk + q] -= Ap[i * NP + c] * u;
+            // (b) the chunk's U rows: a warp per column, lane i holds row i; at step c the lanes
+            // below c take row c's final value by a shuffle (the same updates in the same order
+            // as a sequential column solve)
+            {
+                const int lane = tid & 31, nwarps = bd >> 5;
+                for (int q = tid >> 5; q < w; q += nwarps) {
+                    LT v = lane < jb ? Bc[lane * kTailChunkLd + q] : (LT)0;
+                    for (int c = 0; c + 1 < jb; ++c) {
+                        const LT u = __shfl_sync(0xffffffffu, v, c);
+                        if (lane > c && lane < jb) v -= Ap[lane * NP + c] * u;
+                    }
+                    if (lane < jb) Bc[lane * kTailChunkLd + q] = v;
                 }
+            }
             __syncthreads();
             for (int e = tid; e < jb * kTailChunk; e += bd) {
                 const int c = e / kTailChunk, q = e - c * kTailChunk;
-                if (q < w) D[(size_t)(J + c) * ld + j0 + q] = Bc[e];
+                if (q < w) D[(size_t)(J + c) * ld + j0 + q] = Bc[c * kTailChunkLd + q];
             }
             // (c) the trailing rows: a tile of TR rows x 4 columns per thread (columns past the
             // block's last fall in the row padding; their values are never read as entries)
@@ -714,7 +726,7 @@ __device__ __noinline__ void tail_factor(const DevPlan &P, LT *lu, LT *D, LT *sm
                     LT a[TR], bq[TC];
 #pragma unroll
                     for (int r = 0; r < TR; ++r) a[r] = i0 + r < k ? arow[r * NP + c] : (LT)0;
-                    ld4(Bc + c * kTailChunk + q0, bq);
+                    ld4(Bc + c * kTailChunkLd + q0, bq);
 #pragma unroll
                     for (int r = 0; r < TR; ++r)
 #pragma unroll
