@@ -596,7 +596,7 @@ __device__ double voltage_update(const DevPlan &P, double2 *__restrict__ V, doub
 // the block (their updates of the block are the Schur complement of the sparse part),
 // tail_factor gathers the block from the LU and factorises it without pivoting, right-looking
 // in panels of tail_panel<LT>() columns: (a) the panel (rows [J, k)) staged in shared memory and
-// factorised there (its diagonal block on one warp, the rows below it a thread each); then, chunk after chunk of kTailChunk columns right of
+// factorised there, one barrier per pivot; then, chunk after chunk of kTailChunk columns right of
 // the panel, (b) their U rows staged in shared memory (row stride kTailChunkLd) and solved there,
 // a warp per column and a lane per row, the pivots' values passed by shuffles (L of the panel's
 // diagonal block is unit lower) and (c) the trailing rows minus L U, each thread a register tile
@@ -666,32 +666,17 @@ __device__ __noinline__ void tail_factor(const DevPlan &P, LT *lu, LT *D, LT *sm
             Ap[i * NP + c] = c < jb ? D[(size_t)(J + i) * ld + J + c] : (LT)0;
         }
         __syncthreads();
-        // (a) the panel: its diagonal block on warp 0, a lane per row, pivot after pivot (the
-        // pivot row is final after the previous step: a warp barrier between steps); then every
-        // row below it on its own thread, which needs only the diagonal block's U rows (no
-        // barrier per pivot).  Each row sees the updates of a pivot-by-pivot elimination, in
-        // the same order.
-        if (tid < 32) {
-            for (int c = 0; c < jb; ++c) {
-                if (tid > c && tid < jb) {
-                    LT *row = Ap + (size_t)tid * NP;
-                    const LT l = row[c] / Ap[c * NP + c];
-                    row[c] = l;
-                    for (int j = c + 1; j < jb; ++j) row[j] -= l * Ap[c * NP + j];
-                }
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-        for (int i = jb + tid; i < rows; i += bd) {
-            LT *row = Ap + (size_t)i * NP;
-            for (int c = 0; c < jb; ++c) {
-                const LT l = row[c] / Ap[c * NP + c];
+        // (a) the panel, pivot after pivot
+        for (int c = 0; c < jb; ++c) {
+            const LT piv = Ap[c * NP + c];
+            for (int i = c + 1 + tid; i < rows; i += bd) {
+                LT *row = Ap + (size_t)i * NP;
+                const LT l = row[c] / piv;
                 row[c] = l;
                 for (int j = c + 1; j < jb; ++j) row[j] -= l * Ap[c * NP + j];
             }
+            __syncthreads();
         }
-        __syncthreads();
         for (int e = tid; e < rows * NB; e += bd) {
             const int i = e / NB, c = e - i * NB;
             if (c < jb) D[(size_t)(J + i) * ld + J + c] = Ap[i * NP + c];
