@@ -399,7 +399,8 @@ int pf_server_state(const pf_server *server, int *pending, int *inflight, long l
    reference): out[0..1] = p50 / p99 of the admission wait (pf_server_submit to the launch or
    publication by pf_server_poll), out[2..3] = p50 / p99 of the device time (that to the
    pf_server_poll that saw the request finished), in ms of the host's steady clock; out[4] = how
-   many requests.  reset != 0 clears the figures after reading them. */
+   many requests (the first 262,144 per grid and kind since the last reset).  reset != 0 clears
+   the figures after reading them. */
 int pf_server_latency_split(pf_server *server, int grid, int kind, double *out, int reset);
 void pf_server_destroy(pf_server *server);
 

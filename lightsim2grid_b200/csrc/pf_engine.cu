@@ -534,8 +534,8 @@ __device__ double newton_residual(const DevPlan &P, Shared &S, const double2 *__
 // The reference re-derives Vm = |V| and Va = arg(V) before every update (BaseNRSingleSlackAlgo.tpp:
 // 131-132), which changes them only where the last magnitude was negative or the angle left
 // (-pi, pi]; elsewhere they equal the updated values up to rounding.  So a bus keeps its updated Vm
-// and Va and only those buses take |V| and arg(V) (two FP64 library calls per bus fewer: the update
-// is bound by FP64 arithmetic).  The distributed-slack form keeps its own block-wide re-derivation.
+// and Va and only those buses take |V| and arg(V): two FP64 library calls (and their dependent
+// chains) per bus fewer.  The distributed-slack form keeps its own block-wide re-derivation.
 template <typename XT>
 __device__ double voltage_update(const DevPlan &P, double2 *__restrict__ V, double2 *__restrict__ Vs,
                                            double *__restrict__ Vm, double *__restrict__ Va,

@@ -38,6 +38,9 @@ int fail(const std::string &msg) {
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// the latency split keeps at most this many requests per grid and kind between resets
+constexpr size_t kSplitCap = size_t(1) << 18;
+
 // host clock for the latency split (seconds)
 double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -660,7 +663,7 @@ int pf_server_poll(pf_server *s, long long *done_ids, int cap) {
             }
             if (q != cudaSuccess) return fail(std::string("pf_server_poll: ") + cudaGetErrorString(q));
         }
-        {
+        if (s->run_ms[2 * r->grid + r->kind].size() < kSplitCap) {
             const double t = now_s();
             s->wait_ms[2 * r->grid + r->kind].push_back((float)((r->t_adm - r->t_sub) * 1e3));
             s->run_ms[2 * r->grid + r->kind].push_back((float)((t - r->t_adm) * 1e3));
