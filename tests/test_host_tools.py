@@ -49,6 +49,8 @@ def test_bench_arithmetic():
     assert abs(bench._dv(a, b)[0] - 1e-9) < 1e-15
     st = bench._err_stats(np.array([1e-12, 2e-12, 3e-10]))
     assert st["max"] == 3e-10 and st["count"] == 3
+    # the roofline names the kernel variant the library launches for a thread count
+    assert [bench._launch_bound(t) for t in (128, 512, 544, 640, 672, 768)] == [512, 512, 640, 640, 768, 768]
 
 
 def test_threaded_oracle_batch_matches_sequential_slices():
